@@ -1,0 +1,964 @@
+// Context: plan building, device state, per-step launch sequence, deposition,
+// bias-state blob and read-backs.
+#include "context.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+
+#include "../../include/glued_b200.h"
+#include "kernels.hpp"
+
+namespace glued {
+
+void cudaCheck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(GLUED_E_CUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+DBuf::~DBuf() { release(); }
+
+void DBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void DBuf::alloc(size_t n) {
+    if (p) { cudaFree(p); p = nullptr; }
+    bytes = n;
+    if (n == 0) n = 16;
+    cudaCheck(cudaMalloc(&p, n), "cudaMalloc");
+    cudaCheck(cudaMemset(p, 0, n), "cudaMemset");
+}
+
+template <class T> void DBuf::upload(const std::vector<T>& v, cudaStream_t) {
+    alloc(v.size() * sizeof(T));
+    if (!v.empty()) cudaCheck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+
+namespace {
+
+const char* cvName(int t) {
+    switch (t) {
+        case CV_POSITION: return "POSITION"; case CV_DRMSD: return "DRMSD"; case CV_PLANE: return "PLANE";
+        case CV_PROJECTION: return "PROJECTION"; case CV_PUCKERING: return "PUCKERING";
+        case CV_DIPOLE: return "DIPOLE"; case CV_VOLUME: return "VOLUME"; case CV_CELL: return "CELL";
+        case CV_SECONDARY_STRUCTURE: return "SECONDARY_STRUCTURE"; case CV_ERMSD: return "ERMSD";
+        case CV_ENERGY: return "ENERGY"; case CV_EXPRESSION: return "EXPRESSION"; case CV_PYTORCH: return "PYTORCH";
+        default: return "?";
+    }
+}
+
+bool inScopeCV(int t) {
+    switch (t) {
+        case CV_DISTANCE: case CV_ANGLE: case CV_DIHEDRAL: case CV_COM_DISTANCE: case CV_GYRATION:
+        case CV_COORDINATION: case CV_RMSD: case CV_PATH: case CV_CONTACTMAP: case CV_PCA:
+        case CV_COORDINATION_CUTOFF: case CV_RMSD_KABSCH:
+            return true;
+        default: return false;
+    }
+}
+
+// Jacobian kind order (CommonGluedKernels.cpp:4186-4230); the two extension
+// kinds follow their reference sibling.
+const int kKindOrder[] = {CV_DISTANCE, CV_ANGLE, CV_DIHEDRAL, CV_COM_DISTANCE, CV_GYRATION, CV_COORDINATION,
+                          CV_COORDINATION_CUTOFF, CV_RMSD, CV_RMSD_KABSCH, CV_PATH, CV_CONTACTMAP, CV_PCA};
+
+int bodyRows(const CVSpec& c) {
+    switch (c.type) {
+        case CV_DISTANCE: return 2;
+        case CV_ANGLE: return 3;
+        case CV_DIHEDRAL: return 4;
+        case CV_COORDINATION: case CV_COORDINATION_CUTOFF: return (int)c.atoms.size() - 1;
+        case CV_PATH: return 2 * (int)c.atoms.size();
+        case CV_CONTACTMAP: return 2 * ((int)c.atoms.size() / 2);
+        default: return (int)c.atoms.size();
+    }
+}
+
+int biasEvalRank(int t) {
+    // bias evaluation order of execute() (CommonGluedKernels.cpp:4955-5026)
+    switch (t) {
+        case BIAS_HARMONIC: return 0;
+        case BIAS_OPES: return 2;
+        case BIAS_METAD: return 4;
+        case BIAS_METAD_HILLS: return 20;
+        default: return 100;
+    }
+}
+
+}  // namespace
+
+Context::Context(const GluedForce& f, int numParticles, const double* masses)
+    : force_(f), numParticles_(numParticles) {
+    if (numParticles < 0) throw Error(GLUED_E_INVALID, "num_particles must be >= 0");
+    masses_.assign(numParticles, 1.0);
+    if (masses) for (int i = 0; i < numParticles; i++) masses_[i] = masses[i];
+    periodic_ = f.usesPBC;
+    std::memset(lastBox_, 0, sizeof lastBox_);
+    cudaCheck(cudaMallocHost(&boxPinned_, sizeof(BoxDev)), "cudaMallocHost");
+    cudaCheck(cudaMallocHost(&energiesPinned_, sizeof(double) * 64), "cudaMallocHost");
+    cudaCheck(cudaStreamCreateWithFlags(&capStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    box_.alloc(sizeof(BoxDev));
+    u2g_.alloc(sizeof(int) * std::max(1, numParticles));
+    boxHost_ = BoxDev{};
+    boxHost_.kind = 0;
+    cudaCheck(cudaMemcpy(box_.p, &boxHost_, sizeof(BoxDev), cudaMemcpyHostToDevice), "box");
+    if (f.numCVSpecs() > 0) {
+        buildPlan(f);
+        setupBiases(f);
+    }
+    if (!f.testBiasGradients.empty()) {
+        std::vector<double> g(std::max(numCVs_, 1), 0.0);
+        for (int i = 0; i < numCVs_ && i < (int)f.testBiasGradients.size(); i++) g[i] = f.testBiasGradients[i];
+        testGrad_.upload(g);
+    }
+}
+
+Context::~Context() {
+    invalidateGraphs();
+    if (capStream_) cudaStreamDestroy(capStream_);
+    if (boxPinned_) cudaFreeHost(boxPinned_);
+    if (energiesPinned_) cudaFreeHost(energiesPinned_);
+}
+
+void Context::invalidateGraphs() {
+    for (auto& g : graph_) {
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+}
+
+// --------------------------------------------------------------------- plan
+void Context::buildPlan(const GluedForce& f) {
+    numCVs_ = f.numCVValues();
+    const int nSpecs = f.numCVSpecs();
+    // Validation pass (CommonGluedKernels.cpp:3879-3927).
+    {
+        std::map<int, int> kindFirst, kindCount;
+        int v = 0;
+        for (int i = 0; i < nSpecs; i++) {
+            const CVSpec& c = f.cv(i);
+            auto err = [&](const std::string& m) { throw Error(GLUED_E_INVALID, "GluedForce CV " + std::to_string(i) + ": " + m); };
+            auto needA = [&](size_t n) { if (c.atoms.size() < n) err("expected >= " + std::to_string(n) + " atoms, got " + std::to_string(c.atoms.size())); };
+            auto needP = [&](size_t n) { if (c.params.size() < n) err("expected >= " + std::to_string(n) + " parameters, got " + std::to_string(c.params.size())); };
+            // Every entry of atoms is range-checked, including the coordination
+            // group-size slot and expression inputs, as the reference does.
+            for (int a : c.atoms)
+                if (a < 0 || a >= numParticles_)
+                    err("atom index " + std::to_string(a) + " out of range [0," + std::to_string(numParticles_) + ")");
+            int nValues = 1;
+            bool contig = true;
+            switch (c.type) {
+                case CV_DISTANCE: needA(2); break;
+                case CV_ANGLE: needA(3); break;
+                case CV_DIHEDRAL: needA(4); break;
+                case CV_COM_DISTANCE: needA(1); needP(1); break;
+                case CV_GYRATION: needA(1); break;
+                case CV_COORDINATION: case CV_COORDINATION_CUTOFF:
+                    needA(2); needP(c.type == CV_COORDINATION ? 3 : 4);
+                    if (c.atoms[0] < 1 || c.atoms[0] >= (int)c.atoms.size())
+                        err("coordination group-A size atoms[0]=" + std::to_string(c.atoms[0]) + " invalid");
+                    break;
+                case CV_RMSD: case CV_RMSD_KABSCH: needA(1); needP(3 * c.atoms.size()); break;
+                case CV_PATH: {
+                    needP(2);
+                    int N = (int)c.params[1];
+                    if (N < 2) err("path needs >= 2 frames");
+                    if (N > 128) err("path frame count " + std::to_string(N) + " exceeds MAX_PATH_FRAMES=128");
+                    needP(2 + (size_t)N * 3 * c.atoms.size());
+                    nValues = 2;
+                } break;
+                case CV_CONTACTMAP: needA(2); needP(4 * (c.atoms.size() / 2)); break;
+                case CV_PCA: needA(1); needP(6 * c.atoms.size()); break;
+                case CV_EXPRESSION: case CV_PYTORCH: contig = false; break;
+                default:
+                    if (c.type < 1 || c.type > 23) err("unknown CV type " + std::to_string(c.type));
+            }
+            if (contig) {
+                if (kindFirst.find(c.type) == kindFirst.end()) kindFirst[c.type] = v;
+                else if (kindFirst[c.type] + kindCount[c.type] != v)
+                    err("CVs of the same kind must be added contiguously (interleaving CV kinds is unsupported)");
+                kindCount[c.type] += nValues;
+            }
+            v += nValues;
+        }
+        for (int i = 0; i < nSpecs; i++) {
+            const CVSpec& c = f.cv(i);
+            if (!inScopeCV(c.type))
+                throw Error(GLUED_E_UNSUPPORTED, std::string("GluedForce CV ") + std::to_string(i) + ": type " +
+                                                     std::to_string(c.type) + " (" + cvName(c.type) +
+                                                     ") is outside this library's hot path (supported: distance, angle, "
+                                                     "dihedral, COM distance, gyration, coordination, RMSD, path, "
+                                                     "contact map, PCA)");
+        }
+    }
+    // Value slots and Jacobian offsets per kind.
+    std::vector<int> slot(nSpecs);
+    {
+        int v = 0;
+        for (int i = 0; i < nSpecs; i++) { slot[i] = v; v += f.cv(i).type == CV_PATH ? 2 : 1; }
+    }
+    std::map<int, int> kindRows, kindJac0;
+    for (int i = 0; i < nSpecs; i++) kindRows[f.cv(i).type] += bodyRows(f.cv(i));
+    {
+        int off = 0;
+        for (int t : kKindOrder) { kindJac0[t] = off; off += kindRows[t]; }
+        numRows_ = off;
+    }
+    std::vector<int> jAtom(std::max(numRows_, 1), 0), jCv(std::max(numRows_, 1), 0);
+    std::map<int, int> kindCursor;  // rows used so far inside each kind
+    std::vector<SimpleItem> simple;
+    std::vector<GroupItem> groups;
+    std::vector<int> gAtoms;
+    std::vector<float> gMass, gRef, gEv;
+    std::vector<int2> cmPairs;
+    std::vector<float4> cmParams;
+    std::vector<CoordItem> coord;
+    std::vector<int> coordAtoms;
+    // per-kind atom cursors into the shared group arrays (the reference keeps one
+    // array per kind; the row offset of an atom inside its kind is what matters)
+    for (int i = 0; i < nSpecs; i++) {
+        const CVSpec& c = f.cv(i);
+        const int t = c.type;
+        const int cv = slot[i];
+        const int jac0 = kindJac0[t] + kindCursor[t];
+        kindCursor[t] += bodyRows(c);
+        if (t == CV_DISTANCE || t == CV_ANGLE || t == CV_DIHEDRAL) {
+            SimpleItem it{};
+            it.type = t; it.cv = cv; it.jac0 = jac0;
+            int na = t == CV_DISTANCE ? 2 : t == CV_ANGLE ? 3 : 4;
+            for (int k = 0; k < na; k++) { it.atoms[k] = c.atoms[k]; jAtom[jac0 + k] = c.atoms[k]; jCv[jac0 + k] = cv; }
+            simple.push_back(it);
+        } else if (t == CV_COORDINATION || t == CV_COORDINATION_CUTOFF) {
+            CoordItem it{};
+            it.cv = cv; it.jac0 = jac0;
+            it.nA = c.atoms[0];
+            it.nB = (int)c.atoms.size() - 1 - it.nA;
+            it.a0 = (int)coordAtoms.size();
+            it.b0 = it.a0 + it.nA;
+            for (size_t k = 1; k < c.atoms.size(); k++) coordAtoms.push_back(c.atoms[k]);
+            it.r0 = (float)c.params[0]; it.n = (float)c.params[1]; it.m = (float)c.params[2];
+            double rc = (t == CV_COORDINATION_CUTOFF) ? c.params[3] : 0.0;
+            it.rc2 = (float)(rc * rc);
+            it.kind = 0;
+            bool integral = it.n == std::floor(it.n) && it.m == std::floor(it.m) && it.n >= 1 && it.m >= 1 &&
+                            it.n <= 64 && it.m <= 64;
+            if (integral) it.kind = -1;
+            if (integral && it.m == 2.0f * it.n && (int)it.n % 2 == 0 && it.n <= 8) it.kind = (int)it.n / 2;
+            for (int k = 0; k < it.nA + it.nB; k++) { jAtom[jac0 + k] = c.atoms[1 + k]; jCv[jac0 + k] = cv; }
+            coord.push_back(it);
+        } else {
+            GroupItem it{};
+            it.type = t; it.cv = cv;
+            if (t == CV_COM_DISTANCE || t == CV_GYRATION || t == CV_RMSD || t == CV_RMSD_KABSCH || t == CV_PCA) {
+                int s0 = (int)gAtoms.size();
+                it.jac0 = jac0 - s0;  // rows addressed as jac0 + j with j the global atom slot
+                for (size_t k = 0; k < c.atoms.size(); k++) {
+                    gAtoms.push_back(c.atoms[k]);
+                    gMass.push_back((float)masses_[c.atoms[k]]);
+                    jAtom[jac0 + k] = c.atoms[k]; jCv[jac0 + k] = cv;
+                }
+                it.s0 = s0; it.s1 = (int)gAtoms.size(); it.s2 = it.s1;
+                // keep gRef/gEv indexed by the same slot
+                gRef.resize(3 * gAtoms.size(), 0.0f);
+                gEv.resize(3 * gAtoms.size(), 0.0f);
+                if (t == CV_COM_DISTANCE) {
+                    int ng1 = (int)std::lround(c.params.empty() ? 1.0 : c.params[0]);
+                    it.s1 = s0 + ng1; it.s2 = (int)gAtoms.size();
+                    float m1 = 0, m2 = 0;
+                    for (int j = s0; j < it.s1; j++) m1 += gMass[j];
+                    for (int j = it.s1; j < it.s2; j++) m2 += gMass[j];
+                    it.f0 = m1; it.f1 = m2;
+                } else if (t == CV_GYRATION) {
+                    float m = 0;
+                    for (int j = s0; j < it.s1; j++) m += gMass[j];
+                    it.f0 = m;
+                } else if (t == CV_RMSD || t == CV_RMSD_KABSCH) {
+                    for (size_t k = 0; k < 3 * c.atoms.size(); k++) gRef[3 * s0 + k] = (float)c.params[k];
+                } else {
+                    size_t n3 = 3 * c.atoms.size();
+                    for (size_t k = 0; k < n3; k++) { gRef[3 * s0 + k] = (float)c.params[k]; gEv[3 * s0 + k] = (float)c.params[n3 + k]; }
+                    for (size_t k = 0; k < c.atoms.size(); k++) {
+                        // PCA Jacobian rows are the eigenvector (constant)
+                    }
+                }
+            } else if (t == CV_PATH) {
+                int M = (int)c.atoms.size(), N = (int)c.params[1];
+                int s0 = (int)gAtoms.size();
+                for (int k = 0; k < M; k++) {
+                    gAtoms.push_back(c.atoms[k]);
+                    gMass.push_back(1.0f);
+                    jAtom[jac0 + 2 * k] = c.atoms[k]; jCv[jac0 + 2 * k] = cv;
+                    jAtom[jac0 + 2 * k + 1] = c.atoms[k]; jCv[jac0 + 2 * k + 1] = cv + 1;
+                }
+                gRef.resize(3 * gAtoms.size(), 0.0f);
+                gEv.resize(3 * gAtoms.size(), 0.0f);
+                // frames appended after all per-atom data: offset in atom units
+                int r0 = (int)(gRef.size() / 3);
+                for (int k = 0; k < 3 * N * M; k++) gRef.push_back((float)c.params[2 + k]);
+                gEv.resize(gRef.size(), 0.0f);
+                // later per-atom slots must stay aligned with gAtoms: pad gAtoms/gMass too
+                while ((int)gAtoms.size() < (int)(gRef.size() / 3)) { gAtoms.push_back(0); gMass.push_back(0.0f); }
+                it.s0 = s0; it.s1 = s0 + M; it.r0 = r0; it.n = N; it.f0 = (float)c.params[0];
+                it.jac0 = jac0;
+            } else if (t == CV_CONTACTMAP) {
+                int np = (int)c.atoms.size() / 2;
+                it.s0 = (int)cmPairs.size();
+                for (int p = 0; p < np; p++) {
+                    cmPairs.push_back(make_int2(c.atoms[2 * p], c.atoms[2 * p + 1]));
+                    cmParams.push_back(make_float4((float)c.params[4 * p], (float)c.params[4 * p + 1],
+                                                   (float)c.params[4 * p + 2], (float)c.params[4 * p + 3]));
+                    jAtom[jac0 + 2 * p] = c.atoms[2 * p]; jCv[jac0 + 2 * p] = cv;
+                    jAtom[jac0 + 2 * p + 1] = c.atoms[2 * p + 1]; jCv[jac0 + 2 * p + 1] = cv;
+                }
+                it.s1 = (int)cmPairs.size();
+                it.jac0 = jac0;
+            }
+            groups.push_back(it);
+        }
+    }
+    // device uploads
+    cvv_.alloc(sizeof(double) * std::max(numCVs_, 1));
+    dudcv_.alloc(sizeof(double) * std::max(numCVs_, 1));
+    jAtom_.upload(jAtom);
+    jCv_.upload(jCv);
+    jx_.alloc(sizeof(float) * std::max(numRows_, 1));
+    jy_.alloc(sizeof(float) * std::max(numRows_, 1));
+    jz_.alloc(sizeof(float) * std::max(numRows_, 1));
+    J_.atom = jAtom_.as<int>(); J_.cv = jCv_.as<int>();
+    J_.gx = jx_.as<float>(); J_.gy = jy_.as<float>(); J_.gz = jz_.as<float>();
+    J_.rows = numRows_;
+    simple_.upload(simple);
+    numSimple_ = (int)simple.size();
+    groupItems_.upload(groups);
+    gAtoms_.upload(gAtoms); gMass_.upload(gMass); gRef_.upload(gRef); gEv_.upload(gEv);
+    cmPairs_.upload(cmPairs); cmParams_.upload(cmParams);
+    G_.items = groupItems_.as<GroupItem>(); G_.numItems = (int)groups.size();
+    G_.atoms = gAtoms_.as<int>(); G_.mass = gMass_.as<float>(); G_.ref = gRef_.as<float>();
+    G_.ev = gEv_.as<float>(); G_.cmPairs = cmPairs_.as<int2>(); G_.cmParams = cmParams_.as<float4>();
+    // coordination tiling
+    if (!coord.empty()) {
+        const int TA = 8 * coordRA_;
+        long long pairs = 0;
+        for (auto& it : coord) pairs += (long long)it.nA * it.nB;
+        long long target = 148LL * 8;
+        long long perCta = std::max<long long>(1, pairs / target);
+        int bSplit = (int)std::min<long long>(1 << 20, std::max<long long>(128, ((perCta / TA + 127) / 128) * 128));
+        C_.bSplit = bSplit;
+        int blocks = 0, pa = 0, pb = 0, cn = 0, rows = 0;
+        std::vector<int> blockItem;
+        for (size_t i = 0; i < coord.size(); i++) {
+            CoordItem& it = coord[i];
+            it.tilesA = std::max(1, (it.nA + TA - 1) / TA);
+            it.splitsB = std::max(1, (it.nB + bSplit - 1) / bSplit);
+            it.block0 = blocks;
+            it.partA = pa; it.partB = pb; it.cn0 = cn;
+            int nb = it.tilesA * it.splitsB;
+            for (int k = 0; k < nb; k++) blockItem.push_back((int)i);
+            blocks += nb; cn += nb;
+            pa += it.splitsB * it.nA; pb += it.tilesA * it.nB;
+            rows += it.nA + it.nB;
+        }
+        coordItems_.upload(coord);
+        coordAtoms_.upload(coordAtoms);
+        coordBlockItem_.upload(blockItem);
+        partA_.alloc(sizeof(float) * 3 * std::max(pa, 1));
+        partB_.alloc(sizeof(float) * 3 * std::max(pb, 1));
+        cnPart_.alloc(sizeof(double) * std::max(cn, 1));
+        C_.items = coordItems_.as<CoordItem>(); C_.numItems = (int)coord.size();
+        C_.atoms = coordAtoms_.as<int>(); C_.blockItem = coordBlockItem_.as<int>();
+        C_.partA = partA_.as<float>(); C_.partB = partB_.as<float>(); C_.cnPart = cnPart_.as<double>();
+        coordBlocks_ = blocks; coordRows_ = rows;
+    }
+}
+
+void Context::setupBiases(const GluedForce& f) {
+    const int nb = f.numBiases();
+    std::map<int, int> typeCount;
+    for (int b = 0; b < nb; b++) {
+        const BiasSpec& s = f.bias(b);
+        if (s.type != BIAS_HARMONIC && s.type != BIAS_METAD && s.type != BIAS_OPES && s.type != BIAS_METAD_HILLS)
+            throw Error(GLUED_E_UNSUPPORTED, "GluedForce bias " + std::to_string(b) + ": type " + std::to_string(s.type) +
+                                                 " is outside this library's hot path (supported: HARMONIC, METAD, "
+                                                 "OPES, METAD_HILLS)");
+        if (s.cvs.empty() || s.cvs.size() > 8)
+            throw Error(GLUED_E_INVALID, "GluedForce bias " + std::to_string(b) + ": needs 1..8 CVs");
+    }
+    biases_.resize(nb);
+    numEnergySlots_ = nb;
+    energies_.alloc(sizeof(double) * std::max(nb, 1));
+    for (int b = 0; b < nb; b++) {
+        HostBias& hb = biases_[b];
+        hb.spec = f.bias(b);
+        hb.index = b;
+        hb.local = typeCount[hb.spec.type]++;
+        BiasDev& d = hb.dev;
+        d = BiasDev{};
+        const std::vector<double>& p = hb.spec.params;
+        const std::vector<int>& ip = hb.spec.iparams;
+        const int D = (int)hb.spec.cvs.size();
+        d.type = hb.spec.type; d.slot = b; d.D = D;
+        for (int k = 0; k < D; k++) d.cvIdx[k] = hb.spec.cvs[k];
+        auto needP = [&](size_t n) {
+            if (p.size() < n) throw Error(GLUED_E_INVALID, "GluedForce bias " + std::to_string(b) + ": expected >= " + std::to_string(n) + " parameters");
+        };
+        auto needI = [&](size_t n) {
+            if (ip.size() < n) throw Error(GLUED_E_INVALID, "GluedForce bias " + std::to_string(b) + ": expected >= " + std::to_string(n) + " integer parameters");
+        };
+        if (d.type == BIAS_HARMONIC) {
+            // params [k_0, s0_0, ...] stored as float (CommonBiasKernels.cpp:115-125)
+            needP(2 * D);
+            for (int k = 0; k < D; k++) { d.hk[k] = (float)p[2 * k]; d.hs0[k] = (float)p[2 * k + 1]; }
+            d.periodicFlag = ip.empty() ? 0 : ip[0];
+        } else if (d.type == BIAS_METAD) {
+            // CommonBiasKernels.cpp:206-257
+            needP(3 + 3 * D); needI(1 + 2 * D);
+            d.h0 = p[0];
+            for (int k = 0; k < D; k++) d.sigma[k] = p[1 + k];
+            double gamma = p[1 + D], kT = p[2 + D];
+            d.gamma = gamma; d.kT = kT;
+            d.pace = ip[0];
+            int total = 1;
+            for (int k = 0; k < D; k++) {
+                double lo = p[3 + D + k], hi = p[3 + 2 * D + k];
+                int bins = ip[1 + k];
+                d.per[k] = ip[1 + D + k];
+                d.origin[k] = lo;
+                d.invSp[k] = bins / (hi - lo);
+                d.npts[k] = bins + (d.per[k] ? 0 : 1);
+                if (bins < 1) throw Error(GLUED_E_INVALID, "METAD: bins must be >= 1");
+            }
+            if (D > 3) throw Error(GLUED_E_INVALID, "METAD grid supports at most 3 CVs (CommonGluedKernels.cpp:3589)");
+            d.strides[0] = 1;
+            for (int k = 1; k < D; k++) d.strides[k] = d.strides[k - 1] * d.npts[k - 1];
+            total = d.strides[D - 1] * d.npts[D - 1];
+            d.total = total;
+            d.hif = gamma <= 1.0 ? 0.0 : 1.0 / ((gamma - 1.0) * kT);
+            hb.grid.alloc(sizeof(double) * total);
+            d.grid = hb.grid.as<double>();
+        } else if (d.type == BIAS_METAD_HILLS) {
+            needP(3 + 3 * D); needI(2 + D);
+            d.h0 = p[0];
+            for (int k = 0; k < D; k++) d.sigma[k] = p[1 + k];
+            double gamma = p[1 + D], kT = p[2 + D];
+            d.gamma = gamma; d.kT = kT;
+            d.pace = ip[0];
+            d.maxHills = ip[1];
+            for (int k = 0; k < D; k++) {
+                d.per[k] = ip[2 + k];
+                d.period[k] = d.per[k] ? (p[3 + 2 * D + k] - p[3 + D + k]) : 0.0;
+            }
+            d.hif = gamma <= 1.0 ? 0.0 : 1.0 / ((gamma - 1.0) * kT);
+            hb.hCenters.alloc(sizeof(double) * std::max(1, d.maxHills * D));
+            hb.hHeights.alloc(sizeof(double) * std::max(1, d.maxHills));
+            hb.ints.alloc(sizeof(int) * 8);
+            d.hCenters = hb.hCenters.as<double>(); d.hHeights = hb.hHeights.as<double>();
+            d.hCount = hb.ints.as<int>();
+        } else {  // OPES (CommonBiasKernels.cpp:489-588)
+            needP(3 + D);
+            double kT = p[0], gamma = p[1];
+            hb.sigma0Host.assign(p.begin() + 2, p.begin() + 2 + D);
+            d.sigmaMin = p[2 + D];
+            d.variant = ip.size() > 0 ? ip[0] : 0;
+            d.pace = ip.size() > 1 ? ip[1] : 500;
+            d.maxKernels = ip.size() > 2 ? ip[2] : 100000;
+            bool adaptive = hb.sigma0Host[0] <= 0.0;
+            d.adaptiveStride = adaptive ? (ip.size() > 3 ? ip[3] : 10 * d.pace) : 0;
+            d.kT = kT; d.gamma = gamma;
+            if (d.variant == 1) {
+                d.invGF = 1.0; d.cutoff2 = 2.0 * gamma; d.eps = 0.0; d.barrier = gamma * kT;
+            } else if (d.variant == 2) {
+                if (!std::isfinite(gamma) || gamma <= 1.0)
+                    throw Error(GLUED_E_INVALID, "OPES_METAD_EXPLORE (variant=2) requires finite gamma > 1");
+                d.invGF = gamma - 1.0; d.cutoff2 = 2.0 * gamma; d.eps = std::exp(-gamma / (gamma - 1.0));
+                d.barrier = gamma * kT;
+                if (!adaptive) for (auto& s : hb.sigma0Host) s *= std::sqrt(gamma);
+            } else {
+                d.invGF = (gamma - 1.0) / gamma;
+                d.cutoff2 = 2.0 * gamma / d.invGF;
+                d.eps = std::exp(-1.0 / (d.invGF * (1.0 - d.invGF)));
+                d.barrier = kT / (1.0 - d.invGF);
+            }
+            if (D > 16) throw Error(GLUED_E_INVALID, "OPES supports at most 16 CVs (CommonGluedKernels.cpp:2638)");
+            size_t K = (size_t)std::max(1, d.maxKernels);
+            hb.centers.alloc(sizeof(double) * K * D);
+            hb.sigmas.alloc(sizeof(double) * K * D);
+            hb.logW.alloc(sizeof(double) * K);
+            {
+                std::vector<double> ones(K * D, 1.0);
+                cudaCheck(cudaMemcpy(hb.sigmas.p, ones.data(), sizeof(double) * K * D, cudaMemcpyHostToDevice), "opes");
+            }
+            hb.ints.alloc(sizeof(int) * 8);   // numKernels, numAllocated, stepCount, nSamples, lastDecision
+            hb.dbls.alloc(sizeof(double) * 8); // sumUprob, sumWeights, sumW[2]
+            hb.mean.alloc(sizeof(double) * D);
+            hb.m2.alloc(sizeof(double) * D);
+            hb.sigma0.upload(hb.sigma0Host);
+            int* I = hb.ints.as<int>();
+            double* Dd = hb.dbls.as<double>();
+            d.centers = hb.centers.as<double>(); d.sigmas = hb.sigmas.as<double>(); d.logW = hb.logW.as<double>();
+            d.numKernels = I; d.numAllocated = I + 1; d.stepCount = I + 2; d.nSamples = I + 3; d.lastDecision = I + 4;
+            d.sumUprob = Dd; d.sumWeights = Dd + 1; d.sumW = Dd + 2;
+            d.runMean = hb.mean.as<double>(); d.runM2 = hb.m2.as<double>(); d.sigma0 = hb.sigma0.as<double>();
+            // sentinels exp(-gamma) (CommonBiasKernels.cpp:547, :599)
+            double init[4] = {0.0, std::exp(-gamma), std::exp(-gamma), std::exp(-2.0 * gamma)};
+            cudaCheck(cudaMemcpy(Dd, init, sizeof init, cudaMemcpyHostToDevice), "opes");
+            int ii[8] = {0, 0, 0, 0, -4, 0, 0, 0};
+            cudaCheck(cudaMemcpy(I, ii, sizeof ii, cudaMemcpyHostToDevice), "opes");
+        }
+    }
+    // evaluation order: stable sort by type rank
+    evalOrder_.resize(nb);
+    for (int b = 0; b < nb; b++) evalOrder_[b] = b;
+    std::stable_sort(evalOrder_.begin(), evalOrder_.end(), [&](int x, int y) {
+        return biasEvalRank(biases_[x].spec.type) < biasEvalRank(biases_[y].spec.type);
+    });
+    std::vector<BiasDev> arr(std::max(nb, 1));
+    for (int k = 0; k < nb; k++) { arr[k] = biases_[evalOrder_[k]].dev; biases_[evalOrder_[k]].depositIndex = k; }
+    biasDev_.upload(arr);
+    mergeFlag_.alloc(sizeof(int) * 4);
+    uprobPartial_.alloc(sizeof(double) * nUprobPartial_);
+}
+
+void Context::syncUploadBias(HostBias& hb) {
+    cudaCheck(cudaMemcpy(biasDev_.as<BiasDev>() + hb.depositIndex, &hb.dev, sizeof(BiasDev),
+                         cudaMemcpyHostToDevice), "bias upload");
+}
+
+// ---------------------------------------------------------------- binding
+void Context::bind(cudaStream_t s, const void* posq, const int* atomIndex, long long* force, int padded) {
+    if (padded < numParticles_) throw Error(GLUED_E_INVALID, "padded_num_atoms < num_particles");
+    stream_ = s;
+    posq_ = static_cast<const float4*>(posq);
+    atomIndex_ = atomIndex;
+    force_buf_ = force;
+    padded_ = padded;
+    bound_ = true;
+    invalidateGraphs();
+    atomsReordered();
+}
+
+void Context::atomsReordered() {
+    requireBound();
+    launchInvertIndex(stream_, atomIndex_, u2g_.as<int>(), numParticles_);
+    cudaCheck(cudaGetLastError(), "invert index");
+}
+
+void Context::requireBound() const {
+    if (!bound_) throw Error(GLUED_E_STATE, "context has no bound device buffers (call glued_context_bind)");
+}
+
+void Context::setBox(const double box[9]) {
+    if (boxSet_ && std::memcmp(box, lastBox_, sizeof lastBox_) == 0) return;
+    std::memcpy(lastBox_, box, sizeof lastBox_);
+    boxSet_ = true;
+    BoxDev b{};
+    for (int i = 0; i < 3; i++) { b.a[i] = (float)box[i]; b.b[i] = (float)box[3 + i]; b.c[i] = (float)box[6 + i]; }
+    b.inv[0] = (float)(1.0 / box[0]); b.inv[1] = (float)(1.0 / box[4]); b.inv[2] = (float)(1.0 / box[8]);
+    bool rect = box[1] == 0 && box[2] == 0 && box[3] == 0 && box[5] == 0 && box[6] == 0 && box[7] == 0;
+    b.kind = periodic_ ? (rect ? 1 : 2) : 0;
+    boxHost_ = b;
+    // The device copy is read by graph-replayed kernels: stage through pinned memory
+    // on the same stream so it is ordered before the next launch.
+    if (bound_) {
+        cudaCheck(cudaStreamSynchronize(stream_), "box sync");
+        *boxPinned_ = b;
+        cudaCheck(cudaMemcpyAsync(box_.p, boxPinned_, sizeof(BoxDev), cudaMemcpyHostToDevice, stream_), "box");
+    } else {
+        cudaCheck(cudaMemcpy(box_.p, &b, sizeof(BoxDev), cudaMemcpyHostToDevice), "box");
+    }
+}
+
+// ---------------------------------------------------------------- execute
+void Context::enqueueExecute(cudaStream_t s, bool includeForces) {
+    const BoxDev* box = box_.as<BoxDev>();
+    double* cvv = cvv_.as<double>();
+    const int* u2g = u2g_.as<int>();
+    launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
+    launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_);
+    launchCoord(s, posq_, u2g, C_, coordBlocks_, coordRows_, boxHost_.kind, coordRA_, box, J_, cvv);
+    launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
+                 testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>());
+    if (includeForces) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
+}
+
+double Context::execute(bool includeForces, bool includeEnergy) {
+    requireBound();
+    if (force_.testForceMode != 0) {
+        launchTestForce(stream_, posq_, atomIndex_, force_buf_, padded_, numParticles_, force_.testForceMode,
+                        force_.testForceScale, box_.as<BoxDev>());
+        cudaCheck(cudaGetLastError(), "test force");
+        return 0.0;
+    }
+    if (numCVs_ == 0) return 0.0;
+    int gi = includeForces ? 1 : 0;
+    if (useGraphs_) {
+        if (!graph_[gi]) {
+            cudaGraph_t g;
+            cudaCheck(cudaStreamBeginCapture(capStream_, cudaStreamCaptureModeThreadLocal), "capture begin");
+            enqueueExecute(capStream_, includeForces);
+            cudaError_t e = cudaStreamEndCapture(capStream_, &g);
+            cudaCheck(e, "capture end");
+            cudaCheck(cudaGraphInstantiate(&graph_[gi], g, 0), "graph instantiate");
+            cudaGraphDestroy(g);
+        }
+        cudaCheck(cudaGraphLaunch(graph_[gi], stream_), "graph launch");
+    } else {
+        enqueueExecute(stream_, includeForces);
+        cudaCheck(cudaGetLastError(), "execute");
+    }
+    cvReady_ = true;
+    double total = 0.0;
+    if (includeEnergy && numEnergySlots_ > 0) {
+        int n = std::min(numEnergySlots_, 64);
+        cudaCheck(cudaMemcpyAsync(energiesPinned_, energies_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_),
+                  "energy download");
+        cudaCheck(cudaStreamSynchronize(stream_), "energy sync");
+        for (int i = 0; i < n; i++) total += energiesPinned_[i];
+        if (numEnergySlots_ > 64) {
+            std::vector<double> rest(numEnergySlots_);
+            cudaCheck(cudaMemcpy(rest.data(), energies_.p, sizeof(double) * numEnergySlots_, cudaMemcpyDeviceToHost), "energy");
+            total = 0.0;
+            for (double e : rest) total += e;
+        }
+    }
+    return total;
+}
+
+// ------------------------------------------------------------ updateState
+void Context::updateState(int step) {
+    // CommonGluedKernels.cpp:5050-5157: deposits use the previous execute()'s
+    // cvValues and bias energies; never before the first execute, once per step,
+    // not at step 0, OPES before MetaD.
+    step_ = step;
+    if (!cvReady_) return;
+    if (step == lastUpdateStep_) return;
+    bool any = false;
+    for (auto& hb : biases_)
+        if (hb.spec.type == BIAS_OPES || hb.spec.type == BIAS_METAD || hb.spec.type == BIAS_METAD_HILLS) any = true;
+    if (!any) return;
+    lastUpdateStep_ = step;
+    requireBound();
+    const double* cvv = cvv_.as<double>();
+    const double* en = energies_.as<double>();
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        if (step == 0 || step % hb.dev.pace != 0) continue;
+        if (hb.numKernelsCPU >= hb.dev.maxKernels) continue;
+        bool will = hb.dev.adaptiveStride == 0 || hb.nSamplesCPU >= hb.dev.adaptiveStride;
+        launchOpesDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en, mergeFlag_.as<int>(),
+                          uprobPartial_.as<double>(), nUprobPartial_);
+        if (will) hb.numKernelsCPU++;
+    }
+    for (auto& hb : biases_) {
+        if (hb.spec.type == BIAS_METAD) {
+            if (step == 0 || step % hb.dev.pace != 0) continue;
+            launchMetadDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en);
+            hb.numDeposited++;
+        }
+    }
+    for (auto& hb : biases_) {
+        if (hb.spec.type == BIAS_METAD_HILLS) {
+            if (step == 0 || step % hb.dev.pace != 0) continue;
+            launchHillsDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en);
+        }
+    }
+    cudaCheck(cudaGetLastError(), "updateState");
+}
+
+// ---------------------------------------------------------------- reads
+std::vector<double> Context::cvValues() {
+    if (numCVs_ == 0) return {};
+    std::vector<double> v(numCVs_);
+    if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    cudaCheck(cudaMemcpy(v.data(), cvv_.p, sizeof(double) * numCVs_, cudaMemcpyDeviceToHost), "cv download");
+    return v;
+}
+
+double Context::lastBias() {
+    if (numEnergySlots_ == 0) return 0.0;
+    std::vector<double> e(numEnergySlots_);
+    if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    cudaCheck(cudaMemcpy(e.data(), energies_.p, sizeof(double) * numEnergySlots_, cudaMemcpyDeviceToHost), "bias");
+    double t = 0;
+    for (double x : e) t += x;
+    return t;
+}
+
+// Multiwalker sharing: raw device pointers of a bias's shared arrays.
+std::vector<long long> Context::multiWalkerPtrs(int biasIndex) {
+    if (biasIndex < 0 || biasIndex >= (int)biases_.size()) throw Error(GLUED_E_INVALID, "GluedForce: bias index out of range");
+    HostBias& hb = biases_[biasIndex];
+    if (hb.spec.type == BIAS_METAD) return {(long long)(uintptr_t)hb.dev.grid};
+    if (hb.spec.type == BIAS_OPES)
+        return {(long long)(uintptr_t)hb.dev.centers, (long long)(uintptr_t)hb.dev.sigmas,
+                (long long)(uintptr_t)hb.dev.logW, (long long)(uintptr_t)hb.dev.numKernels,
+                (long long)(uintptr_t)hb.dev.numAllocated};
+    return {};
+}
+
+void Context::setMultiWalkerPtrs(int biasIndex, const std::vector<long long>& ptrs) {
+    if (biasIndex < 0 || biasIndex >= (int)biases_.size()) throw Error(GLUED_E_INVALID, "GluedForce: bias index out of range");
+    HostBias& hb = biases_[biasIndex];
+    if (hb.spec.type == BIAS_METAD) {
+        if (ptrs.size() < 1) throw Error(GLUED_E_INVALID, "METAD multiwalker pointers: expected [grid]");
+        hb.dev.grid = reinterpret_cast<double*>((uintptr_t)ptrs[0]);
+    } else if (hb.spec.type == BIAS_OPES) {
+        if (ptrs.size() < 5) throw Error(GLUED_E_INVALID, "OPES multiwalker pointers: expected 5");
+        hb.dev.centers = reinterpret_cast<double*>((uintptr_t)ptrs[0]);
+        hb.dev.sigmas = reinterpret_cast<double*>((uintptr_t)ptrs[1]);
+        hb.dev.logW = reinterpret_cast<double*>((uintptr_t)ptrs[2]);
+        hb.dev.numKernels = reinterpret_cast<int*>((uintptr_t)ptrs[3]);
+        hb.dev.numAllocated = reinterpret_cast<int*>((uintptr_t)ptrs[4]);
+    } else {
+        return;
+    }
+    if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    syncUploadBias(hb);
+}
+
+int Context::opesLastDecision(int opesIndex) {
+    int k = 0;
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        if (k++ != opesIndex) continue;
+        int v = 0;
+        if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+        cudaCheck(cudaMemcpy(&v, hb.dev.lastDecision, sizeof(int), cudaMemcpyDeviceToHost), "decision");
+        return v;
+    }
+    throw Error(GLUED_E_INVALID, "opes index out of range");
+}
+
+std::vector<double> Context::opesMetrics(int opesIndex) {
+    // CommonGluedKernels.cpp:5164-5210
+    int k = 0;
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        if (k++ != opesIndex) continue;
+        if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+        double dd[4];
+        int ii[4];
+        cudaCheck(cudaMemcpy(dd, hb.dev.sumUprob, sizeof(double) * 4, cudaMemcpyDeviceToHost), "metrics");
+        cudaCheck(cudaMemcpy(ii, hb.dev.numKernels, sizeof(int) * 4, cudaMemcpyDeviceToHost), "metrics");
+        int nker;
+        cudaCheck(cudaMemcpy(&nker, hb.dev.numKernels, sizeof(int), cudaMemcpyDeviceToHost), "metrics");
+        double sumUp = hb.numKernelsCPU > 0 ? dd[0] : 0.0;
+        double counter = (double)ii[2];
+        double KDEnorm = hb.dev.variant == 2 ? counter : dd[1];
+        double zed = (nker > 0 && KDEnorm > 0.0) ? sumUp / (KDEnorm * (double)nker) : 1.0;
+        double rct = (counter > 0.0 && dd[1] > 0.0) ? hb.dev.kT * std::log(dd[1] / counter) : 0.0;
+        double neff = (1.0 + dd[2]) * (1.0 + dd[2]) / (1.0 + dd[3]);
+        return {zed, rct, (double)nker, neff};
+    }
+    throw Error(GLUED_E_INVALID, "getOPESMetrics: biasIndex out of range");
+}
+
+std::vector<float> Context::kernelSigmas(int opesIndex) {
+    int k = 0;
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        if (k++ != opesIndex) continue;
+        if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+        int nk = 0;
+        cudaCheck(cudaMemcpy(&nk, hb.dev.numKernels, sizeof(int), cudaMemcpyDeviceToHost), "sigmas");
+        if (nk <= 0) return {};
+        std::vector<double> s((size_t)nk * hb.dev.D);
+        cudaCheck(cudaMemcpy(s.data(), hb.dev.sigmas, sizeof(double) * s.size(), cudaMemcpyDeviceToHost), "sigmas");
+        return std::vector<float>(s.begin(), s.end());
+    }
+    return {};
+}
+
+// ------------------------------------------------------- bias-state blob
+// 'GPUS' v1 layout of platforms/common/src/CommonSerialization.cpp:20-177. Only
+// OPES and METAD carry state in this library; the counts of the other reference
+// sections are written as 0 so a reference reader accepts the blob. State of the
+// hill-sum extension follows the reference sections under its own 'HILL' tag,
+// which a reference reader ignores (it stops after its last section).
+std::vector<char> Context::getBiasState() {
+    if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    std::vector<char> buf;
+    auto w = [&](const void* src, size_t n) { const char* p = (const char*)src; buf.insert(buf.end(), p, p + n); };
+    auto w32 = [&](int32_t v) { w(&v, 4); };
+    const char magic[4] = {'G', 'P', 'U', 'S'};
+    w(magic, 4);
+    w32(1);
+    int nOpes = 0, nMetad = 0, nHills = 0;
+    for (auto& hb : biases_) {
+        nOpes += hb.spec.type == BIAS_OPES;
+        nMetad += hb.spec.type == BIAS_METAD;
+        nHills += hb.spec.type == BIAS_METAD_HILLS;
+    }
+    w32(nOpes);
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        const int D = hb.dev.D;
+        int ii[4];
+        double dd[1];
+        cudaCheck(cudaMemcpy(ii, hb.dev.numKernels, sizeof ii, cudaMemcpyDeviceToHost), "blob");
+        cudaCheck(cudaMemcpy(dd, hb.dev.sumUprob, sizeof dd, cudaMemcpyDeviceToHost), "blob");
+        int nk = ii[0];
+        hb.numKernelsCPU = nk;
+        std::vector<double> mean(D), m2(D), c((size_t)nk * D), s((size_t)nk * D), lw(nk);
+        cudaCheck(cudaMemcpy(mean.data(), hb.dev.runMean, 8 * D, cudaMemcpyDeviceToHost), "blob");
+        cudaCheck(cudaMemcpy(m2.data(), hb.dev.runM2, 8 * D, cudaMemcpyDeviceToHost), "blob");
+        if (nk > 0) {
+            cudaCheck(cudaMemcpy(c.data(), hb.dev.centers, 8 * c.size(), cudaMemcpyDeviceToHost), "blob");
+            cudaCheck(cudaMemcpy(s.data(), hb.dev.sigmas, 8 * s.size(), cudaMemcpyDeviceToHost), "blob");
+            cudaCheck(cudaMemcpy(lw.data(), hb.dev.logW, 8 * lw.size(), cudaMemcpyDeviceToHost), "blob");
+        }
+        w32(nk);
+        w(dd, 8);
+        w32(ii[3]);  // nSamples
+        w(mean.data(), 8 * D);
+        w(m2.data(), 8 * D);
+        w(c.data(), 8 * c.size());
+        w(s.data(), 8 * s.size());
+        w(lw.data(), 8 * lw.size());
+    }
+    w32(0);  // ABMD
+    w32(nMetad);
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_METAD) continue;
+        std::vector<double> g(hb.dev.total);
+        cudaCheck(cudaMemcpy(g.data(), hb.dev.grid, 8 * g.size(), cudaMemcpyDeviceToHost), "blob");
+        w32(hb.numDeposited);
+        w(g.data(), 8 * g.size());
+    }
+    for (int k = 0; k < 9; k++) w32(0);  // PBMETAD, EXTERNAL, LINEAR, WALL, OPES_EXPANDED, EXTLAG, EDS, MAXENT, MULTITHERMAL
+    if (nHills > 0) {
+        const char tag[4] = {'H', 'I', 'L', 'L'};
+        w(tag, 4);
+        w32(nHills);
+        for (auto& hb : biases_) {
+            if (hb.spec.type != BIAS_METAD_HILLS) continue;
+            int n = 0;
+            cudaCheck(cudaMemcpy(&n, hb.dev.hCount, sizeof(int), cudaMemcpyDeviceToHost), "blob");
+            std::vector<double> c((size_t)n * hb.dev.D), h(n);
+            if (n > 0) {
+                cudaCheck(cudaMemcpy(c.data(), hb.dev.hCenters, 8 * c.size(), cudaMemcpyDeviceToHost), "blob");
+                cudaCheck(cudaMemcpy(h.data(), hb.dev.hHeights, 8 * h.size(), cudaMemcpyDeviceToHost), "blob");
+            }
+            w32(n);
+            w(c.data(), 8 * c.size());
+            w(h.data(), 8 * h.size());
+        }
+    }
+    return buf;
+}
+
+void Context::setBiasState(const std::vector<char>& bytes) {
+    // CommonSerialization.cpp:180-411: bounds-checked reader, optional header,
+    // count checks per section. Deviation: numAllocated is set to the restored
+    // kernel count (the reference leaves it at its previous value, so the next
+    // append after a restore into a fresh context would claim slot 0).
+    if (bytes.empty()) return;
+    if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    const char* p = bytes.data();
+    const char* const end = p + bytes.size();
+    auto rd = [&](void* dst, size_t n) {
+        if ((size_t)(end - p) < n) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: truncated/corrupt blob");
+        std::memcpy(dst, p, n);
+        p += n;
+    };
+    auto more = [&]() { return p < end; };
+    if ((size_t)(end - p) >= 8 && std::memcmp(p, "GPUS", 4) == 0) {
+        p += 4;
+        int32_t ver;
+        rd(&ver, 4);
+        if (ver != 1) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: unknown blob version");
+    }
+    int nOpes = 0, nMetad = 0;
+    for (auto& hb : biases_) { nOpes += hb.spec.type == BIAS_OPES; nMetad += hb.spec.type == BIAS_METAD; }
+    int32_t nb;
+    rd(&nb, 4);
+    if (nb != nOpes)
+        throw Error(GLUED_E_CORRUPT, "GLUED bias-state: OPES bias count mismatch (expected " + std::to_string(nOpes) +
+                                         ", got " + std::to_string((long long)nb) + ")");
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_OPES) continue;
+        const size_t D = hb.dev.D;
+        int32_t nk, ns;
+        double logZ;
+        rd(&nk, 4); rd(&logZ, 8); rd(&ns, 4);
+        if (nk < 0 || nk > hb.dev.maxKernels) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: OPES kernel count out of range");
+        size_t need = D * 16 + (size_t)nk * D * 16 + (size_t)nk * 8;
+        if ((size_t)(end - p) < need) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: truncated/corrupt blob");
+        std::vector<double> mean(D), m2(D), c((size_t)nk * D), s((size_t)nk * D), lw(nk);
+        rd(mean.data(), 8 * D); rd(m2.data(), 8 * D);
+        rd(c.data(), 8 * c.size()); rd(s.data(), 8 * s.size()); rd(lw.data(), 8 * lw.size());
+        if (nk > 0) {
+            cudaCheck(cudaMemcpy(hb.dev.centers, c.data(), 8 * c.size(), cudaMemcpyHostToDevice), "restore");
+            cudaCheck(cudaMemcpy(hb.dev.sigmas, s.data(), 8 * s.size(), cudaMemcpyHostToDevice), "restore");
+            cudaCheck(cudaMemcpy(hb.dev.logW, lw.data(), 8 * lw.size(), cudaMemcpyHostToDevice), "restore");
+        }
+        cudaCheck(cudaMemcpy(hb.dev.runMean, mean.data(), 8 * D, cudaMemcpyHostToDevice), "restore");
+        cudaCheck(cudaMemcpy(hb.dev.runM2, m2.data(), 8 * D, cudaMemcpyHostToDevice), "restore");
+        int counts[2] = {nk, nk};
+        cudaCheck(cudaMemcpy(hb.dev.numKernels, counts, sizeof counts, cudaMemcpyHostToDevice), "restore");
+        cudaCheck(cudaMemcpy(hb.dev.nSamples, &ns, 4, cudaMemcpyHostToDevice), "restore");
+        cudaCheck(cudaMemcpy(hb.dev.sumUprob, &logZ, 8, cudaMemcpyHostToDevice), "restore");
+        // KDNorm = exp(-gamma) + sum exp(logW) (CommonSerialization.cpp:259-265)
+        double sumW = std::exp(-hb.dev.gamma);
+        for (int k = 0; k < nk; k++) sumW += std::exp(lw[k]);
+        cudaCheck(cudaMemcpy(hb.dev.sumWeights, &sumW, 8, cudaMemcpyHostToDevice), "restore");
+        hb.numKernelsCPU = nk;
+        hb.nSamplesCPU = ns;
+    }
+    if (more()) {
+        int32_t na;
+        rd(&na, 4);
+        if (na != 0) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: ABMD bias count mismatch (expected 0, got " + std::to_string((long long)na) + ")");
+    }
+    if (more()) {
+        int32_t nm;
+        rd(&nm, 4);
+        if (nm != nMetad)
+            throw Error(GLUED_E_CORRUPT, "GLUED bias-state: MetaD bias count mismatch (expected " + std::to_string(nMetad) +
+                                             ", got " + std::to_string((long long)nm) + ")");
+        for (auto& hb : biases_) {
+            if (hb.spec.type != BIAS_METAD) continue;
+            int32_t nd;
+            rd(&nd, 4);
+            std::vector<double> g(hb.dev.total);
+            rd(g.data(), 8 * g.size());
+            hb.numDeposited = nd;
+            cudaCheck(cudaMemcpy(hb.dev.grid, g.data(), 8 * g.size(), cudaMemcpyHostToDevice), "restore");
+        }
+    }
+    // Remaining reference sections: counts must be zero for this library's biases.
+    const char* names[9] = {"PBMetaD", "external", "linear", "wall", "OPES_EXPANDED", "extended-Lagrangian", "EDS", "MaxEnt", "OPES multithermal"};
+    for (int k = 0; k < 9 && more(); k++) {
+        if ((size_t)(end - p) >= 4 && std::memcmp(p, "HILL", 4) == 0) break;
+        int32_t n;
+        rd(&n, 4);
+        if (n != 0 && k != 1 && k != 2 && k != 3)
+            throw Error(GLUED_E_CORRUPT, std::string("GLUED bias-state: ") + names[k] + " bias count mismatch (expected 0, got " + std::to_string((long long)n) + ")");
+    }
+    if ((size_t)(end - p) >= 8 && std::memcmp(p, "HILL", 4) == 0) {
+        p += 4;
+        int32_t nh;
+        rd(&nh, 4);
+        int expect = 0;
+        for (auto& hb : biases_) expect += hb.spec.type == BIAS_METAD_HILLS;
+        if (nh != expect) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: hill-sum bias count mismatch");
+        for (auto& hb : biases_) {
+            if (hb.spec.type != BIAS_METAD_HILLS) continue;
+            int32_t n;
+            rd(&n, 4);
+            if (n < 0 || n > hb.dev.maxHills) throw Error(GLUED_E_CORRUPT, "GLUED bias-state: hill count out of range");
+            std::vector<double> c((size_t)n * hb.dev.D), h(n);
+            rd(c.data(), 8 * c.size()); rd(h.data(), 8 * h.size());
+            if (n > 0) {
+                cudaCheck(cudaMemcpy(hb.dev.hCenters, c.data(), 8 * c.size(), cudaMemcpyHostToDevice), "restore");
+                cudaCheck(cudaMemcpy(hb.dev.hHeights, h.data(), 8 * h.size(), cudaMemcpyHostToDevice), "restore");
+            }
+            cudaCheck(cudaMemcpy(hb.dev.hCount, &n, 4, cudaMemcpyHostToDevice), "restore");
+        }
+    }
+}
+
+}  // namespace glued

@@ -1,0 +1,136 @@
+// Device-side data layout of one context, shared by the host plan builder and the
+// kernels. All atom indices held on the device are USER atom indices; kernels map
+// them to OpenMM GPU slots through u2g (user -> slot), rebuilt on the device when
+// OpenMM reorders atoms. All pointers are device pointers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace glued {
+
+// Periodic box, reduced triclinic form (OpenMM): a = (ax,0,0), b = (bx,by,0),
+// c = (cx,cy,cz). kind 0: no PBC; 1: rectangular; 2: triclinic.
+struct BoxDev {
+    float inv[3];
+    float a[3], b[3], c[3];
+    int kind;
+    int pad[2];
+};
+
+// Jacobian table rows (the reference's SoA, CommonGluedKernels.h:95-100).
+struct JacDev {
+    int* atom;   // user atom
+    float* gx;
+    float* gy;
+    float* gz;
+    int* cv;
+    int rows;
+};
+
+// Simple geometric CVs, one thread each: distance (2 atoms), angle (3), dihedral (4).
+struct SimpleItem {
+    int type;
+    int cv;
+    int jac0;
+    int atoms[4];
+};
+
+// CVs reduced by one CTA each. Field use per type:
+//   COM distance : s0=g1Start s1=g2Start s2=g2End (into gAtoms/gMass), f0=M1 f1=M2
+//   gyration     : s0=start s1=end, f0=M
+//   RMSD / Kabsch: s0=start s1=end (gRef indexed 3*(row))
+//   PCA          : s0=start s1=end (gRef, gEv)
+//   path         : s0=start s1=end, r0=frame offset (atoms) into gRef, n=frames, f0=lambda
+//   contact map  : s0=pair start s1=pair end (into cmPairs/cmParams)
+struct GroupItem {
+    int type;
+    int cv;
+    int jac0;
+    int s0, s1, s2;
+    int r0;
+    int n;
+    float f0, f1;
+};
+
+struct GroupDev {
+    const GroupItem* items;
+    int numItems;
+    const int* atoms;
+    const float* mass;
+    const float* ref;      // xyz per atom (RMSD/PCA/Kabsch) or per frame-atom (path)
+    const float* ev;       // PCA eigenvectors, xyz per atom
+    const int2* cmPairs;
+    const float4* cmParams;  // r0, n, m, w
+};
+
+// Coordination CVs: all-pairs tiles with deterministic partial sums.
+struct CoordItem {
+    int cv;
+    int jac0;       // first Jacobian row (A atoms, then B atoms)
+    int a0, nA;     // into coordAtoms
+    int b0, nB;
+    float r0, n, m;
+    float rc2;      // squared cutoff, 0 = none (reference semantics)
+    int kind;       // switch kind: 0 general (reference formula), k>0: m == 2n, n == 2k
+    int tilesA;     // number of A tiles
+    int splitsB;    // number of B splits
+    int block0;     // first CTA of this item in the pair launch
+    int partA;      // offset (float3 units) of this item's A partials: [splitsB][nA]
+    int partB;      // offset of B partials: [tilesA][nB]
+    int cn0;        // offset of this item's per-CTA CN partials
+};
+
+struct CoordDev {
+    const CoordItem* items;
+    int numItems;
+    const int* atoms;
+    const int* blockItem;  // CTA -> item
+    float* partA;          // float3 as 3 floats
+    float* partB;
+    double* cnPart;
+    int bSplit;            // B atoms per split (multiple of the B chunk)
+};
+
+// Bias records, evaluated in the reference's bias-type order.
+struct BiasDev {
+    int type;
+    int slot;       // biasEnergies slot (addBias order)
+    int D;
+    int cvIdx[8];
+    int periodicFlag;       // harmonic periodic wrap
+    // harmonic: k, s0 per dim (float, as the reference stores them)
+    float hk[8], hs0[8];
+    // MetaD grid / hills
+    double h0, hif;         // initial height, 1/((gamma-1) kT) or 0
+    double sigma[8];
+    double origin[8], invSp[8], period[8];
+    int npts[8], strides[8], per[8];
+    double* grid;
+    int total;
+    int pace;
+    // hills table (METAD_HILLS): centers [maxH][D], heights [maxH]
+    double* hCenters;
+    double* hHeights;
+    int* hCount;
+    int maxHills;
+    // OPES
+    double* centers;        // [maxK][D]
+    double* sigmas;         // [maxK][D]
+    double* logW;           // [maxK]
+    int* numKernels;
+    int* numAllocated;
+    double* sumUprob;       // "logZ" buffer of the reference (linear sum_uprob)
+    double* sumWeights;     // KDNorm
+    double* sumW;           // {sum_w, sum_w2}
+    int* stepCount;
+    int* nSamples;
+    double* runMean;
+    double* runM2;
+    double* sigma0;
+    int* lastDecision;
+    double invGF, kT, cutoff2, eps, barrier, sigmaMin, gamma;
+    int variant, adaptiveStride, maxKernels;
+};
+
+}  // namespace glued

@@ -1,0 +1,27 @@
+// Host-callable launchers of the device kernels (plain C++ signatures).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "dev.hpp"
+
+namespace glued {
+
+void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n);
+void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
+                     const BoxDev* box, double* cvv, const JacDev& J);
+void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
+                    double* cvv, const JacDev& J);
+void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
+                     int numAtoms, int mode, double scale, const BoxDev* box);
+void launchCoord(cudaStream_t s, const float4* posq, const int* u2g, const CoordDev& C, int numBlocks,
+                 int totalRows, int boxKind, int ra, const BoxDev* box, const JacDev& J, double* cvv);
+void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
+                  const double* testGrad, double* dUdCV, double* energies);
+void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
+                   int padded);
+void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
+void launchHillsDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
+void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies,
+                       int* mergeFlag, double* partial, int nPartial);
+
+}  // namespace glued

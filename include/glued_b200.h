@@ -1,0 +1,193 @@
+/*
+ * glued_b200.h — C ABI of the B200-native GLUED hot path.
+ *
+ * The library replaces the device side of GLUED's CalcGluedForceKernel (CV
+ * evaluation -> MetaD/OPES bias -> chain-rule force scatter into OpenMM's 2^32
+ * fixed-point force buffer) with hand-written sm_100a CUDA kernels, behind the
+ * same descriptor (GluedForce) and kernel (CalcGluedForceKernel) interfaces.
+ * Reference citations are relative to the GLUED source tree.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative GLUED_E_* code; the
+ *     message of the last failure on the calling thread is glued_last_error().
+ *     No C++ exception crosses this boundary (the reference throws
+ *     OpenMMException for the same conditions: openmmapi/src/GluedForce.cpp:48-99,
+ *     platforms/common/src/CommonGluedKernels.cpp:3886-3927,
+ *     platforms/common/src/CommonSerialization.cpp:187-236).
+ *   - Caller owns every host buffer and the bound device buffers (posq, atom
+ *     index, force buffer). Handles own their device state.
+ *   - Device work is enqueued on the bound stream; only the calls documented as
+ *     "synchronizing" wait for the device.
+ *   - Positions: OpenMM posq layout, float4 per GPU slot (x, y, z, charge), in nm.
+ *     Force buffer: int64[3 * padded_num_atoms], field-major, value * 2^32,
+ *     accumulated with += (OpenMM's long force buffer).
+ */
+#ifndef GLUED_B200_H
+#define GLUED_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GLUED_OK 0
+#define GLUED_E_INVALID (-1)    /* bad argument / spec validation failure */
+#define GLUED_E_CUDA (-2)       /* CUDA runtime error */
+#define GLUED_E_STATE (-3)      /* call not valid in the current state */
+#define GLUED_E_CORRUPT (-4)    /* corrupt / mismatched bias-state blob */
+#define GLUED_E_UNSUPPORTED (-5)/* CV or bias type outside this build's scope */
+#define GLUED_E_TIMEOUT (-6)    /* a bounded device wait gave up */
+
+typedef struct glued_force glued_force;     /* GluedForce descriptor */
+typedef struct glued_context glued_context; /* per-Context kernel state */
+typedef struct glued_batch glued_batch;     /* many walkers, one launch per step */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* glued_last_error(void);
+/* Library version string. */
+const char* glued_version(void);
+
+/* ------------------------------------------------------------------ descriptor
+ * GluedForce (openmmapi/include/GluedForce.h:113-239,
+ * openmmapi/src/GluedForce.cpp:11-133). Type codes are the reference's
+ * CVType/BiasType enums (GluedForce.h:27-95).                                  */
+int glued_force_create(glued_force** out);
+int glued_force_copy(const glued_force* src, glued_force** out);      /* GluedForce.cpp:16-26 */
+int glued_force_destroy(glued_force* f);
+/* addCollectiveVariable (GluedForce.cpp:44-61): *out_index = first CV value slot. */
+int glued_force_add_cv(glued_force* f, int type, const int* atoms, int n_atoms,
+                       const double* params, int n_params, int* out_index);
+/* addBias (GluedForce.cpp:81-105): rejects CV indices outside [0, numCVValues). */
+int glued_force_add_bias(glued_force* f, int type, const int* cv_indices, int n_cvs,
+                         const double* params, int n_params, const int* int_params,
+                         int n_int_params, int* out_index);
+/* addExpressionCV / addPyTorchCV (GluedForce.cpp:164-203): stored and serialized;
+ * a context built from a force holding them reports GLUED_E_UNSUPPORTED.       */
+int glued_force_add_expression_cv(glued_force* f, const char* expression, const int* inputs,
+                                  int n_inputs, int* out_index);
+int glued_force_add_pytorch_cv(glued_force* f, const char* model_path, const int* atoms,
+                               int n_atoms, const double* params, int n_params, int* out_index);
+int glued_force_num_cv_values(const glued_force* f, int* out);        /* getNumCollectiveVariables */
+int glued_force_num_cv_specs(const glued_force* f, int* out);         /* getNumCollectiveVariableSpecs */
+int glued_force_num_biases(const glued_force* f, int* out);
+/* getCollectiveVariableInfo (GluedForce.cpp:67-76). Two-call protocol: pass
+ * NULL buffers to read the sizes into *n_atoms / *n_params.                     */
+int glued_force_get_cv(const glued_force* f, int idx, int* type, int* atoms, int* n_atoms,
+                       double* params, int* n_params);
+/* getExpressionCVInfo / getPyTorchCVModelPath: *len in/out, bytes incl. NUL.   */
+int glued_force_get_cv_string(const glued_force* f, int idx, char* buf, size_t* len);
+/* getBiasInfo (GluedForce.cpp:111-121), same two-call protocol.                 */
+int glued_force_get_bias(const glued_force* f, int idx, int* type, int* cvs, int* n_cvs,
+                         double* params, int* n_params, int* int_params, int* n_int_params);
+int glued_force_set_temperature(glued_force* f, double kelvin);
+int glued_force_get_temperature(const glued_force* f, double* kelvin);
+int glued_force_set_pbc(glued_force* f, int yes);
+int glued_force_get_pbc(const glued_force* f, int* yes);
+int glued_force_set_force_group(glued_force* f, int group);
+int glued_force_get_force_group(const glued_force* f, int* group);
+/* Test-only hooks (GluedForce.h:181-193): constant/per-atom/PBC test forces and
+ * injected dU/dCV that bypass the bias kernels.                                 */
+int glued_force_set_test_force(glued_force* f, int mode, double scale);
+int glued_force_get_test_force(const glued_force* f, int* mode, double* scale);
+int glued_force_set_test_bias_gradients(glued_force* f, const double* g, int n);
+int glued_force_get_test_bias_gradients(const glued_force* f, double* g, int* n);
+/* XML in OpenMM's XmlSerializer layout for GluedForceProxy
+ * (serialization/src/GluedForceProxy.cpp:15-138). *len in/out incl. NUL.       */
+int glued_force_serialize_xml(const glued_force* f, char* buf, size_t* len);
+int glued_force_deserialize_xml(const char* xml, glued_force** out);
+
+/* --------------------------------------------------------------------- context
+ * CalcGluedForceKernel (openmmapi/include/GluedKernels.h:23-105) as implemented
+ * by CommonCalcGluedForceKernel (platforms/common/src/CommonGluedKernels.cpp:
+ * 4608-5288). One context per OpenMM Context on one GPU.                       */
+/* initialize(System, GluedForce) (CommonGluedKernels.cpp:4608-4644): validates the
+ * specs, flattens them and allocates device state on the current device.
+ * masses: double[num_particles] (System::getParticleMass), may be NULL = 1.0.   */
+int glued_context_create(const glued_force* f, int num_particles, const double* masses,
+                         glued_context** out);
+int glued_context_destroy(glued_context* c);
+/* Bind OpenMM's device buffers (ComputeContext::getPosq / getAtomIndexArray /
+ * getLongForceBuffer / getPaddedNumAtoms) and the stream to enqueue on.
+ * atom_index: int[num_particles], GPU slot -> user atom; NULL = identity.       */
+int glued_context_bind(glued_context* c, void* stream, const void* posq, const int* atom_index,
+                       long long* force_buffer, int padded_num_atoms);
+/* OpenMM reordered atoms (ComputeContext::getAtomsWereReordered): rebuild the
+ * user -> GPU slot map on the device (CommonCVKernels.cpp:113-320).             */
+int glued_context_atoms_reordered(glued_context* c);
+/* Periodic box vectors a, b, c (reduced form, nm), row-major double[9].        */
+int glued_context_set_box(glued_context* c, const double box[9]);
+/* Current step count, for callers that evaluate outside updateState.           */
+int glued_context_set_step(glued_context* c, long long step);
+/* execute(ContextImpl&, includeForces, includeEnergy) (CommonGluedKernels.cpp:
+ * 4646-5048). With include_energy, synchronizing; *energy_out = total bias.     */
+int glued_context_execute(glued_context* c, int include_forces, int include_energy,
+                          double* energy_out);
+/* updateState(ContextImpl&, step) (CommonGluedKernels.cpp:5050-5157): pace-gated
+ * deposition from the previous execute()'s CVs; once per step.                  */
+int glued_context_update_state(glued_context* c, int step);
+/* downloadCVValues / getCurrentCVs (CommonGluedKernels.cpp:5264-5271); synchronizing. */
+int glued_context_get_cv_values(glued_context* c, double* out, int n);
+/* downloadLastBias (CommonGluedKernels.cpp:5273-5287); synchronizing.           */
+int glued_context_get_last_bias(glued_context* c, double* out);
+/* getBiasStateBytes / setBiasStateBytes: 'GPUS' v1 blob
+ * (platforms/common/src/CommonSerialization.cpp:20-411). *len in/out.          */
+int glued_context_get_bias_state(glued_context* c, char* buf, size_t* len);
+int glued_context_set_bias_state(glued_context* c, const char* buf, size_t len);
+/* getOPESMetrics (CommonGluedKernels.cpp:5164-5210): out = [zed, rct, nker, neff]. */
+int glued_context_opes_metrics(glued_context* c, int opes_index, double out[4]);
+/* getKernelSigmas (CommonGluedKernels.cpp:5212-5232); *n in/out floats.         */
+int glued_context_kernel_sigmas(glued_context* c, int opes_index, float* out, int* n);
+/* getMultiWalkerPtrs / redirectToPrimaryBias (platforms/cuda/src/
+ * CudaGluedKernelFactory.cpp:30-46, CommonGluedKernels.cpp:5234-5262). bias_index
+ * is the global addBias index. METAD: [grid]; OPES: [centers, sigmas, logW,
+ * numKernels, numAllocated]. *n in/out.                                         */
+int glued_context_multiwalker_ptrs(glued_context* c, int bias_index, long long* out, int* n);
+int glued_context_set_multiwalker_ptrs(glued_context* c, int bias_index, const long long* ptrs, int n);
+/* Device pointers of the per-step outputs (for zero-copy consumers such as the
+ * autograd path): cvValues double[numCV], cvBiasGradients double[numCV],
+ * Jacobian rows (atom int, gx/gy/gz float, cv int)[num_rows].                   */
+int glued_context_device_arrays(glued_context* c, void** cv_values, void** dudcv, void** jac_atom,
+                                void** jac_gx, void** jac_gy, void** jac_gz, void** jac_cv,
+                                int* num_cvs, int* num_rows);
+/* Test hook: index of the last OPES deposit decision of OPES bias opes_index
+ * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
+int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);
+
+/* ----------------------------------------------------------------------- batch
+ * Many walkers on one GPU evaluated by one persistent launch per step (no
+ * reference counterpart as a kernel: it replaces the reference's one-Context-
+ * per-walker stepping, tests/test_multiwalker.py:156-158, and its shared-bias
+ * pointer aliasing, CommonGluedKernels.cpp:5234-5262).                          */
+typedef struct glued_walker_desc {
+    const void* posq;          /* float4[num_atoms] device */
+    long long* force_buffer;   /* int64[3 * padded] device */
+    int num_atoms;
+    int padded_num_atoms;
+    double box[9];
+} glued_walker_desc;
+
+/* All walkers share one force descriptor (same CV/bias specs, user atom indices
+ * valid for every walker) and one hill table for their METAD_HILLS bias.        */
+int glued_batch_create(const glued_force* f, int num_walkers, const glued_walker_desc* walkers,
+                       const double* masses, glued_batch** out);
+int glued_batch_destroy(glued_batch* b);
+int glued_batch_set_stream(glued_batch* b, void* stream);
+/* Tile choice for the pair kernels; 0 = autotuned. Synchronizing when tuning.   */
+int glued_batch_autotune(glued_batch* b, int* chosen_tile);
+/* One step for all walkers: CVs, bias, scatter (one launch, graph-replayed). */
+int glued_batch_execute(glued_batch* b);
+int glued_batch_update_state(glued_batch* b, int step);
+/* energies: double[num_walkers]; cv_values: double[num_walkers * numCV].        */
+int glued_batch_get_energies(glued_batch* b, double* energies);
+int glued_batch_get_cv_values(glued_batch* b, double* cv_values);
+/* Hill table of the shared METAD_HILLS bias: read count / centres / heights.     */
+int glued_batch_num_hills(glued_batch* b, int* n);
+int glued_batch_set_hills(glued_batch* b, const double* centers, const double* heights, int n);
+/* Status word of the persistent kernel's bounded grid barrier (0 = ok).         */
+int glued_batch_status(glued_batch* b, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLUED_B200_H */
