@@ -1,0 +1,489 @@
+"""Benchmark of the per-step CV -> bias -> force-scatter path on B200.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--config c4|c2|c1|c3] [--impl ours|reference]
+
+A step is one pass of the hot path over one batch of synthetic input:
+updateState(step) (pace-gated deposition) followed by execute(forces) for every
+walker of the configuration. Inputs stay resident in HBM for `value`; `e2e`
+repeats the measurement through the C ABI with host buffers (pinned host ->
+device positions before, device -> host forces and energies after, every step).
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on
+the launching stream with a 256 MB L2 flush between steps (outside the events);
+device time summed over steps, max over ranks. nvidia-smi clocks are sampled
+during the timed region. Under torchrun each rank runs its own copy of the
+workload (walkers shard across GPUs, no data-path collective: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOP_PAIR = 45.0      # coordination pair, FMA = 2 flops (per-pair count of the workload spec)
+FLOP_HILL = 14.0      # one hill Gaussian + gradient (plus one exp)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------- workloads
+def build_single(w, torch, device):
+    """One plain context for a single-walker workload (C1/C2/C3)."""
+    from gluedmd_b200 import GluedForce
+    from gluedmd_b200.context import Context, System
+    s = System()
+    for m in w.masses:
+        s.addParticle(float(m))
+    f = GluedForce()
+    f.setUsesPeriodicBoundaryConditions(w.pbc)
+    for t, a, p in w.cvs:
+        f.addCollectiveVariable(t, [int(x) for x in a], [float(x) for x in p])
+    for t, c, p, ip in w.biases:
+        f.addBias(t, c, p, ip)
+    s.addForce(f)
+    s.setDefaultPeriodicBoxVectors(*w.box)
+    ctx = Context(s, w.positions, device=device)
+    if w.blob:
+        f.setBiasState(w.blob)
+    return ctx, f
+
+
+def time_steps(torch, step_fn, steps, warmup, flush):
+    stream = torch.cuda.current_stream()
+    for i in range(warmup):
+        step_fn(i)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        flush.add_(1.0)
+        starts[i].record(stream)
+        step_fn(warmup + i)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def run_single(args, torch, cfg):
+    from gluedmd_b200 import workloads as W, _native
+    import ctypes
+    w = {"c1": lambda: W.config1("grid"), "c2": W.config2, "c3": W.config3}[cfg]()
+    ctx, f = build_single(w, torch, "cuda")
+    nc = ctx.glued_context_for(f)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step(i):
+        nc.update_state(i)
+        nc.execute(True, False)
+
+    launches0 = nc.launch_count()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms = time_steps(torch, step, args.steps, args.warmup, flush)
+    launches = (nc.launch_count() - launches0)
+    kernels_per_step = launches / float(args.steps + args.warmup)
+    us = ms * 1e3 / args.steps
+    # dominant kernel, timed with CUDA events on the launching stream
+    phases = nc.profile_phases(20)
+    names = ["simple_cvs", "group_cvs", "coord_pairs", "coord_finalize", "biases", "scatter"]
+    dom = int(np.argmax(phases))
+    # e2e through the C ABI with host buffers
+    n = len(w.positions)
+    host_pos = torch.zeros((ctx.padded, 4), dtype=torch.float32).pin_memory()
+    host_pos[:n, :3] = torch.as_tensor(w.positions, dtype=torch.float32)
+    host_f = torch.zeros(3 * ctx.padded, dtype=torch.int64).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def e2e_step(i):
+        ctx.posq.copy_(host_pos, non_blocking=True)
+        ctx.force_buf.zero_()
+        nc.update_state(args.warmup + args.steps + i)
+        e = nc.execute(True, True)  # synchronizing energy read
+        host_f.copy_(ctx.force_buf, non_blocking=True)
+        return e
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        e2e_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_us = e0.elapsed_time(e1) * 1e3 / args.steps
+    info = dict(workload=w.name, us_per_step=us, phases_ms=dict(zip(names, phases)), dominant=names[dom],
+                dom_ms=phases[dom], kernels_per_step=kernels_per_step, e2e_us=e2e_us,
+                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 8 + 8), clocks=clk.summary(), w=w)
+    return info
+
+
+def cpu_baseline_single(cfg, w, budget_s=12.0):
+    """Reference kernels compiled for the host (oracle/_ref) when present, else the
+    oracle's FP32 restatement; bounded sample of steps on one host thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ref_runner import RefSystem
+    kind = "reference" if RefSystem.available() else "port"
+    cls = RefSystem if kind == "reference" else O.OracleSystem
+    biases = [b for b in w.biases if b[0] in (1, 3, 5)]
+    sysm = cls(w.cvs, biases, masses=w.masses, periodic=w.pbc, mode="f32", num_particles=len(w.positions))
+    if w.blob:
+        sysm.load_blob(w.blob)
+    box = np.asarray(w.box).ravel()
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        sysm.execute(w.positions, box)
+        n += 1
+        if time.perf_counter() - t0 > budget_s or n >= 50:
+            break
+    dt = (time.perf_counter() - t0) / n
+    return dict(value=dt * 1e6, unit="us/step", cores=1, kind=kind,
+                sample=f"{n} force evaluations of {w.name} ({'reference kernel text compiled for the host' if kind == 'reference' else 'oracle FP32 restatement'}), 1 thread")
+
+
+def c4_inputs(n_walkers=64, n_hills=50000):
+    from gluedmd_b200 import workloads as W
+    ws, hill = W.config4_walkers(n_walkers=n_walkers, n_hills=n_hills)
+    for w in ws:
+        w["cn0"] = W.coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"])
+    return ws, hill
+
+
+def c4_biases(w, hill):
+    from gluedmd_b200.batch import c4_biases as cb
+    return cb(w, hill["params"], hill["iparams"], cn0=w["cn0"])
+
+
+def run_c4(args, torch, ws, hill):
+    from gluedmd_b200.batch import Batch, Walker, force_for
+    forces = [force_for(w["cvs"], c4_biases(w, hill)) for w in ws]
+    walkers = [Walker(w["pos"], w["box"]) for w in ws]
+    b = Batch(forces, walkers)
+    b.set_hills(hill["centers"], hill["heights"])
+    tune = b.autotune()
+    for wk in walkers:
+        wk.force.zero_()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    W_ = len(ws)
+
+    def step(i):
+        b.update_state(i)
+        b.execute()
+
+    l0 = b.launch_count()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms = time_steps(torch, step, args.steps, args.warmup, flush)
+    launches = b.launch_count() - l0
+    status = b.status()
+    # the persistent step kernel is the whole step: its per-launch time
+    step_ms = ms / args.steps
+    # plain per-walker path: one context per walker, stepped one after another
+    plain_ctx = []
+    from gluedmd_b200.context import Context, System
+    from gluedmd_b200 import GluedForce, workloads as Wl
+    hb = Wl.blob(hills=[(hill["centers"], hill["heights"])])
+    for w in ws:
+        s_ = System()
+        for m in w["masses"]:
+            s_.addParticle(float(m))
+        f = force_for(w["cvs"], c4_biases(w, hill))
+        s_.addForce(f)
+        s_.setDefaultPeriodicBoxVectors(*w["box"])
+        ctx = Context(s_, w["pos"])
+        f.setBiasState(hb)
+        plain_ctx.append((ctx, ctx.glued_context_for(f)))
+
+    def plain_step(i):
+        for ctx, nc in plain_ctx:
+            nc.update_state(i)
+            nc.execute(True, False)
+
+    psteps = max(3, min(args.steps, 20))
+    plain_ms = time_steps(torch, plain_step, psteps, 3, flush) / psteps
+    plain_launches = sum(nc.launch_count() for _, nc in plain_ctx) / float(psteps + 3)
+    del plain_ctx
+    # e2e through the C ABI with host buffers: every walker's positions H2D from
+    # pinned memory, one step, every force buffer and the energies D2H
+    host_pos = [torch.zeros_like(wk.posq, device="cpu").pin_memory() for wk in walkers]
+    host_f = [torch.zeros_like(wk.force, device="cpu").pin_memory() for wk in walkers]
+    for hp, wk in zip(host_pos, walkers):
+        hp.copy_(wk.posq)
+    stream = torch.cuda.current_stream()
+
+    def e2e_step(i):
+        for hp, wk in zip(host_pos, walkers):
+            wk.posq.copy_(hp, non_blocking=True)
+            wk.force.zero_()
+        b.update_state(10 ** 6 + i)
+        b.execute()
+        for hf, wk in zip(host_f, walkers):
+            hf.copy_(wk.force, non_blocking=True)
+        return b.energies()  # synchronizing read of the per-walker energies
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        e2e_step(args.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    h2d = sum(hp.numel() * 4 for hp in host_pos)
+    d2h = sum(hf.numel() * 8 for hf in host_f) + 8 * W_
+    pairs = sum(256 * 1024 for _ in ws)
+    flops = pairs * FLOP_PAIR + W_ * b.num_hills() * FLOP_HILL
+    return dict(walkers=W_, step_ms=step_ms, value=W_ * 1e3 / step_ms, plain_ms=plain_ms,
+                plain_value=W_ * 1e3 / plain_ms, plain_launches=plain_launches, e2e_value=W_ * 1e3 / e2e_ms,
+                h2d=int(h2d), d2h=int(d2h), launches_per_step=launches / float(args.steps + args.warmup),
+                flops=flops, clocks=clk.summary(), tune=tune, status=status, hills=b.num_hills(),
+                graphed=True)
+
+
+def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
+    """The reference's kernels compiled for the host (oracle/_ref), one RefSystem
+    per walker, walkers spread over host threads (ctypes releases the GIL).
+    The reference's MetaD is grid-based: the 50,000 shared hills are deposited on
+    its 256 x 256 grid over (dihedral, angle) and evaluated by its metaDEvalBias."""
+    import concurrent.futures as cf
+    import math as _m
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ref_runner import RefSystem
+    from gluedmd_b200 import workloads as Wl
+    kind = "reference" if RefSystem.available() else "port"
+    cls = RefSystem if kind == "reference" else O.OracleSystem
+    sig = [0.35, 0.35]
+    lo, hi = [-_m.pi, 0.0], [_m.pi, _m.pi]
+    grid = Wl.grid_from_hills_windowed(hill["centers"], hill["heights"], sig, lo, hi, [256, 256], [1, 0])
+    systems = []
+    for w in ws:
+        biases = [b for b in c4_biases(w, hill) if b[0] == 1]
+        biases.append((3, [2, 1], [1.2] + sig + [10.0, 2.494338785] + lo + hi, [500, 256, 256, 1, 0]))
+        s_ = cls(w["cvs"], biases, masses=w["masses"], periodic=True, mode="f32", num_particles=w["n"])
+        for st in s_.bias_state:
+            if st["type"] == 3:
+                st["grid"][:] = grid
+        systems.append((s_, w))
+    threads = threads or os.cpu_count() or 1
+    pool = cf.ThreadPoolExecutor(max_workers=threads)
+
+    def one(sw):
+        s_, w = sw
+        return s_.execute(w["pos"], w["box"].ravel())["energy"]
+
+    list(pool.map(one, systems))  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        list(pool.map(one, systems))
+        n += 1
+        if time.perf_counter() - t0 > steps_budget_s or n >= 20:
+            break
+    dt = (time.perf_counter() - t0) / n
+    pool.shutdown()
+    return dict(value=len(ws) / dt, unit="walker-steps/s", cores=threads, kind=kind,
+                sample=f"{n} steps x {len(ws)} walkers of the 64-walker workload on {threads} host threads "
+                       f"({'reference kernel text compiled for the host' if kind == 'reference' else 'oracle FP32 restatement'}; "
+                       "MetaD as the reference's 256x256 grid holding the same 50,000 hills)")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # The reference's own CPU implementation of the path on the host cores;
+        # rank 0 alone runs and prints.
+        if rank != 0:
+            return
+        if args.config == "c4":
+            ws, hill = c4_inputs()
+            cb = cpu_reference_c4(ws, hill, steps_budget_s=min(60.0, max(10.0, 0.2 * args.steps)))
+            line = {"impl": "reference", "metric": "walker-steps/s (CV+bias+force, 64 walkers)", "value": cb["value"],
+                    "unit": "walker-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                    "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": "C4: 64 walkers 1k-50k atoms, dist/angle/dihedral + 256x1024 coordination, "
+                                           "harmonic restraints, shared 50,000-hill WT MetaD"},
+                    "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "walker-steps/s",
+                                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        else:
+            from gluedmd_b200 import workloads as W
+            w = {"c1": lambda: W.config1("grid"), "c2": W.config2, "c3": W.config3}[args.config]()
+            cb = cpu_baseline_single(args.config, w, budget_s=max(5.0, 0.5 * args.steps))
+            line = {"impl": "reference", "metric": "CV+bias+force us/step", "value": cb["value"], "unit": "us/step",
+                    "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                    "dtype": "f32", "data": "synthetic", "config": {"workload": w.name},
+                    "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "us/step", "h2d_bytes_per_step": 0,
+                                                "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    from gluedmd_b200 import dist as D
+    torch.cuda.set_device(local)
+    dist = D.init("nccl", timeout_s=120) if world > 1 else None
+
+    def max_over_ranks(x):
+        return D.max_over_ranks(x, device="cuda")
+
+    from gluedmd_b200 import _native
+    import ctypes
+    pk, src = peaks()
+
+    if args.config == "c4":
+        ws, hill = c4_inputs()
+        info = run_c4(args, torch, ws, hill)
+        step_ms = max_over_ranks(info["step_ms"])
+        if dist is not None:
+            dist.barrier()
+        if rank == 0:
+            fp32 = ctypes.c_double()
+            _native.call("glued_measure_fp32_peak", ctypes.byref(fp32))
+            ach = info["flops"] / (info["step_ms"] * 1e-3) / 1e12
+            roof = {"bound": "fp32", "kernel": "k_batch_step (whole step, one launch)", "achieved": ach,
+                    "peak": fp32.value, "unit": "TFLOP/s", "frac": ach / fp32.value, "traffic": None,
+                    "peak_source": "FP32 FMA microkernel measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
+                    "algorithmic": f"64 x 262144 pairs x {FLOP_PAIR:.0f} flop + 64 x {info['hills']} hills x {FLOP_HILL:.0f} flop"}
+            cb = None
+            if not args.no_cpu_baseline and world == 1:
+                cb = cpu_reference_c4(ws, hill, steps_budget_s=15.0)
+            value = world * info["walkers"] * 1e3 / step_ms
+            line = {
+                "metric": "walker-steps/s (CV+bias+force, 64 walkers)", "value": value, "unit": "walker-steps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "C4: 64 walkers 1k-50k atoms (log-uniform), dist/angle/dihedral + 256x1024 "
+                                       "coordination, harmonic restraints, shared 50,000-hill WT MetaD",
+                           "walkers_per_gpu": info["walkers"], "l2": "flushed between steps (256 MB write)",
+                           "parallelism": f"walkers x{world} GPUs (no data-path collective)", "tuning": info["tune"]},
+                "e2e": {"value": world * info["e2e_value"], "unit": "walker-steps/s", "h2d_bytes_per_step": info["h2d"],
+                        "d2h_bytes_per_step": info["d2h"]},
+                "gpu_launches": int(round(info["launches_per_step"] * args.steps)),
+                "roofline": roof, "cpu_baseline": cb, "clocks": info["clocks"],
+                "plain_per_walker_gpu": {"value": world * info["plain_value"], "unit": "walker-steps/s",
+                                         "launches_per_step": info["plain_launches"],
+                                         "speedup_batched_vs_plain": info["plain_ms"] / info["step_ms"]},
+                "status": info["status"], "peaks_source": src,
+            }
+            print(json.dumps(line))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    info = run_single(args, torch, args.config)
+    us = max_over_ranks(info["us_per_step"])
+    if dist is not None:
+        dist.barrier()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    fp32 = ctypes.c_double()
+    _native.call("glued_measure_fp32_peak", ctypes.byref(fp32))
+    w = info["w"]
+    roof = None
+    if info["dominant"] == "coord_pairs":
+        pairs = sum((len(a) - 1 - a[0]) * a[0] for t, a, p in w.cvs if t == 6)
+        flops = pairs * FLOP_PAIR
+        ach = flops / (info["dom_ms"] * 1e-3) / 1e12
+        roof = {"bound": "fp32", "kernel": "k_coord_pairs", "achieved": ach, "peak": fp32.value,
+                "unit": "TFLOP/s", "frac": ach / fp32.value, "traffic": None,
+                "peak_source": "FP32 FMA microkernel measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
+                "algorithmic": f"{pairs} pairs x {FLOP_PAIR:.0f} flop"}
+    cb = None
+    if not args.no_cpu_baseline and world == 1:
+        cb = cpu_baseline_single(args.config, w)
+    line = {
+        "metric": "CV+bias+force us/step", "value": us, "unit": "us/step", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": us / 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": info["workload"], "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": info["e2e_us"], "unit": "us/step", "h2d_bytes_per_step": info["h2d"],
+                "d2h_bytes_per_step": info["d2h"]},
+        "gpu_launches": int(round(info["kernels_per_step"] * args.steps)),
+        "roofline": roof, "cpu_baseline": cb, "clocks": info["clocks"],
+        "phases_ms": info["phases_ms"], "peaks_source": src,
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

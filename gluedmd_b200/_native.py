@@ -78,17 +78,25 @@ _SIGS = {
     "glued_context_set_multiwalker_ptrs": [c_void_p, c_int, P(c_ll), c_int],
     "glued_context_device_arrays": [c_void_p] + [P(c_void_p)] * 7 + [P(c_int), P(c_int)],
     "glued_context_opes_last_decision": [c_void_p, c_int, P(c_int)],
-    "glued_batch_create": [c_void_p, c_int, P(WalkerDesc), P(c_double), P(c_void_p)],
+    "glued_context_profile_phases": [c_void_p, c_int, P(c_double), P(c_int)],
+    "glued_context_launch_count": [c_void_p, P(c_ll)],
+    "glued_measure_fp32_peak": [P(c_double)],
+    "glued_batch_create": [P(c_void_p), c_int, P(WalkerDesc), P(c_void_p)],
     "glued_batch_destroy": [c_void_p],
     "glued_batch_set_stream": [c_void_p, c_void_p],
+    "glued_batch_set_tuning": [c_void_p, P(c_int)],
+    "glued_batch_get_tuning": [c_void_p, P(c_int)],
     "glued_batch_autotune": [c_void_p, P(c_int)],
     "glued_batch_execute": [c_void_p],
     "glued_batch_update_state": [c_void_p, c_int],
     "glued_batch_get_energies": [c_void_p, P(c_double)],
     "glued_batch_get_cv_values": [c_void_p, P(c_double)],
+    "glued_batch_num_cvs": [c_void_p, P(c_int)],
     "glued_batch_num_hills": [c_void_p, P(c_int)],
     "glued_batch_set_hills": [c_void_p, P(c_double), P(c_double), c_int],
+    "glued_batch_get_hills": [c_void_p, P(c_double), P(c_double), c_int],
     "glued_batch_status": [c_void_p, P(c_int)],
+    "glued_batch_launch_count": [c_void_p, P(c_ll)],
 }
 
 

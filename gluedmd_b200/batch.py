@@ -1,0 +1,156 @@
+"""Batched multi-walker evaluation (glued_batch_* of include/glued_b200.h).
+
+All walkers of one GPU are evaluated by a single cooperative persistent launch
+per step. Each walker owns a float4 posq buffer and an int64 fixed-point force
+buffer in device memory (torch tensors here); walkers may have different atom
+counts and boxes but the same CV / bias structure.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from ._native import WalkerDesc, call, lib, c_int, c_double, c_void_p, c_ll
+from .gluedplugin import GluedForce
+
+FIXED = 4294967296.0
+
+
+class Walker:
+    """Device buffers of one walker: posq (padded, 4) float32 and force (3*padded) int64."""
+
+    def __init__(self, positions, box, device="cuda", padding=32):
+        pos = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+        self.n = len(pos)
+        self.padded = ((self.n + padding - 1) // padding) * padding
+        self.posq = torch.zeros((self.padded, 4), dtype=torch.float32, device=device)
+        self.posq[: self.n, :3] = torch.as_tensor(pos, dtype=torch.float32, device=device)
+        self.force = torch.zeros(3 * self.padded, dtype=torch.int64, device=device)
+        self.box = np.asarray(box, dtype=np.float64).reshape(3, 3)
+
+    def forces(self):
+        f = self.force.view(3, self.padded)[:, : self.n].cpu().numpy().astype(np.float64) / FIXED
+        return f.T.copy()
+
+
+class Batch:
+    def __init__(self, forces, walkers, stream=None):
+        if len(forces) != len(walkers):
+            raise ValueError("one force per walker")
+        self.forces = list(forces)
+        self.walkers = list(walkers)
+        W = len(walkers)
+        descs = (WalkerDesc * W)()
+        for i, w in enumerate(walkers):
+            descs[i].posq = w.posq.data_ptr()
+            descs[i].force_buffer = w.force.data_ptr()
+            descs[i].num_atoms = w.n
+            descs[i].padded_num_atoms = w.padded
+            for k, v in enumerate(w.box.ravel()):
+                descs[i].box[k] = float(v)
+        fptrs = (c_void_p * W)(*[f._h.value for f in forces])
+        h = c_void_p()
+        call("glued_batch_create", fptrs, W, descs, ctypes.byref(h))
+        self._h = h
+        self.num_walkers = W
+        s = torch.cuda.current_stream() if stream is None else stream
+        call("glued_batch_set_stream", self._h, c_void_p(s.cuda_stream))
+        n = c_int()
+        call("glued_batch_num_cvs", self._h, ctypes.byref(n))
+        self.num_cvs = n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().glued_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def execute(self):
+        call("glued_batch_execute", self._h)
+
+    def update_state(self, step):
+        call("glued_batch_update_state", self._h, int(step))
+
+    def step(self, step):
+        self.update_state(step)
+        self.execute()
+
+    def energies(self):
+        out = (c_double * self.num_walkers)()
+        call("glued_batch_get_energies", self._h, out)
+        return np.array(out[:])
+
+    def cv_values(self):
+        out = (c_double * (self.num_walkers * max(1, self.num_cvs)))()
+        call("glued_batch_get_cv_values", self._h, out)
+        return np.array(out[: self.num_walkers * self.num_cvs]).reshape(self.num_walkers, self.num_cvs)
+
+    def num_hills(self):
+        n = c_int()
+        call("glued_batch_num_hills", self._h, ctypes.byref(n))
+        return n.value
+
+    def set_hills(self, centers, heights):
+        c = np.ascontiguousarray(centers, dtype=np.float64)
+        h = np.ascontiguousarray(heights, dtype=np.float64)
+        call("glued_batch_set_hills", self._h, c.ctypes.data_as(ctypes.POINTER(c_double)),
+             h.ctypes.data_as(ctypes.POINTER(c_double)), len(h))
+
+    def get_hills(self, D=2):
+        n = self.num_hills()
+        c = np.zeros(n * D)
+        h = np.zeros(n)
+        call("glued_batch_get_hills", self._h, c.ctypes.data_as(ctypes.POINTER(c_double)),
+             h.ctypes.data_as(ctypes.POINTER(c_double)), n)
+        return c.reshape(n, D), h
+
+    def status(self):
+        s = c_int()
+        call("glued_batch_status", self._h, ctypes.byref(s))
+        return s.value
+
+    def launch_count(self):
+        v = c_ll()
+        call("glued_batch_launch_count", self._h, ctypes.byref(v))
+        return v.value
+
+    @property
+    def tuning(self):
+        t = (c_int * 4)()
+        call("glued_batch_get_tuning", self._h, t)
+        return dict(ra=t[0], b_split=t[1], hill_items=t[2], parts=t[3])
+
+    def set_tuning(self, ra=8, b_split=256, hill_items=96, parts=4):
+        t = (c_int * 4)(ra, b_split, hill_items, parts)
+        call("glued_batch_set_tuning", self._h, t)
+
+    def autotune(self):
+        t = (c_int * 4)()
+        call("glued_batch_autotune", self._h, t)
+        return dict(ra=t[0], b_split=t[1], hill_items=t[2], parts=t[3])
+
+
+def force_for(cvs, biases, pbc=True):
+    f = GluedForce()
+    f.setUsesPeriodicBoundaryConditions(pbc)
+    for t, a, p in cvs:
+        f.addCollectiveVariable(t, [int(x) for x in a], [float(x) for x in p])
+    for t, c, p, ip in biases:
+        f.addBias(t, c, p, ip)
+    return f
+
+
+def c4_biases(walker, hill_params, hill_iparams, restraint_k=100.0, cn0=None):
+    """Per-walker biases of the 64-walker workload: harmonic restraints on the
+    distance (CV 0) and coordination (CV 3) at their initial values, and the shared
+    hill-sum MetaD on (dihedral, angle) = CVs (2, 1)."""
+    b = [(1, [0], [restraint_k, walker["d0"]], [0])]
+    if cn0 is not None:
+        b.append((1, [3], [restraint_k, cn0], [0]))
+    b.append((103, [2, 1], hill_params, hill_iparams))
+    return b

@@ -1,5 +1,5 @@
-// Batched multi-walker evaluation: many walkers with the same force descriptor,
-// one persistent launch per step.
+// Batched multi-walker evaluation: many walkers with the same CV / bias
+// structure evaluated by one cooperative persistent launch per step.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,19 +10,34 @@
 
 namespace glued {
 
+struct BatchTuning {
+    int ra = 8;        // A atoms per thread in the coordination tile (TA = 8 * ra)
+    int bSplit = 256;  // B atoms per coordination CTA item
+    int hillItems = 96;  // hill-table work items (each walks chunks hillItems apart)
+    int parts = 4;     // finalize items per walker
+};
+
 class Batch {
 public:
-    Batch(const GluedForce& f, int numWalkers, const glued_walker_desc* walkers, const double* masses);
+    Batch(const std::vector<const GluedForce*>& forces, const glued_walker_desc* walkers);
     ~Batch();
     void setStream(cudaStream_t s);
-    int autotune();
+    BatchTuning autotune();
+    void setTuning(const BatchTuning& t);
+    BatchTuning tuning() const;
     void execute();
     void updateState(int step);
     void energies(double* out);
     void cvValues(double* out);
+    int numCVs() const;
+    int numWalkers() const;
     int numHills();
     void setHills(const double* centers, const double* heights, int n);
+    void getHills(double* centers, double* heights, int n);
     int status();
+    long long launchCount() const;
+    bool graphed() const;
+    double lastStepMs();
 
 private:
     struct Impl;

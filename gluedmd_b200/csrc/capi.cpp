@@ -10,6 +10,7 @@
 #include "batch.hpp"
 #include "context.hpp"
 #include "force.hpp"
+#include "kernels.hpp"
 
 struct glued_force { glued::GluedForce f; };
 struct glued_context { glued::Context* c; };
@@ -296,16 +297,28 @@ int glued_context_device_arrays(glued_context* c, void** cvv, void** dudcv, void
         if (num_rows) *num_rows = c->c->numRows();
     });
 }
+int glued_context_profile_phases(glued_context* c, int reps, double* out, int* n) {
+    return guard([&] { need(c, "context"); copyOut(c->c->profilePhases(reps), out, n, "phases"); });
+}
+int glued_context_launch_count(glued_context* c, long long* count) {
+    return guard([&] { need(c, "context"); need(count, "out"); *count = c->c->launchCount(); });
+}
+int glued_measure_fp32_peak(double* tflops) {
+    return guard([&] { need(tflops, "out"); *tflops = glued::measureFp32Peak(); });
+}
 int glued_context_opes_last_decision(glued_context* c, int idx, int* decision) {
     return guard([&] { need(c, "context"); need(decision, "out"); *decision = c->c->opesLastDecision(idx); });
 }
 
 // ------------------------------------------------------------------ batch
-int glued_batch_create(const glued_force* f, int num_walkers, const glued_walker_desc* walkers, const double* masses,
+int glued_batch_create(const glued_force* const* forces, int num_walkers, const glued_walker_desc* walkers,
                        glued_batch** out) {
     return guard([&] {
-        need(f, "force"); need(walkers, "walkers"); need(out, "out");
-        *out = new glued_batch{new glued::Batch(f->f, num_walkers, walkers, masses)};
+        need(forces, "forces"); need(walkers, "walkers"); need(out, "out");
+        if (num_walkers < 1) throw glued::Error(GLUED_E_INVALID, "num_walkers must be >= 1");
+        std::vector<const glued::GluedForce*> fs;
+        for (int w = 0; w < num_walkers; w++) { need(forces[w], "forces[w]"); fs.push_back(&forces[w]->f); }
+        *out = new glued_batch{new glued::Batch(fs, walkers)};
     });
 }
 int glued_batch_destroy(glued_batch* b) {
@@ -316,8 +329,27 @@ int glued_batch_destroy(glued_batch* b) {
 int glued_batch_set_stream(glued_batch* b, void* stream) {
     return guard([&] { need(b, "batch"); b->b->setStream((cudaStream_t)stream); });
 }
-int glued_batch_autotune(glued_batch* b, int* chosen) {
-    return guard([&] { need(b, "batch"); int t = b->b->autotune(); if (chosen) *chosen = t; });
+int glued_batch_set_tuning(glued_batch* b, const int tune[4]) {
+    return guard([&] {
+        need(b, "batch"); need(tune, "tune");
+        glued::BatchTuning t;
+        t.ra = tune[0]; t.bSplit = tune[1]; t.hillItems = tune[2]; t.parts = tune[3];
+        b->b->setTuning(t);
+    });
+}
+int glued_batch_get_tuning(glued_batch* b, int tune[4]) {
+    return guard([&] {
+        need(b, "batch"); need(tune, "tune");
+        glued::BatchTuning t = b->b->tuning();
+        tune[0] = t.ra; tune[1] = t.bSplit; tune[2] = t.hillItems; tune[3] = t.parts;
+    });
+}
+int glued_batch_autotune(glued_batch* b, int tune[4]) {
+    return guard([&] {
+        need(b, "batch");
+        glued::BatchTuning t = b->b->autotune();
+        if (tune) { tune[0] = t.ra; tune[1] = t.bSplit; tune[2] = t.hillItems; tune[3] = t.parts; }
+    });
 }
 int glued_batch_execute(glued_batch* b) {
     return guard([&] { need(b, "batch"); b->b->execute(); });
@@ -331,14 +363,31 @@ int glued_batch_get_energies(glued_batch* b, double* e) {
 int glued_batch_get_cv_values(glued_batch* b, double* v) {
     return guard([&] { need(b, "batch"); need(v, "out"); b->b->cvValues(v); });
 }
+int glued_batch_num_cvs(glued_batch* b, int* n) {
+    return guard([&] { need(b, "batch"); need(n, "out"); *n = b->b->numCVs(); });
+}
 int glued_batch_num_hills(glued_batch* b, int* n) {
     return guard([&] { need(b, "batch"); need(n, "out"); *n = b->b->numHills(); });
 }
 int glued_batch_set_hills(glued_batch* b, const double* c, const double* h, int n) {
-    return guard([&] { need(b, "batch"); b->b->setHills(c, h, n); });
+    return guard([&] {
+        need(b, "batch");
+        if (n > 0) { need(c, "centers"); need(h, "heights"); }
+        b->b->setHills(c, h, n);
+    });
+}
+int glued_batch_get_hills(glued_batch* b, double* c, double* h, int n) {
+    return guard([&] {
+        need(b, "batch");
+        if (n > 0) { need(c, "centers"); need(h, "heights"); }
+        b->b->getHills(c, h, n);
+    });
 }
 int glued_batch_status(glued_batch* b, int* status) {
     return guard([&] { need(b, "batch"); need(status, "out"); *status = b->b->status(); });
+}
+int glued_batch_launch_count(glued_batch* b, long long* count) {
+    return guard([&] { need(b, "batch"); need(count, "out"); *count = b->b->launchCount(); });
 }
 
 }  // extern "C"

@@ -34,10 +34,6 @@ void DBuf::alloc(size_t n) {
     cudaCheck(cudaMemset(p, 0, n), "cudaMemset");
 }
 
-template <class T> void DBuf::upload(const std::vector<T>& v, cudaStream_t) {
-    alloc(v.size() * sizeof(T));
-    if (!v.empty()) cudaCheck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
-}
 
 namespace {
 
@@ -78,6 +74,19 @@ int bodyRows(const CVSpec& c) {
         default: return (int)c.atoms.size();
     }
 }
+
+}  // namespace
+
+// Switch kind of a coordination CV: 3 for n = 6, m = 12 (sqrt- and pow-free),
+// -1 for other integer exponents (cancellation-free polynomial quotient),
+// 0 for non-integer exponents (the reference's pow formula).
+int coordKind(float n, float m) {
+    bool integral = n == std::floor(n) && m == std::floor(m) && n >= 1 && m >= 1 && n <= 64 && m <= 64;
+    if (integral && n == 6.0f && m == 12.0f) return 3;
+    return integral ? -1 : 0;
+}
+
+namespace {
 
 int biasEvalRank(int t) {
     // bias evaluation order of execute() (CommonGluedKernels.cpp:4955-5026)
@@ -243,11 +252,7 @@ void Context::buildPlan(const GluedForce& f) {
             it.r0 = (float)c.params[0]; it.n = (float)c.params[1]; it.m = (float)c.params[2];
             double rc = (t == CV_COORDINATION_CUTOFF) ? c.params[3] : 0.0;
             it.rc2 = (float)(rc * rc);
-            it.kind = 0;
-            bool integral = it.n == std::floor(it.n) && it.m == std::floor(it.m) && it.n >= 1 && it.m >= 1 &&
-                            it.n <= 64 && it.m <= 64;
-            if (integral) it.kind = -1;
-            if (integral && it.m == 2.0f * it.n && (int)it.n % 2 == 0 && it.n <= 8) it.kind = (int)it.n / 2;
+            it.kind = coordKind(it.n, it.m);
             for (int k = 0; k < it.nA + it.nB; k++) { jAtom[jac0 + k] = c.atoms[1 + k]; jCv[jac0 + k] = cv; }
             coord.push_back(it);
         } else {
@@ -362,6 +367,13 @@ void Context::buildPlan(const GluedForce& f) {
             pa += it.splitsB * it.nA; pb += it.tilesA * it.nB;
             rows += it.nA + it.nB;
         }
+        // one kernel instantiation per launch: items with different switch kinds
+        // fall back to the most general kind present
+        coordKind_ = coord[0].kind;
+        for (auto& it : coord)
+            if (it.kind != coordKind_) coordKind_ = (coordKind_ == 0 || it.kind == 0) ? 0 : -1;
+        if (coordKind_ != 3)
+            for (auto& it : coord) it.kind = coordKind_;
         coordItems_.upload(coord);
         coordAtoms_.upload(coordAtoms);
         coordBlockItem_.upload(blockItem);
@@ -572,16 +584,55 @@ void Context::setBox(const double box[9]) {
 }
 
 // ---------------------------------------------------------------- execute
-void Context::enqueueExecute(cudaStream_t s, bool includeForces) {
+// Launch groups of one force evaluation, in order:
+//   0 simple CVs, 1 group CVs, 2 coordination pairs, 3 coordination finalize,
+//   4 biases, 5 scatter. onlyPhase >= 0 enqueues a single group (profiling).
+void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) {
     const BoxDev* box = box_.as<BoxDev>();
     double* cvv = cvv_.as<double>();
     const int* u2g = u2g_.as<int>();
-    launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
-    launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_);
-    launchCoord(s, posq_, u2g, C_, coordBlocks_, coordRows_, boxHost_.kind, coordRA_, box, J_, cvv);
-    launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
-                 testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>());
-    if (includeForces) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
+    auto want = [&](int p) { return onlyPhase < 0 || onlyPhase == p; };
+    if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
+    if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_);
+    if (want(2) || want(3))
+        launchCoord(s, posq_, u2g, C_, coordBlocks_, coordRows_, boxHost_.kind, coordRA_, coordKind_, box, J_, cvv,
+                    onlyPhase < 0 ? 3 : (onlyPhase == 2 ? 1 : 2));
+    if (want(4))
+        launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
+                     testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>());
+    if (includeForces && want(5)) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
+}
+
+int Context::kernelsPerExecute(bool includeForces) const {
+    int k = 1;  // biases
+    if (numSimple_ > 0) k++;
+    if (G_.numItems > 0) k++;
+    if (C_.numItems > 0) k += 2;
+    if (includeForces && numRows_ > 0) k++;
+    return k;
+}
+
+std::vector<double> Context::profilePhases(int reps) {
+    requireBound();
+    if (reps < 1) reps = 1;
+    std::vector<double> out(6, 0.0);
+    if (numCVs_ == 0) return out;
+    cudaEvent_t a, b;
+    cudaCheck(cudaEventCreate(&a), "event");
+    cudaCheck(cudaEventCreate(&b), "event");
+    for (int p = 0; p < 6; p++) {
+        enqueueExecute(stream_, true, p);  // warm-up
+        cudaCheck(cudaEventRecord(a, stream_), "event");
+        for (int r = 0; r < reps; r++) enqueueExecute(stream_, true, p);
+        cudaCheck(cudaEventRecord(b, stream_), "event");
+        cudaCheck(cudaEventSynchronize(b), "event");
+        float ms = 0;
+        cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
+        out[p] = ms / reps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return out;
 }
 
 double Context::execute(bool includeForces, bool includeEnergy) {
@@ -589,6 +640,7 @@ double Context::execute(bool includeForces, bool includeEnergy) {
     if (force_.testForceMode != 0) {
         launchTestForce(stream_, posq_, atomIndex_, force_buf_, padded_, numParticles_, force_.testForceMode,
                         force_.testForceScale, box_.as<BoxDev>());
+        launches_ += 1;
         cudaCheck(cudaGetLastError(), "test force");
         return 0.0;
     }
@@ -609,6 +661,7 @@ double Context::execute(bool includeForces, bool includeEnergy) {
         enqueueExecute(stream_, includeForces);
         cudaCheck(cudaGetLastError(), "execute");
     }
+    launches_ += kernelsPerExecute(includeForces);
     cvReady_ = true;
     double total = 0.0;
     if (includeEnergy && numEnergySlots_ > 0) {
@@ -650,12 +703,14 @@ void Context::updateState(int step) {
         bool will = hb.dev.adaptiveStride == 0 || hb.nSamplesCPU >= hb.dev.adaptiveStride;
         launchOpesDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en, mergeFlag_.as<int>(),
                           uprobPartial_.as<double>(), nUprobPartial_);
+        launches_ += 3;
         if (will) hb.numKernelsCPU++;
     }
     for (auto& hb : biases_) {
         if (hb.spec.type == BIAS_METAD) {
             if (step == 0 || step % hb.dev.pace != 0) continue;
             launchMetadDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en);
+            launches_ += 1;
             hb.numDeposited++;
         }
     }
@@ -663,6 +718,7 @@ void Context::updateState(int step) {
         if (hb.spec.type == BIAS_METAD_HILLS) {
             if (step == 0 || step % hb.dev.pace != 0) continue;
             launchHillsDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, en);
+            launches_ += 1;
         }
     }
     cudaCheck(cudaGetLastError(), "updateState");

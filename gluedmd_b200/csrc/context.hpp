@@ -33,6 +33,12 @@ struct DBuf {
 };
 
 void cudaCheck(cudaError_t e, const char* what);
+int coordKind(float n, float m);
+
+template <class T> void DBuf::upload(const std::vector<T>& v, cudaStream_t) {
+    alloc(v.size() * sizeof(T));
+    if (!v.empty()) cudaCheck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
 
 struct HostBias {
     BiasSpec spec;
@@ -68,6 +74,8 @@ public:
     std::vector<long long> multiWalkerPtrs(int biasIndex);
     void setMultiWalkerPtrs(int biasIndex, const std::vector<long long>& ptrs);
     int opesLastDecision(int opesIndex);
+    std::vector<double> profilePhases(int reps);
+    long long launchCount() const { return launches_; }
 
     int numCVs() const { return numCVs_; }
     int numRows() const { return numRows_; }
@@ -78,7 +86,8 @@ public:
 private:
     void buildPlan(const GluedForce& f);
     void setupBiases(const GluedForce& f);
-    void enqueueExecute(cudaStream_t s, bool includeForces);
+    void enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase = -1);
+    int kernelsPerExecute(bool includeForces) const;
     void invalidateGraphs();
     void syncUploadBias(HostBias& hb);
     void requireBound() const;
@@ -111,7 +120,7 @@ private:
     int numSimple_ = 0;
     GroupDev G_{};
     CoordDev C_{};
-    int coordBlocks_ = 0, coordRows_ = 0, coordRA_ = 8;
+    int coordBlocks_ = 0, coordRows_ = 0, coordRA_ = 8, coordKind_ = 3;
     int nUprobPartial_ = 296;
 
     std::vector<HostBias> biases_;       // addBias order
@@ -127,6 +136,7 @@ private:
     cudaStream_t capStream_ = nullptr;
     cudaGraphExec_t graph_[2] = {nullptr, nullptr};
     bool useGraphs_ = true;
+    long long launches_ = 0;
 };
 
 }  // namespace glued

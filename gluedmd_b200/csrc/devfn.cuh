@@ -15,8 +15,10 @@ __device__ __forceinline__ F3 cross3(F3 a, F3 b) {
     return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
+// u2g == nullptr means the identity map (walker buffers of the batched path).
 __device__ __forceinline__ F3 loadPos(const float4* __restrict__ posq, const int* __restrict__ u2g, int userAtom) {
-    float4 p = __ldg(posq + __ldg(u2g + userAtom));
+    int slot = u2g ? __ldg(u2g + userAtom) : userAtom;
+    float4 p = __ldg(posq + slot);
     return f3(p.x, p.y, p.z);
 }
 
@@ -74,6 +76,60 @@ __device__ __forceinline__ void blockSum(double (&v)[NV], double* scratch) {
 #pragma unroll
     for (int k = 0; k < NV; k++) v[k] = scratch[k];
     __syncthreads();
+}
+
+// Distance / angle / dihedral value and Jacobian rows (jac[k] for atoms[k]), the
+// reference's formulas (CommonGluedKernels.cpp:177-444). jac may be null.
+__device__ __forceinline__ float simpleCV(int type, const int* atoms, const float4* __restrict__ posq,
+                                         const int* __restrict__ u2g, const BoxDev& box, F3* jac) {
+    if (type == 1) {  // distance
+        F3 d = minImage(sub3(loadPos(posq, u2g, atoms[1]), loadPos(posq, u2g, atoms[0])), box);
+        float dist = sqrtf(dot3(d, d));
+        float inv = dist > 1e-10f ? 1.0f / dist : 0.0f;
+        if (jac) { jac[0] = f3(-d.x * inv, -d.y * inv, -d.z * inv); jac[1] = f3(d.x * inv, d.y * inv, d.z * inv); }
+        return dist;
+    }
+    if (type == 2) {  // angle at atoms[1]
+        F3 pb = loadPos(posq, u2g, atoms[1]);
+        F3 d1 = minImage(sub3(loadPos(posq, u2g, atoms[0]), pb), box);
+        F3 d2 = minImage(sub3(loadPos(posq, u2g, atoms[2]), pb), box);
+        float r1 = sqrtf(dot3(d1, d1)), r2 = sqrtf(dot3(d2, d2));
+        float i1 = r1 > 1e-10f ? 1.0f / r1 : 0.0f, i2 = r2 > 1e-10f ? 1.0f / r2 : 0.0f;
+        F3 n1 = f3(d1.x * i1, d1.y * i1, d1.z * i1), n2 = f3(d2.x * i2, d2.y * i2, d2.z * i2);
+        float ct = fmaxf(-1.0f, fminf(1.0f, dot3(n1, n2)));
+        float th = acosf(ct);
+        if (jac) {
+            float st = sqrtf(1.0f - ct * ct);
+            float is = st > 1e-6f ? 1.0f / st : 0.0f;
+            float s1 = i1 * is, s2 = i2 * is;
+            F3 jA = f3(-(n2.x - ct * n1.x) * s1, -(n2.y - ct * n1.y) * s1, -(n2.z - ct * n1.z) * s1);
+            F3 jC = f3(-(n1.x - ct * n2.x) * s2, -(n1.y - ct * n2.y) * s2, -(n1.z - ct * n2.z) * s2);
+            jac[0] = jA; jac[1] = f3(-(jA.x + jC.x), -(jA.y + jC.y), -(jA.z + jC.z)); jac[2] = jC;
+        }
+        return th;
+    }
+    // dihedral, Blondel-Karplus
+    F3 pa = loadPos(posq, u2g, atoms[0]), pb = loadPos(posq, u2g, atoms[1]);
+    F3 pc = loadPos(posq, u2g, atoms[2]), pd = loadPos(posq, u2g, atoms[3]);
+    F3 b1 = minImage(sub3(pb, pa), box), b2 = minImage(sub3(pc, pb), box), b3 = minImage(sub3(pd, pc), box);
+    F3 t = cross3(b1, b2), u = cross3(b2, b3);
+    float d = sqrtf(dot3(b2, b2));
+    float phi = atan2f(d * dot3(b1, u), dot3(t, u));
+    if (jac) {
+        float t2 = dot3(t, t), u2 = dot3(u, u);
+        float it2 = t2 > 1e-10f ? 1.0f / t2 : 0.0f;
+        float iu2 = u2 > 1e-10f ? 1.0f / u2 : 0.0f;
+        float id = d > 1e-10f ? 1.0f / d : 0.0f;
+        float c1 = dot3(b1, b2) * id, c2 = dot3(b3, b2) * id;
+        float aT = d * it2, aU = d * iu2, bTB = (d + c1) * it2, bUB = c2 * iu2;
+        F3 jA = f3(-aT * t.x, -aT * t.y, -aT * t.z);
+        F3 jD = f3(aU * u.x, aU * u.y, aU * u.z);
+        F3 jB = f3(bTB * t.x + bUB * u.x, bTB * t.y + bUB * u.y, bTB * t.z + bUB * u.z);
+        jac[0] = jA; jac[1] = jB;
+        jac[2] = f3(-(jA.x + jB.x + jD.x), -(jA.y + jB.y + jD.y), -(jA.z + jB.z + jD.z));
+        jac[3] = jD;
+    }
+    return phi;
 }
 
 // Rational switch (1 - x^n)/(1 - x^m) for positive integer n, m evaluated as

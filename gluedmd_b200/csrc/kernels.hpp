@@ -13,8 +13,12 @@ void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const Gr
                     double* cvv, const JacDev& J);
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
                      int numAtoms, int mode, double scale, const BoxDev* box);
+// parts: bit 0 = pair kernel, bit 1 = finalize kernel
+// kind: switch kind shared by every item of the launch (3: n = 6, m = 12;
+// -1: other integer exponents; 0: non-integer exponents).
 void launchCoord(cudaStream_t s, const float4* posq, const int* u2g, const CoordDev& C, int numBlocks,
-                 int totalRows, int boxKind, int ra, const BoxDev* box, const JacDev& J, double* cvv);
+                 int totalRows, int boxKind, int ra, int kind, const BoxDev* box, const JacDev& J, double* cvv,
+                 int parts = 3);
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies);
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
@@ -23,5 +27,7 @@ void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, con
 void launchHillsDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
 void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies,
                        int* mergeFlag, double* partial, int nPartial);
+
+double measureFp32Peak();
 
 }  // namespace glued

@@ -360,6 +360,17 @@ class NativeContext:
         call("glued_context_opes_last_decision", self._h, int(idx), ctypes.byref(d))
         return d.value
 
+    def profile_phases(self, reps=20):
+        n = c_int(6)
+        out = (c_double * 6)()
+        call("glued_context_profile_phases", self._h, int(reps), out, ctypes.byref(n))
+        return list(out[:n.value])
+
+    def launch_count(self):
+        v = c_ll()
+        call("glued_context_launch_count", self._h, ctypes.byref(v))
+        return v.value
+
     def device_arrays(self):
         ptrs = [c_void_p() for _ in range(7)]
         nc, nr = c_int(), c_int()

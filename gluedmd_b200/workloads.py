@@ -49,7 +49,13 @@ def _cube(L):
 def wt_hill_heights(centers, sigma, period, h0, gamma, kT, chunk=512):
     """Sequential well-tempered heights: h_k = h0 exp(-V_{k-1}(c_k) / ((gamma-1) kT)),
     V_{k-1} the truncated (exponent <= 8) hill sum of the previous hills. O(K^2),
-    blocked so that only the within-block part is sequential."""
+    blocked so that only the within-block part is sequential. Large tables use
+    torch float64 (on the GPU when one is present)."""
+    if len(centers) > 4000:
+        try:
+            return _wt_hill_heights_torch(centers, sigma, period, h0, gamma, kT)
+        except ImportError:
+            pass
     c = np.asarray(centers, float)
     K, D = c.shape
     sig = np.asarray(sigma, float)
@@ -73,6 +79,69 @@ def wt_hill_heights(centers, sigma, period, h0, gamma, kT, chunk=512):
             V = Vpre[i] + (W[i, :i] @ h[s:s + i] if i else 0.0)
             h[s + i] = h0 * math.exp(-V * hif) if hif > 0 else h0
     return h
+
+
+def _wt_hill_heights_torch(centers, sigma, period, h0, gamma, kT, chunk=1024):
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    c = torch.as_tensor(np.asarray(centers, float), dtype=torch.float64, device=dev)
+    K, D = c.shape
+    sig = torch.as_tensor(np.asarray(sigma, float), dtype=torch.float64, device=dev)
+    per = [float(x) for x in period]
+    hif = 0.0 if gamma <= 1.0 else 1.0 / ((gamma - 1.0) * kT)
+    h = torch.zeros(K, dtype=torch.float64, device=dev)
+
+    def kern(a, b):
+        d = a[:, None, :] - b[None, :, :]
+        for k in range(D):
+            if per[k] > 0:
+                d[..., k] -= torch.round(d[..., k] / per[k]) * per[k]
+        ex = (d * d / (2.0 * sig * sig)).sum(-1)
+        return torch.where(ex <= 8.0, torch.exp(-ex), torch.zeros_like(ex))
+
+    for s in range(0, K, chunk):
+        e = min(K, s + chunk)
+        Vpre = kern(c[s:e], c[:s]) @ h[:s] if s > 0 else torch.zeros(e - s, dtype=torch.float64, device=dev)
+        Wm = kern(c[s:e], c[s:e]).cpu().numpy()
+        Vp = Vpre.cpu().numpy()
+        hb = np.zeros(e - s)
+        for i in range(e - s):
+            V = Vp[i] + (Wm[i, :i] @ hb[:i] if i else 0.0)
+            hb[i] = h0 * math.exp(-V * hif) if hif > 0 else h0
+        h[s:e] = torch.as_tensor(hb, dtype=torch.float64, device=dev)
+    return h.cpu().numpy()
+
+
+def grid_from_hills_windowed(centers, heights, sigma, origin, maxv, bins, periodic):
+    """Same grid as grid_from_hills, touching only each hill's +-4 sigma window."""
+    D = len(bins)
+    assert D == 2
+    npts = [bins[d] + (0 if periodic[d] else 1) for d in range(D)]
+    inv = [bins[d] / (maxv[d] - origin[d]) for d in range(D)]
+    grid = np.zeros((npts[1], npts[0]))
+    wins = []
+    for d in range(D):
+        half = int(math.ceil(4.0 * sigma[d] * inv[d])) + 1
+        wins.append(np.arange(-half, half + 1))
+    for c, h in zip(np.asarray(centers, float), heights):
+        idx, dcs = [], []
+        for d in range(D):
+            b0 = int(math.floor((c[d] - origin[d]) * inv[d]))
+            bi = b0 + wins[d]
+            if periodic[d]:
+                bi = np.unique(bi % npts[d])
+            else:
+                bi = bi[(bi >= 0) & (bi < npts[d])]
+            pos = origin[d] + bi / inv[d]
+            dc = pos - c[d]
+            if periodic[d]:
+                L = npts[d] / inv[d]
+                dc = dc - np.round(dc / L) * L
+            idx.append(bi)
+            dcs.append(dc * dc / (2.0 * sigma[d] * sigma[d]))
+        ex = dcs[1][:, None] + dcs[0][None, :]
+        grid[np.ix_(idx[1], idx[0])] += np.where(ex <= 8.0, h * np.exp(-ex), 0.0)
+    return grid.ravel()
 
 
 def grid_from_hills(centers, heights, sigma, origin, maxv, bins, periodic):

@@ -150,42 +150,68 @@ int glued_context_set_multiwalker_ptrs(glued_context* c, int bias_index, const l
 int glued_context_device_arrays(glued_context* c, void** cv_values, void** dudcv, void** jac_atom,
                                 void** jac_gx, void** jac_gy, void** jac_gz, void** jac_cv,
                                 int* num_cvs, int* num_rows);
+/* Measurement hooks (no reference counterpart). profile_phases times each launch
+ * group of execute() separately with CUDA events on the bound stream, reps
+ * launches each: out[i] = mean ms of phase i in the order simple CVs, group CVs,
+ * coordination pairs, coordination finalize, biases, scatter (*n in/out).
+ * launch_count = kernels this context enqueued so far (graph replays count
+ * their kernel nodes).                                                        */
+int glued_context_profile_phases(glued_context* c, int reps, double* out, int* n);
+int glued_context_launch_count(glued_context* c, long long* count);
+/* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 flops),
+ * measured with a register-resident FMA-chain kernel (synchronizing).         */
+int glued_measure_fp32_peak(double* tflops);
 /* Test hook: index of the last OPES deposit decision of OPES bias opes_index
  * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
 int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);
 
 /* ----------------------------------------------------------------------- batch
- * Many walkers on one GPU evaluated by one persistent launch per step (no
- * reference counterpart as a kernel: it replaces the reference's one-Context-
- * per-walker stepping, tests/test_multiwalker.py:156-158, and its shared-bias
- * pointer aliasing, CommonGluedKernels.cpp:5234-5262).                          */
+ * Many walkers on one GPU evaluated by one cooperative persistent launch per step
+ * (no reference counterpart as a kernel: it replaces the reference's
+ * one-Context-per-walker stepping, tests/test_multiwalker.py:156-158, and its
+ * shared-bias pointer aliasing, CommonGluedKernels.cpp:5234-5262).
+ * Scope: distance, angle, dihedral and coordination CVs; HARMONIC biases per
+ * walker; at most one METAD_HILLS bias (<= 2 CVs, on distance/angle/dihedral
+ * CVs) whose hill table is shared by all walkers (parameters of walker 0). */
 typedef struct glued_walker_desc {
-    const void* posq;          /* float4[num_atoms] device */
-    long long* force_buffer;   /* int64[3 * padded] device */
+    const void* posq;          /* float4[padded] device; slot order = user atom order */
+    long long* force_buffer;   /* int64[3 * padded] device, += 2^32 fixed point */
     int num_atoms;
     int padded_num_atoms;
-    double box[9];
+    double box[9];             /* a, b, c (nm) */
 } glued_walker_desc;
 
-/* All walkers share one force descriptor (same CV/bias specs, user atom indices
- * valid for every walker) and one hill table for their METAD_HILLS bias.        */
-int glued_batch_create(const glued_force* f, int num_walkers, const glued_walker_desc* walkers,
-                       const double* masses, glued_batch** out);
+/* forces[w] describes walker w. Every walker must have the same CV and bias
+ * structure (types, order, coordination group sizes); atoms and parameters may
+ * differ per walker. The descriptors are copied.                               */
+int glued_batch_create(const glued_force* const* forces, int num_walkers, const glued_walker_desc* walkers,
+                       glued_batch** out);
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
-/* Tile choice for the pair kernels; 0 = autotuned. Synchronizing when tuning.   */
-int glued_batch_autotune(glued_batch* b, int* chosen_tile);
-/* One step for all walkers: CVs, bias, scatter (one launch, graph-replayed). */
+/* Tiling of the persistent launch: tune[4] = {ra (4|8), b_split (multiple of
+ * 128), hill_items, parts}. autotune times every candidate on the live walkers
+ * (forces of the trial launches go to a scratch buffer), keeps the fastest and
+ * returns it in tune (synchronizing).                                          */
+int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
+int glued_batch_get_tuning(glued_batch* b, int tune[4]);
+int glued_batch_autotune(glued_batch* b, int tune[4]);
+/* One step for all walkers: CVs, biases and force scatter (one launch,
+ * graph-replayed). Forces are added to each walker's buffer.                  */
 int glued_batch_execute(glued_batch* b);
+/* Deposition at pace (once per step, after the step's first execute): one hill
+ * per walker, walker order.                                                    */
 int glued_batch_update_state(glued_batch* b, int step);
-/* energies: double[num_walkers]; cv_values: double[num_walkers * numCV].        */
+/* energies: double[num_walkers]; cv_values: double[num_walkers * num_cvs].     */
 int glued_batch_get_energies(glued_batch* b, double* energies);
 int glued_batch_get_cv_values(glued_batch* b, double* cv_values);
-/* Hill table of the shared METAD_HILLS bias: read count / centres / heights.     */
+int glued_batch_num_cvs(glued_batch* b, int* n);
+/* Shared hill table: count, load (replace) and read back (centres n*D, heights n). */
 int glued_batch_num_hills(glued_batch* b, int* n);
 int glued_batch_set_hills(glued_batch* b, const double* centers, const double* heights, int n);
-/* Status word of the persistent kernel's bounded grid barrier (0 = ok).         */
+int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int n);
+/* Status word of the bounded waits (0 = ok; bit 0 grid barrier, bit 1 bulk copy). */
 int glued_batch_status(glued_batch* b, int* status);
+int glued_batch_launch_count(glued_batch* b, long long* count);
 
 #ifdef __cplusplus
 }

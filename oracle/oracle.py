@@ -447,6 +447,49 @@ class OracleSystem:
                 st["centers"] = np.vstack([st["centers"], center[None, :]])
                 st["heights"] = np.append(st["heights"], h)
 
+    def load_blob(self, blob: bytes):
+        """Restore OPES / MetaD / hill-sum state from a 'GPUS' v1 bias-state blob
+        (CommonSerialization.cpp:180-290 reader; hill section of this library)."""
+        import struct
+        p = 0
+        if blob[:4] == b"GPUS":
+            p = 8
+        nb, = struct.unpack_from("<i", blob, p); p += 4
+        opes = [st for st in self.bias_state if st["type"] == BIAS_OPES]
+        assert nb == len(opes)
+        for st in opes:
+            D = st["D"]
+            nk, su, ns = struct.unpack_from("<idi", blob, p); p += 16
+            arr = np.frombuffer(blob, "<f8", count=2 * D + 2 * nk * D + nk, offset=p).copy()
+            p += 8 * len(arr)
+            st["mean"][:] = arr[:D]; st["m2"][:] = arr[D:2 * D]
+            st["centers"][:nk * D] = arr[2 * D:2 * D + nk * D]
+            st["sigmas"][:nk * D] = arr[2 * D + nk * D:2 * D + 2 * nk * D]
+            st["logw"][:nk] = arr[2 * D + 2 * nk * D:]
+            st["ist"][0] = nk; st["ist"][1] = ns; st["ist"][3] = nk
+            st["dst"][0] = su
+            st["dst"][1] = math.exp(-st["gamma"]) + float(np.exp(st["logw"][:nk]).sum())
+            st["nker_cpu"] = nk; st["nsamp_cpu"] = ns
+        if p < len(blob):
+            p += 4  # ABMD count (0)
+        if p < len(blob):
+            nm, = struct.unpack_from("<i", blob, p); p += 4
+            for st in [s_ for s_ in self.bias_state if s_["type"] == BIAS_METAD]:
+                nd, = struct.unpack_from("<i", blob, p); p += 4
+                st["grid"][:] = np.frombuffer(blob, "<f8", count=st["total"], offset=p)
+                p += 8 * st["total"]
+                st["deposited"] = nd
+        p += 36
+        if blob[p:p + 4] == b"HILL":
+            p += 8
+            for st in [s_ for s_ in self.bias_state if s_["type"] == BIAS_METAD_HILLS]:
+                n, = struct.unpack_from("<i", blob, p); p += 4
+                D = st["D"]
+                st["centers"] = np.frombuffer(blob, "<f8", count=n * D, offset=p).reshape(n, D).copy()
+                p += 8 * n * D
+                st["heights"] = np.frombuffer(blob, "<f8", count=n, offset=p).copy()
+                p += 8 * n
+
     def welford(self):
         """Per-execute Welford update for fully adaptive OPES (CommonGluedKernels.cpp:4976-4981)."""
         L = lib()

@@ -1,0 +1,131 @@
+"""Batched multi-walker path vs the FP64 oracle evaluated walker by walker.
+
+Gate: forces within 1e-4 relative (max-norm) of the FP64 oracle per walker, CV
+values within 1e-5 relative, energies within 1e-4 relative; deposition centres
+bit-exact (they are the walkers' CV values), heights to 1e-13 relative."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _walkers(n_walkers=6, n_hills=3000, coord=(64, 256), seed=8):
+    from gluedmd_b200 import workloads as W
+    ws, hill = W.config4_walkers(n_walkers=n_walkers, n_hills=n_hills, coord=coord)
+    return ws, hill
+
+
+def _setup(ws, hill, with_hills=True, coord_restraint=True):
+    import torch
+    from gluedmd_b200.batch import Batch, Walker, force_for, c4_biases
+    from gluedmd_b200 import workloads as W
+    forces, walkers, specs = [], [], []
+    for w in ws:
+        cn0 = W.coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"]) if coord_restraint else None
+        # restraint centres away from the current values, so that dU/dCV is not a
+        # difference of nearly equal numbers (forces would be pure rounding noise)
+        wr = dict(w, d0=w["d0"] + 0.05)
+        biases = c4_biases(wr, hill["params"], hill["iparams"], cn0=None if cn0 is None else cn0 + 2.0)
+        if not with_hills:
+            biases = [b for b in biases if b[0] != 103]
+        forces.append(force_for(w["cvs"], biases))
+        walkers.append(Walker(w["pos"], w["box"]))
+        specs.append(biases)
+    b = Batch(forces, walkers)
+    if with_hills:
+        b.set_hills(hill["centers"], hill["heights"])
+    return b, walkers, specs
+
+
+def _oracle(w, biases, hill):
+    s = O.OracleSystem(w["cvs"], biases, masses=w["masses"], periodic=True, mode="f64", num_particles=w["n"])
+    for st in s.bias_state:
+        if st["type"] == O.BIAS_METAD_HILLS:
+            st["centers"] = np.array(hill["centers"], float)
+            st["heights"] = np.array(hill["heights"], float)
+    return s
+
+
+@pytest.mark.parametrize("with_hills", [False, True])
+def test_batch_matches_fp64_oracle(with_hills):
+    ws, hill = _walkers()
+    b, walkers, specs = _setup(ws, hill, with_hills)
+    for wk in walkers:
+        wk.force.zero_()
+    b.execute()
+    E = b.energies()
+    cv = b.cv_values()
+    assert b.status() == 0
+    for i, w in enumerate(ws):
+        r = _oracle(w, specs[i], hill).execute(w["pos"], w["box"].ravel())
+        np.testing.assert_allclose(cv[i], r["cv_values"], rtol=1e-5, atol=1e-5)
+        # energies carry restraint-amplified FP32 CV error: k * (s - s0) * dCV
+        assert abs(E[i] - r["energy"]) <= 1e-4 * max(1.0, abs(r["energy"])), (i, E[i], r["energy"])
+        err = O.max_rel_force_err(walkers[i].forces(), r["forces"])
+        assert err < 1e-4, (i, err)
+
+
+def test_batch_repeatable_and_autotuned():
+    ws, hill = _walkers(n_walkers=5)
+    b, walkers, specs = _setup(ws, hill, True)
+    for wk in walkers:
+        wk.force.zero_()
+    b.execute()
+    f1 = [w.forces() for w in walkers]
+    for wk in walkers:
+        wk.force.zero_()
+    b.execute()
+    f2 = [w.forces() for w in walkers]
+    for a, c in zip(f1, f2):
+        assert np.array_equal(a, c)  # deterministic reductions: bitwise repeatable
+    t = b.autotune()
+    assert t["ra"] in (4, 8) and t["b_split"] % 128 == 0
+    for wk in walkers:
+        wk.force.zero_()
+    b.execute()
+    for i, w in enumerate(walkers):
+        assert O.max_rel_force_err(w.forces(), f1[i]) < 2e-6
+    assert b.status() == 0
+
+
+def test_batch_deposit_walker_order():
+    ws, hill = _walkers(n_walkers=4, n_hills=500)
+    hill["iparams"] = [2, 100000, 1, 0]  # pace 2
+    b, walkers, specs = _setup(ws, hill, True, coord_restraint=False)
+    n0 = b.num_hills()
+    b.update_state(0)        # nothing before the first execute
+    b.execute()
+    cv = b.cv_values()
+    E = b.energies()
+    b.update_state(1)        # not a pace step
+    assert b.num_hills() == n0
+    b.update_state(2)
+    assert b.num_hills() == n0 + 4
+    b.update_state(2)        # once per step
+    assert b.num_hills() == n0 + 4
+    c, h = b.get_hills()
+    hif = 1.0 / ((10.0 - 1.0) * 2.494338785)
+    for i in range(4):
+        assert c[n0 + i, 0] == cv[i, 2] and c[n0 + i, 1] == cv[i, 1]
+        # hill-bias energy of walker i = its energy minus the distance restraint
+        d = cv[i, 0] - np.float32(ws[i]["d0"] + 0.05)
+        Vh = E[i] - 0.5 * 100.0 * d * d
+        assert abs(h[n0 + i] - 1.2 * math.exp(-Vh * hif)) < 1e-9
+
+
+def test_batch_rejects_unsupported_structure():
+    from gluedmd_b200.batch import Batch, Walker, force_for
+    from gluedmd_b200 import GluedError
+    import numpy as np
+    pos = np.random.default_rng(0).uniform(0, 2, (20, 3))
+    f = force_for([(5, list(range(10)), [])], [])
+    with pytest.raises(GluedError, match="not supported"):
+        Batch([f], [Walker(pos, np.eye(3) * 2)])
+    f1 = force_for([(1, [0, 1], [])], [])
+    f2 = force_for([(2, [0, 1, 2], [])], [])
+    with pytest.raises(GluedError, match="type differs|different"):
+        Batch([f1, f2], [Walker(pos, np.eye(3) * 2), Walker(pos, np.eye(3) * 2)])
