@@ -81,6 +81,8 @@ _SIGS = {
     "glued_context_profile_phases": [c_void_p, c_int, P(c_double), P(c_int)],
     "glued_context_launch_count": [c_void_p, P(c_ll)],
     "glued_measure_fp32_peak": [P(c_double)],
+    "glued_coordination_noalloc": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double,
+                                   c_double, c_int, P(c_double), c_void_p, c_void_p],
     "glued_batch_create": [P(c_void_p), c_int, P(WalkerDesc), P(c_void_p)],
     "glued_batch_destroy": [c_void_p],
     "glued_batch_set_stream": [c_void_p, c_void_p],

@@ -306,6 +306,14 @@ int glued_context_launch_count(glued_context* c, long long* count) {
 int glued_measure_fp32_peak(double* tflops) {
     return guard([&] { need(tflops, "out"); *tflops = glued::measureFp32Peak(); });
 }
+int glued_coordination_noalloc(void* stream, const void* posq, const int* group_a, int n_a, const int* group_b,
+                               int n_b, double r0, double n, double m, int periodic, const double box[9],
+                               double* cn_out, float* grad_out) {
+    return guard([&] {
+        glued::coordinationNoAlloc((cudaStream_t)stream, posq, group_a, n_a, group_b, n_b, r0, n, m, periodic, box,
+                                   cn_out, grad_out);
+    });
+}
 int glued_context_opes_last_decision(glued_context* c, int idx, int* decision) {
     return guard([&] { need(c, "context"); need(decision, "out"); *decision = c->c->opesLastDecision(idx); });
 }

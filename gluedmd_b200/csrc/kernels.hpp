@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include "../../include/glued_b200.h"
 #include "dev.hpp"
 
 namespace glued {
@@ -29,5 +30,8 @@ void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, cons
                        int* mergeFlag, double* partial, int nPartial);
 
 double measureFp32Peak();
+void coordinationNoAlloc(cudaStream_t stream, const void* posq, const int* groupA, int nA, const int* groupB, int nB,
+                         double r0, double n, double m, int periodic, const double* box9, double* cnOut,
+                         float* gradOut);
 
 }  // namespace glued

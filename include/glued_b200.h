@@ -165,6 +165,34 @@ int glued_measure_fp32_peak(double* tflops);
  * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
 int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);
 
+/* ------------------------------------------------------ no-allocation variant
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory while they evaluate forces (an engine that reserves all device memory
+ * at start-up and forbids cudaMalloc in its step loop, or that manages the
+ * device heap with its own allocator): one coordination CV evaluated with its
+ * tile partials in a fixed array that is part of this library's device image,
+ * GLUED_NOALLOC_SCRATCH_BYTES (4 MiB) per GPU, resident on every GPU that
+ * loads the library until the process exits. The call allocates nothing:
+ * no cudaMalloc, no cudaFree, no allocating library routine.
+ *   posq       float4[...] device positions (slot order)
+ *   group_a/b  int device arrays of slot indices, n_a and n_b entries
+ *   r0, n, m   rational switch (1 - (r/r0)^n) / (1 - (r/r0)^m), no cutoff
+ *   periodic   minimum image in box[9] (a, b, c; host array) when non-zero
+ *   cn_out     device double[1]: the coordination number
+ *   grad_out   device float[3 * (n_a + n_b)]: dCN/dx, component-major
+ *              (x of all rows, then y, then z), rows = group A then group B
+ * Sizes whose partials exceed the array are rejected with GLUED_E_INVALID
+ * (about 2,048 x 8,192 atoms fit). The first call on a device looks up the
+ * array's device address (which may load the module): make it before any
+ * stream capture. Every call shares the one array and leaves its contents
+ * behind; nothing in it needs to start at zero. Calls whose work overlaps on
+ * the GPU (different streams, or a second call before the first finished on
+ * another stream) race on the array and corrupt each other's results.     */
+#define GLUED_NOALLOC_SCRATCH_BYTES 4194304
+int glued_coordination_noalloc(void* stream, const void* posq, const int* group_a, int n_a, const int* group_b,
+                               int n_b, double r0, double n, double m, int periodic, const double box[9],
+                               double* cn_out, float* grad_out);
+
 /* ----------------------------------------------------------------------- batch
  * Many walkers on one GPU evaluated by one cooperative persistent launch per step
  * (no reference counterpart as a kernel: it replaces the reference's
