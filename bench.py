@@ -116,11 +116,14 @@ def time_steps(torch, step_fn, steps, warmup, flush):
     torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    # NVTX range "timed": lets a profiler restrict its launch list to these steps
+    torch.cuda.nvtx.range_push("timed")
     for i in range(steps):
         flush.add_(1.0)
         starts[i].record(stream)
         step_fn(warmup + i)
         ends[i].record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
@@ -217,9 +220,10 @@ def c4_biases(w, hill):
 
 
 def run_c4(args, torch, ws, hill):
-    from gluedmd_b200.batch import Batch, Walker, force_for
+    from gluedmd_b200.batch import Batch, WalkerPool, force_for
     forces = [force_for(w["cvs"], c4_biases(w, hill)) for w in ws]
-    walkers = [Walker(w["pos"], w["box"]) for w in ws]
+    pool = WalkerPool([w["pos"] for w in ws], [w["box"] for w in ws])
+    walkers = pool.walkers
     b = Batch(forces, walkers)
     b.set_hills(hill["centers"], hill["heights"])
     tune = b.autotune()
@@ -266,20 +270,18 @@ def run_c4(args, torch, ws, hill):
     del plain_ctx
     # e2e through the C ABI with host buffers: every walker's positions H2D from
     # pinned memory, one step, every force buffer and the energies D2H
-    host_pos = [torch.zeros_like(wk.posq, device="cpu").pin_memory() for wk in walkers]
-    host_f = [torch.zeros_like(wk.force, device="cpu").pin_memory() for wk in walkers]
-    for hp, wk in zip(host_pos, walkers):
-        hp.copy_(wk.posq)
+    # one pooled buffer per direction: all walkers' positions in, all forces out
+    host_pos = torch.zeros_like(pool.posq, device="cpu").pin_memory()
+    host_f = torch.zeros_like(pool.force, device="cpu").pin_memory()
+    host_pos.copy_(pool.posq)
     stream = torch.cuda.current_stream()
 
     def e2e_step(i):
-        for hp, wk in zip(host_pos, walkers):
-            wk.posq.copy_(hp, non_blocking=True)
-            wk.force.zero_()
+        pool.posq.copy_(host_pos, non_blocking=True)
+        pool.force.zero_()
         b.update_state(10 ** 6 + i)
         b.execute()
-        for hf, wk in zip(host_f, walkers):
-            hf.copy_(wk.force, non_blocking=True)
+        host_f.copy_(pool.force, non_blocking=True)
         return b.energies()  # synchronizing read of the per-walker energies
 
     for i in range(args.warmup):
@@ -292,8 +294,8 @@ def run_c4(args, torch, ws, hill):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    h2d = sum(hp.numel() * 4 for hp in host_pos)
-    d2h = sum(hf.numel() * 8 for hf in host_f) + 8 * W_
+    h2d = host_pos.numel() * 4
+    d2h = host_f.numel() * 8 + 8 * W_
     pairs = sum(256 * 1024 for _ in ws)
     flops = pairs * FLOP_PAIR + W_ * b.num_hills() * FLOP_HILL
     return dict(walkers=W_, step_ms=step_ms, value=W_ * 1e3 / step_ms, plain_ms=plain_ms,
@@ -359,6 +361,11 @@ def main():
     ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: warm-up + timed steps only, fixed tiling, no baselines (for ncu)")
+    ap.add_argument("--walkers", type=int, default=64, help="C4 walker count (profiling of small cases)")
+    ap.add_argument("--hills", type=int, default=50000, help="C4 hill count (profiling of small cases)")
+    ap.add_argument("--tuning", default="8,512,128,4", help="fixed C4 tiling ra,b_split,hill_items,parts (--profile)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -404,6 +411,20 @@ def main():
     from gluedmd_b200 import _native
     import ctypes
     pk, src = peaks()
+
+    if args.config == "c4" and args.profile:
+        ws, hill = c4_inputs(args.walkers, args.hills)
+        from gluedmd_b200.batch import Batch, WalkerPool, force_for
+        pool = WalkerPool([w["pos"] for w in ws], [w["box"] for w in ws])
+        b = Batch([force_for(w["cvs"], c4_biases(w, hill)) for w in ws], pool.walkers)
+        b.set_hills(hill["centers"], hill["heights"])
+        ra, bs, hi, parts = (int(x) for x in args.tuning.split(","))
+        b.set_tuning(ra, bs, hi, parts)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        ms = time_steps(torch, lambda i: (b.update_state(i), b.execute()), args.steps, args.warmup, flush)
+        print(json.dumps({"profile": "c4", "walkers": args.walkers, "hills": b.num_hills(), "ms_per_step": ms / args.steps,
+                          "status": b.status(), "tuning": b.tuning}))
+        return
 
     if args.config == "c4":
         ws, hill = c4_inputs()

@@ -81,6 +81,9 @@ _SIGS = {
     "glued_context_profile_phases": [c_void_p, c_int, P(c_double), P(c_int)],
     "glued_context_launch_count": [c_void_p, P(c_ll)],
     "glued_measure_fp32_peak": [P(c_double)],
+    "glued_ad_forward": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int],
+    "glued_ad_backward": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                          c_void_p],
     "glued_coordination_noalloc": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double,
                                    c_double, c_int, P(c_double), c_void_p, c_void_p],
     "glued_batch_create": [P(c_void_p), c_int, P(WalkerDesc), P(c_void_p)],
@@ -99,6 +102,7 @@ _SIGS = {
     "glued_batch_get_hills": [c_void_p, P(c_double), P(c_double), c_int],
     "glued_batch_status": [c_void_p, P(c_int)],
     "glued_batch_launch_count": [c_void_p, P(c_ll)],
+    "glued_batch_phase_times": [c_void_p, P(c_double)],
 }
 
 

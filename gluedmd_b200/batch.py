@@ -35,6 +35,30 @@ class Walker:
         return f.T.copy()
 
 
+class WalkerPool:
+    """Walkers whose posq and force buffers are views into one allocation each,
+    so all positions move host->device in one copy and all forces back in one."""
+
+    def __init__(self, positions_list, boxes, device="cuda", padding=32):
+        ns = [len(np.asarray(p).reshape(-1, 3)) for p in positions_list]
+        pads = [((n + padding - 1) // padding) * padding for n in ns]
+        self.offsets = np.concatenate([[0], np.cumsum(pads)]).astype(np.int64)
+        total = int(self.offsets[-1])
+        self.posq = torch.zeros((total, 4), dtype=torch.float32, device=device)
+        self.force = torch.zeros(3 * total, dtype=torch.int64, device=device)
+        self.walkers = []
+        for i, (p, box) in enumerate(zip(positions_list, boxes)):
+            w = Walker.__new__(Walker)
+            w.n, w.padded = ns[i], pads[i]
+            o = int(self.offsets[i])
+            w.posq = self.posq[o:o + pads[i]]
+            w.force = self.force[3 * o:3 * (o + pads[i])]
+            w.posq[: w.n, :3] = torch.as_tensor(np.asarray(p, dtype=np.float64).reshape(-1, 3),
+                                                dtype=torch.float32, device=device)
+            w.box = np.asarray(box, dtype=np.float64).reshape(3, 3)
+            self.walkers.append(w)
+
+
 class Batch:
     def __init__(self, forces, walkers, stream=None):
         if len(forces) != len(walkers):
@@ -118,6 +142,14 @@ class Batch:
         v = c_ll()
         call("glued_batch_launch_count", self._h, ctypes.byref(v))
         return v.value
+
+    def phase_times(self):
+        """One step with per-CTA timestamps: dict of phase ends (us) and item counts."""
+        out = (c_double * 8)()
+        call("glued_batch_phase_times", self._h, out)
+        return dict(phase_a_end_min_us=out[0], phase_a_end_max_us=out[1], barrier_exit_us=out[2],
+                    end_us=out[3], coord_items=int(out[4]), hill_items=int(out[5]),
+                    items_per_cta_max=int(out[6]), items_per_cta_min=int(out[7]))
 
     @property
     def tuning(self):

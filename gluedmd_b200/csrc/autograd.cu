@@ -1,0 +1,215 @@
+// Differentiable bias: contact map + path CV + hill bias on (CMAP, s), with a
+// hand-written backward that gives dE/d(positions), dE/d(r0), dE/d(frames) and
+// dE/d(heights). No reference counterpart as a whole (GLUED has no autograd);
+// the CV definitions are the reference's contact map (CommonGluedKernels.cpp:
+// 1236-1323) and path CV (:641-794).
+//
+//   CMAP = sum_p w_p s_p,  s_p = (1 - x^n)/(1 - x^m), x = d_p / r0_p
+//          (integer n, m: evaluated as S_n(x)/S_m(x), the cancellation-free form)
+//   w_f  = exp(-lambda MSD_f), MSD_f = sum_j |x_j - ref_fj|^2 / M
+//   s    = sum_f (f+1) w_f / S, z = -ln(S)/lambda, S = sum_f w_f
+//   E    = sum_k h_k exp(-(CMAP - c_k0)^2/(2 sig0^2) - (s - c_k1)^2/(2 sig1^2))
+//
+// The backward recomputes every per-pair switching value instead of storing it.
+// Position gradients are summed as 2^40 fixed point with 64-bit integer atomics
+// (order independent, so bitwise repeatable) and converted once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "../../include/glued_b200.h"
+#include "context.hpp"
+#include "devfn.cuh"
+#include "kernels.hpp"
+
+namespace glued {
+
+// The spec crosses the C ABI as glued_ad_spec (include/glued_b200.h).
+typedef glued_ad_spec AdSpec;
+
+namespace {
+constexpr double kFix = 1099511627776.0;  // 2^40
+
+template <class R>
+__device__ __forceinline__ void ratioSwitchT(R x, int n, int m, R& f, R& dfdx) {
+    R sn = 0, dsn = 0, sm = 0, dsm = 0;
+    for (int j = n - 1; j >= 0; j--) { dsn = dsn * x + sn; sn = sn * x + (R)1; }
+    for (int j = m - 1; j >= 0; j--) { dsm = dsm * x + sm; sm = sm * x + (R)1; }
+    R ism = (R)1 / sm;
+    f = sn * ism;
+    dfdx = (dsn * sm - sn * dsm) * ism * ism;
+}
+
+template <class R>
+__device__ __forceinline__ void pairGeom(const AdSpec& S, int p, R& d, R dr[3]) {
+    const R* pos = static_cast<const R*>(S.pos);
+    int a = S.pairs[2 * p], b = S.pairs[2 * p + 1];
+    for (int c = 0; c < 3; c++) {
+        R x = pos[3 * b + c] - pos[3 * a + c];
+        if (S.periodic) x -= (R)S.box[c] * floor(x / (R)S.box[c] + (R)0.5);
+        dr[c] = x;
+    }
+    d = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+}
+}  // namespace
+
+// out: [0] E, [1] CMAP, [2] s, [3] z, [4] S, [5..5+F) w_f; part: per-CTA CMAP partials
+template <class R>
+__global__ void k_ad_cmap(AdSpec S, double* part) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    const R* r0 = static_cast<const R*>(S.r0);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S.nPairs; p += gridDim.x * blockDim.x) {
+        R d, dr[3];
+        pairGeom<R>(S, p, d, dr);
+        R x = d / r0[p], f, dfdx;
+        ratioSwitchT<R>(x, (int)S.nmw[3 * p], (int)S.nmw[3 * p + 1], f, dfdx);
+        acc += (double)((R)S.nmw[3 * p + 2] * f);
+    }
+    double v[1] = {acc};
+    blockSum<1>(v, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+template <class R>
+__global__ void k_ad_path_hills(AdSpec S, const double* part, int nPart, double* out) {
+    __shared__ double red[32 * 3];
+    __shared__ double sw[128];
+    __shared__ double bc[4];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const R* pos = static_cast<const R*>(S.pos);
+    const R* fr = static_cast<const R*>(S.frames);
+    for (int f = warp; f < S.F; f += nw) {
+        double acc = 0.0;
+        for (int j = lane; j < S.M; j += 32) {
+            int a = S.pathAtoms[j];
+            for (int c = 0; c < 3; c++) {
+                R dx = pos[3 * a + c] - fr[((size_t)f * S.M + j) * 3 + c];
+                acc += (double)(dx * dx);
+            }
+        }
+        acc = warpSum(acc);
+        if (lane == 0) sw[f] = exp(-S.lambda * acc / S.M);
+    }
+    if (tid == 0) {
+        double cm = 0;
+        for (int k = 0; k < nPart; k++) cm += part[k];
+        double Ssum = 0, sn = 0;
+        for (int f = 0; f < S.F; f++) { Ssum += sw[f]; sn += (f + 1) * sw[f]; }
+        bc[0] = cm;
+        bc[1] = sn / Ssum;
+        bc[2] = -log(Ssum) / S.lambda;
+        bc[3] = Ssum;
+    }
+    __syncthreads();
+    const double cm = bc[0], s = bc[1];
+    const R* h = static_cast<const R*>(S.heights);
+    double v[3] = {0, 0, 0};
+    for (int k = tid; k < S.K; k += blockDim.x) {
+        double d0 = cm - S.hillC[2 * k], d1 = s - S.hillC[2 * k + 1];
+        double g = (double)h[k] * exp(-d0 * d0 / (2 * S.sig[0] * S.sig[0]) - d1 * d1 / (2 * S.sig[1] * S.sig[1]));
+        v[0] += g;
+        v[1] += -g * d0 / (S.sig[0] * S.sig[0]);
+        v[2] += -g * d1 / (S.sig[1] * S.sig[1]);
+    }
+    blockSum<3>(v, red);
+    if (tid == 0) {
+        out[0] = v[0]; out[1] = cm; out[2] = s; out[3] = bc[2]; out[4] = bc[3];
+        out[5 + S.F] = v[1];      // dE/dCMAP
+        out[6 + S.F] = v[2];      // dE/ds
+    }
+    for (int f = tid; f < S.F; f += blockDim.x) out[5 + f] = sw[f];
+}
+
+// gE: device scalar dL/dE. Position gradient accumulates into fixed-point acc.
+template <class R>
+__global__ void k_ad_back_pairs(AdSpec S, const double* out, const double* gE, long long* acc, R* gR0) {
+    const R* r0 = static_cast<const R*>(S.r0);
+    const double gC = gE[0] * out[5 + S.F];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S.nPairs; p += gridDim.x * blockDim.x) {
+        R d, dr[3];
+        pairGeom<R>(S, p, d, dr);
+        R x = d / r0[p], f, dfdx;
+        ratioSwitchT<R>(x, (int)S.nmw[3 * p], (int)S.nmw[3 * p + 1], f, dfdx);
+        const double w = S.nmw[3 * p + 2];
+        // dCMAP/dd = w dfdx / r0; dd/dr_b = dr/d
+        const double coef = gC * w * (double)dfdx / (double)r0[p] / (double)d;
+        int a = S.pairs[2 * p], b = S.pairs[2 * p + 1];
+        for (int c = 0; c < 3; c++) {
+            long long q = __double2ll_rn(coef * (double)dr[c] * kFix);
+            atomicAdd(reinterpret_cast<unsigned long long*>(acc + 3 * b + c), (unsigned long long)q);
+            atomicAdd(reinterpret_cast<unsigned long long*>(acc + 3 * a + c), (unsigned long long)(-q));
+        }
+        // dCMAP/dr0 = w dfdx * (-x / r0)
+        gR0[p] = (R)(gC * w * (double)dfdx * (-(double)x / (double)r0[p]));
+    }
+}
+
+template <class R>
+__global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, long long* acc, R* gFrames) {
+    const R* pos = static_cast<const R*>(S.pos);
+    const R* fr = static_cast<const R*>(S.frames);
+    const double gS = gE[0] * out[6 + S.F];
+    const double s = out[2], Ssum = out[4];
+    const double* w = out + 5;
+    const double sc = 2.0 * S.lambda / (S.M * Ssum);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < S.M * S.F; t += gridDim.x * blockDim.x) {
+        // thread per (frame, atom): d s / d ref_fj = sc (f+1-s) w_f (x_j - ref_fj)
+        int f = t / S.M, j = t % S.M;
+        int a = S.pathAtoms[j];
+        double k = gS * sc * ((f + 1) - s) * w[f];
+        for (int c = 0; c < 3; c++) {
+            double dx = (double)pos[3 * a + c] - (double)fr[((size_t)f * S.M + j) * 3 + c];
+            gFrames[((size_t)f * S.M + j) * 3 + c] = (R)(k * dx);
+            // d s / d x_j = -(that), summed over frames into the atom's gradient
+            long long q = __double2ll_rn(-k * dx * kFix);
+            atomicAdd(reinterpret_cast<unsigned long long*>(acc + 3 * a + c), (unsigned long long)q);
+        }
+    }
+}
+
+template <class R>
+__global__ void k_ad_back_hills_and_convert(AdSpec S, const double* out, const double* gE, const long long* acc,
+                                            R* gPos, R* gH) {
+    const double cm = out[1], s = out[2];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.K; k += gridDim.x * blockDim.x) {
+        double d0 = cm - S.hillC[2 * k], d1 = s - S.hillC[2 * k + 1];
+        gH[k] = (R)(gE[0] * exp(-d0 * d0 / (2 * S.sig[0] * S.sig[0]) - d1 * d1 / (2 * S.sig[1] * S.sig[1])));
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * S.nAtoms; i += gridDim.x * blockDim.x)
+        gPos[i] = (R)((double)acc[i] / kFix);
+}
+
+template <class R>
+void adForwardT(cudaStream_t st, const AdSpec& S, double* out, double* part, int nPart) {
+    k_ad_cmap<R><<<nPart, 256, 0, st>>>(S, part);
+    k_ad_path_hills<R><<<1, 512, 0, st>>>(S, part, nPart, out);
+}
+
+template <class R>
+void adBackwardT(cudaStream_t st, const AdSpec& S, const double* out, const double* gE, long long* acc, void* gPos,
+                 void* gR0, void* gFrames, void* gH) {
+    cudaCheck(cudaMemsetAsync(acc, 0, sizeof(long long) * 3 * (size_t)S.nAtoms, st), "memset");
+    int bp = (S.nPairs + 255) / 256;
+    if (bp > 0) k_ad_back_pairs<R><<<bp, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gR0));
+    int bf = (S.M * S.F + 255) / 256;
+    if (bf > 0) k_ad_back_path<R><<<bf, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gFrames));
+    int bc = (std::max(S.K, 3 * S.nAtoms) + 255) / 256;
+    k_ad_back_hills_and_convert<R><<<bc, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gPos), static_cast<R*>(gH));
+}
+
+void adForward(int dtype, cudaStream_t st, const AdSpec& S, double* out, double* part, int nPart) {
+    if (S.F > 128) throw Error(GLUED_E_INVALID, "path frame count exceeds 128");
+    if (dtype == 1) adForwardT<double>(st, S, out, part, nPart);
+    else adForwardT<float>(st, S, out, part, nPart);
+    cudaCheck(cudaGetLastError(), "autograd forward");
+}
+
+void adBackward(int dtype, cudaStream_t st, const AdSpec& S, const double* out, const double* gE, long long* acc,
+                void* gPos, void* gR0, void* gFrames, void* gH) {
+    if (dtype == 1) adBackwardT<double>(st, S, out, gE, acc, gPos, gR0, gFrames, gH);
+    else adBackwardT<float>(st, S, out, gE, acc, gPos, gR0, gFrames, gH);
+    cudaCheck(cudaGetLastError(), "autograd backward");
+}
+
+}  // namespace glued

@@ -85,6 +85,7 @@ struct BatchDev {
     int* work;
     int* status;
     unsigned long long spinLimit;
+    unsigned long long* stamps;  // optional [grid][6] phase timestamps (nullptr = off)
 };
 
 // ------------------------------------------------------------- grid barrier
@@ -113,6 +114,12 @@ __device__ bool gridBarrier(unsigned int* bar, int* status, unsigned long long l
     }
     __syncthreads();
     return sOk != 0;
+}
+
+__device__ __forceinline__ unsigned long long globalTimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 // ------------------------------------------------------------- TMA helpers
@@ -346,6 +353,9 @@ __global__ void __launch_bounds__(256, 2) k_batch_step(BatchDev B) {
     __shared__ __align__(8) unsigned long long mbar;
     const int tid = threadIdx.x;
     const int numA = B.coordBlocks + B.hillItems * B.nWB;
+    unsigned long long* stamp = B.stamps ? B.stamps + 6 * (size_t)blockIdx.x : nullptr;
+    int nCoord = 0, nHill = 0;
+    if (stamp && tid == 0) stamp[0] = globalTimer();
     for (;;) {
         if (tid == 0) sItem = atomicAdd(B.work, 1);
         __syncthreads();
@@ -362,13 +372,18 @@ __global__ void __launch_bounds__(256, 2) k_batch_step(BatchDev B) {
             float (*sB)[TB * 3] = reinterpret_cast<float (*)[TB * 3]>(smem);
             coordTile<RA, BOX, NH>(wk.posq, nullptr, B.C, it, ta, sb, box, sB, red);
             __syncthreads();
+            nCoord++;
         } else {
             hillItem(B, item - B.coordBlocks, smem, &mbar);
+            nHill++;
         }
     }
+    if (stamp && tid == 0) { stamp[1] = globalTimer(); stamp[4] = nCoord; stamp[5] = nHill; }
     if (!gridBarrier(B.bar, B.status, B.spinLimit)) return;
+    if (stamp && tid == 0) stamp[2] = globalTimer();
     if (blockIdx.x == 0 && tid == 0) *B.work = 0;
     for (int p = blockIdx.x; p < B.W * B.parts; p += gridDim.x) finalizeWalker(B, p / B.parts, p % B.parts, smem);
+    if (stamp && tid == 0) stamp[3] = globalTimer();
 }
 
 __global__ void k_batch_deposit(BatchDev B) {
@@ -767,6 +782,42 @@ BatchTuning Batch::autotune() {
     int st = status();
     if (st) throw Error(GLUED_E_TIMEOUT, "batch: bounded wait gave up during autotuning (status " + std::to_string(st) + ")");
     return best;
+}
+
+// One regular step launched without the graph, with every CTA recording
+// %globaltimer at entry, end of phase A, barrier exit and exit, and how many
+// coordination / hill items it processed. out[0..7]: phase-A end (earliest,
+// latest CTA), barrier exit (latest), exit (latest) in microseconds after the
+// earliest entry; coordination items, hill items, most and fewest items per CTA.
+void Batch::phaseTimes(double* out) {
+    Impl& I = *impl_;
+    DBuf st;
+    st.alloc(sizeof(unsigned long long) * 6 * (size_t)I.grid);
+    cudaCheck(cudaMemsetAsync(st.p, 0, st.bytes, I.stream), "stamps");
+    I.dev.stamps = st.as<unsigned long long>();
+    I.launch(I.stream);
+    I.dev.stamps = nullptr;
+    I.launches++;
+    I.ready = true;
+    std::vector<unsigned long long> h(6 * (size_t)I.grid);
+    cudaCheck(cudaStreamSynchronize(I.stream), "sync");
+    cudaCheck(cudaMemcpy(h.data(), st.p, st.bytes, cudaMemcpyDeviceToHost), "stamps");
+    unsigned long long t0 = ~0ull, aMin = ~0ull, aMax = 0, bMax = 0, eMax = 0;
+    long long nc = 0, nh = 0, most = 0, fewest = 1ll << 40;
+    for (int g = 0; g < I.grid; g++) {
+        const unsigned long long* r = h.data() + 6 * (size_t)g;
+        t0 = std::min(t0, r[0]);
+        aMin = std::min(aMin, r[1]); aMax = std::max(aMax, r[1]);
+        bMax = std::max(bMax, r[2]); eMax = std::max(eMax, r[3]);
+        nc += (long long)r[4]; nh += (long long)r[5];
+        most = std::max(most, (long long)(r[4] + r[5]));
+        fewest = std::min(fewest, (long long)(r[4] + r[5]));
+    }
+    out[0] = (aMin - t0) * 1e-3; out[1] = (aMax - t0) * 1e-3;
+    out[2] = (bMax - t0) * 1e-3; out[3] = (eMax - t0) * 1e-3;
+    out[4] = (double)nc; out[5] = (double)nh; out[6] = (double)most; out[7] = (double)fewest;
+    int s = status();
+    if (s) throw Error(GLUED_E_TIMEOUT, "batch: bounded wait gave up (status " + std::to_string(s) + ")");
 }
 
 void Batch::updateState(int step) {

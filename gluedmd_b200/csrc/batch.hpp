@@ -38,6 +38,7 @@ public:
     long long launchCount() const;
     bool graphed() const;
     double lastStepMs();
+    void phaseTimes(double* out);
 
 private:
     struct Impl;

@@ -306,6 +306,25 @@ int glued_context_launch_count(glued_context* c, long long* count) {
 int glued_measure_fp32_peak(double* tflops) {
     return guard([&] { need(tflops, "out"); *tflops = glued::measureFp32Peak(); });
 }
+int glued_ad_forward(int dtype, void* stream, const glued_ad_spec* spec, double* out, double* partials,
+                     int n_partials) {
+    return guard([&] {
+        need(spec, "spec"); need(out, "out"); need(partials, "partials");
+        if (n_partials < 1) throw glued::Error(GLUED_E_INVALID, "n_partials must be >= 1");
+        glued::adForward(dtype, (cudaStream_t)stream, *spec, out, partials, n_partials);
+    });
+}
+int glued_ad_backward(int dtype, void* stream, const glued_ad_spec* spec, const double* out,
+                      const double* grad_energy, long long* acc, void* grad_pos, void* grad_r0, void* grad_frames,
+                      void* grad_heights) {
+    return guard([&] {
+        need(spec, "spec"); need(out, "out"); need(grad_energy, "grad_energy"); need(acc, "acc");
+        need(grad_pos, "grad_pos"); need(grad_r0, "grad_r0"); need(grad_frames, "grad_frames");
+        need(grad_heights, "grad_heights");
+        glued::adBackward(dtype, (cudaStream_t)stream, *spec, out, grad_energy, acc, grad_pos, grad_r0, grad_frames,
+                          grad_heights);
+    });
+}
 int glued_coordination_noalloc(void* stream, const void* posq, const int* group_a, int n_a, const int* group_b,
                                int n_b, double r0, double n, double m, int periodic, const double box[9],
                                double* cn_out, float* grad_out) {
@@ -396,6 +415,9 @@ int glued_batch_status(glued_batch* b, int* status) {
 }
 int glued_batch_launch_count(glued_batch* b, long long* count) {
     return guard([&] { need(b, "batch"); need(count, "out"); *count = b->b->launchCount(); });
+}
+int glued_batch_phase_times(glued_batch* b, double* out) {
+    return guard([&] { need(b, "batch"); need(out, "out"); b->b->phaseTimes(out); });
 }
 
 }  // extern "C"

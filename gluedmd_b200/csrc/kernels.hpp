@@ -30,6 +30,9 @@ void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, cons
                        int* mergeFlag, double* partial, int nPartial);
 
 double measureFp32Peak();
+void adForward(int dtype, cudaStream_t st, const glued_ad_spec& S, double* out, double* part, int nPart);
+void adBackward(int dtype, cudaStream_t st, const glued_ad_spec& S, const double* out, const double* gE,
+                long long* acc, void* gPos, void* gR0, void* gFrames, void* gH);
 void coordinationNoAlloc(cudaStream_t stream, const void* posq, const int* groupA, int nA, const int* groupB, int nB,
                          double r0, double n, double m, int periodic, const double* box9, double* cnOut,
                          float* gradOut);

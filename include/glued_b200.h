@@ -165,6 +165,40 @@ int glued_measure_fp32_peak(double* tflops);
  * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
 int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);
 
+/* ------------------------------------------------------ differentiable bias
+ * Contact map + path CV + hill bias E(CMAP, s) with a hand-written backward
+ * (no reference counterpart: GLUED has no autograd path; the CVs are its contact
+ * map, CommonGluedKernels.cpp:1236-1323, and path CV, :641-794). dtype 0 = FP32,
+ * 1 = FP64 for every R-typed array. All arrays are device memory owned by the
+ * caller. out: double[7 + F] = E, CMAP, s, z, S, w_0..w_{F-1}, dE/dCMAP, dE/ds.
+ * partials: double[n_partials] (CMAP partial sums, one per CTA of the forward).
+ * backward: grad_energy = device double dL/dE; acc = int64[3 * n_atoms] scratch
+ * (2^40 fixed point); outputs dL/d(positions, r0, frames, heights).           */
+typedef struct glued_ad_spec {
+    const void* pos;        /* R[n_atoms][3] */
+    int nAtoms;
+    const int* pairs;       /* int[P][2] */
+    int nPairs;
+    const void* r0;         /* R[P] */
+    const float* nmw;       /* float[P][3]: n, m, w (integer n, m) */
+    const int* pathAtoms;   /* int[M] */
+    int M;
+    const void* frames;     /* R[F][M][3] */
+    int F;                  /* <= 128 */
+    double lambda;
+    const double* hillC;    /* double[K][2]: (CMAP, s) centres */
+    const void* heights;    /* R[K] */
+    int K;
+    double sig[2];
+    int periodic;
+    double box[3];          /* rectangular box lengths when periodic */
+} glued_ad_spec;
+int glued_ad_forward(int dtype, void* stream, const glued_ad_spec* spec, double* out, double* partials,
+                     int n_partials);
+int glued_ad_backward(int dtype, void* stream, const glued_ad_spec* spec, const double* out,
+                      const double* grad_energy, long long* acc, void* grad_pos, void* grad_r0, void* grad_frames,
+                      void* grad_heights);
+
 /* ------------------------------------------------------ no-allocation variant
  * No counterpart in the reference. For callers that cannot allocate device
  * memory while they evaluate forces (an engine that reserves all device memory
@@ -240,6 +274,12 @@ int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int 
 /* Status word of the bounded waits (0 = ok; bit 0 grid barrier, bit 1 bulk copy). */
 int glued_batch_status(glued_batch* b, int* status);
 int glued_batch_launch_count(glued_batch* b, long long* count);
+/* Profiling: runs one regular step (forces are accumulated as by execute) with
+ * per-CTA timestamps. out[8]: end of the work-item phase on the earliest and the
+ * latest CTA, grid-barrier exit and kernel exit on the latest CTA (microseconds
+ * after the earliest CTA started), coordination items, hill items, and the most
+ * and fewest items one CTA processed. No reference counterpart.             */
+int glued_batch_phase_times(glued_batch* b, double* out);
 
 #ifdef __cplusplus
 }

@@ -705,10 +705,25 @@ double orc_opes_eval(const double* cvv, const int* idx, int D, const double* cen
 // the deposit was skipped (adaptive warm-up) and -3 when the table is full.
 // Transcendentals use the deterministic gd_exp/gd_log/gd_pow shared with the
 // device code so that decisions can be compared bit for bit.
+int orc_opes_deposit_ex(const double* cvv, const int* idx, int D, double* runMean, double* runM2,
+                        const double* sigma0, double sigmaMin, double* centers, double* sigmas, double* logW,
+                        double* st, int* ist, int variant, int adaptiveStride, double Vlast, double invKT,
+                        double cutoff2, int maxKernels, double gamma, int skipPairSum);
+
 int orc_opes_deposit(const double* cvv, const int* idx, int D, double* runMean, double* runM2,
                      const double* sigma0, double sigmaMin, double* centers, double* sigmas, double* logW,
                      double* st, int* ist, int variant, int adaptiveStride, double Vlast, double invKT,
                      double cutoff2, int maxKernels, double gamma) {
+    return orc_opes_deposit_ex(cvv, idx, D, runMean, runM2, sigma0, sigmaMin, centers, sigmas, logW, st, ist,
+                               variant, adaptiveStride, Vlast, invKT, cutoff2, maxKernels, gamma, 0);
+}
+
+// skipPairSum != 0 leaves sum_uprob untouched (decision replays: the sum feeds
+// only the bias value, never a merge decision).
+int orc_opes_deposit_ex(const double* cvv, const int* idx, int D, double* runMean, double* runM2,
+                        const double* sigma0, double sigmaMin, double* centers, double* sigmas, double* logW,
+                        double* st, int* ist, int variant, int adaptiveStride, double Vlast, double invKT,
+                        double cutoff2, int maxKernels, double gamma, int skipPairSum) {
     using namespace glued_dmath;
     if (adaptiveStride > 0 && ist[1] < adaptiveStride) return -2;
     int nB = ist[0];
@@ -781,6 +796,7 @@ int orc_opes_deposit(const double* cvv, const int* idx, int D, double* runMean, 
     }
     st[1] += hRaw;
     double eps = gd_exp(-0.5 * cutoff2);
+    if (skipPairSum) return ret;
     if (mk < 0 && nA > nB) {
         double delta = hNew * (1.0 - eps);
         for (int j = 0; j < nB; j++) {

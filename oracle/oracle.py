@@ -108,6 +108,7 @@ class OracleSystem:
         self._build_plan()
         self._setup_biases()
         self.cv_ready = False
+        self.decisions_only = False  # skip the sum_uprob update in deposit replays
         self.last_update_step = -1
         self.cv_values = np.zeros(self.num_cvs)
         self.bias_energies = np.zeros(max(1, len(self.biases)))
@@ -417,12 +418,12 @@ class OracleSystem:
             if st["nker_cpu"] >= st["maxk"]:
                 continue
             will = st["astride"] == 0 or st["nsamp_cpu"] >= st["astride"]
-            r = L.orc_opes_deposit(C, _p(st["idx"], _I), st["D"], _p(st["mean"], _D), _p(st["m2"], _D),
-                                   _p(st["sigma0"], _D), _D(st["smin"]), _p(st["centers"], _D),
-                                   _p(st["sigmas"], _D), _p(st["logw"], _D), _p(st["dst"], _D),
-                                   _p(st["ist"], _I), st["variant"], st["astride"],
-                                   _D(self.bias_energies[st["slot"]]), _D(1.0 / st["kT"]), _D(st["cut2"]),
-                                   st["maxk"], _D(st["gamma"]))
+            r = L.orc_opes_deposit_ex(C, _p(st["idx"], _I), st["D"], _p(st["mean"], _D), _p(st["m2"], _D),
+                                      _p(st["sigma0"], _D), _D(st["smin"]), _p(st["centers"], _D),
+                                      _p(st["sigmas"], _D), _p(st["logw"], _D), _p(st["dst"], _D),
+                                      _p(st["ist"], _I), st["variant"], st["astride"],
+                                      _D(self.bias_energies[st["slot"]]), _D(1.0 / st["kT"]), _D(st["cut2"]),
+                                      st["maxk"], _D(st["gamma"]), 1 if self.decisions_only else 0)
             st["decisions"].append(int(r))
             if will:
                 st["nker_cpu"] += 1

@@ -153,6 +153,68 @@ def test_opes_decisions_bit_exact():
     assert np.array_equal(lw, st["logw"][:nk])
 
 
+def test_opes_decisions_bit_exact_c3_scale():
+    """2,000 OPES deposits on the C3 system (50,000 atoms, COM distance + gyration
+    of 5,000 atoms) starting from its 10,000-kernel compressed table: every
+    merge/append decision and the final centres, sigmas and log-weights are
+    bit-identical to the oracle fed the product's CV values and bias energy.
+    The oracle skips the O(N^2) sum_uprob recomputation after merges (the sum
+    enters the bias value, never a decision)."""
+    import gpu_util
+    from gluedmd_b200 import workloads as W
+    import struct
+    w = W.config3()
+    n = len(w.positions)
+    orc = O.OracleSystem(w.cvs, w.biases, mode="f64", num_particles=n, periodic=True)
+    orc.load_blob(w.blob)
+    orc.decisions_only = True
+    ctx, f = gpu_util.make_context(w.positions, w.cvs, w.biases, masses=w.masses, pbc=True, box=w.box,
+                                   blob=w.blob)
+    nc = ctx.glued_context_for(f)
+    pace = w.biases[0][3][1]
+    sel = np.asarray(w.extra["sel"])
+    half = sel[:len(sel) // 2]
+    rng = np.random.default_rng(21)
+    pos0 = np.asarray(w.positions, float)
+    shift = np.zeros(3)
+    scale = 1.0
+    dec_gpu = []
+    n_dep = 2000
+    for k in range(n_dep + 1):
+        step = k * pace
+        ctx.setStepCount(step)
+        ctx.updateContextState()
+        if k > 0:
+            dec_gpu.append(nc.opes_last_decision(0))
+        orc.update_state(step)
+        shift += rng.normal(0.0, 0.02, 3)
+        scale = float(np.clip(scale + rng.normal(0.0, 0.004), 0.9, 1.1))
+        pos = pos0.copy()
+        cen = pos0[sel].mean(0)
+        pos[sel] = cen + (pos0[sel] - cen) * scale
+        pos[half] += shift
+        ctx.setPositions(pos)
+        e, _ = ctx.computeForces()
+        orc.cv_values = np.array(nc.cv_values())
+        orc.bias_energies = np.array([e])
+        orc.cv_ready = True
+    st = orc.bias_state[0]
+    dec_orc = list(st["decisions"])
+    assert len(dec_orc) == n_dep
+    assert dec_gpu == dec_orc
+    assert sum(d >= 0 for d in dec_orc) > 50 and sum(d == -1 for d in dec_orc) > 50
+    blob = f.getBiasState()
+    nk = struct.unpack("<i", blob[12:16])[0]
+    assert nk == int(st["ist"][0])
+    off = 16 + 8 + 4 + 2 * 8 * 2
+    c = np.frombuffer(blob[off:off + 16 * nk], "<f8")
+    s_ = np.frombuffer(blob[off + 16 * nk:off + 32 * nk], "<f8")
+    lw = np.frombuffer(blob[off + 32 * nk:off + 40 * nk], "<f8")
+    assert np.array_equal(c, st["centers"][:2 * nk])
+    assert np.array_equal(s_, st["sigmas"][:2 * nk])
+    assert np.array_equal(lw, st["logw"][:nk])
+
+
 def test_opes_energy_vs_oracle():
     cvs, biases = opes_system(variant=0, pace=1, sigma=0.2)
     rng = np.random.default_rng(5)

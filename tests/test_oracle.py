@@ -171,6 +171,32 @@ def test_opes_deposit_sequence_vs_reference(variant):
     np.testing.assert_allclose(sa["dst"], sb["dst"], rtol=1e-11)
 
 
+@pytest.mark.parametrize("variant", [0, 2])
+def test_opes_decisions_only_replay_matches_full(variant):
+    """The decisions-only deposit mode (no sum_uprob update) produces the same
+    decisions and kernel tables as the full deposit when both are fed the same
+    CV values and bias energies."""
+    cvs, biases = opes_system(variant)
+    rng = np.random.default_rng(4)
+    a = O.OracleSystem(cvs, biases, mode="f64", num_particles=4)
+    b = O.OracleSystem(cvs, biases, mode="f64", num_particles=4)
+    b.decisions_only = True
+    for step in range(80):
+        pos = rng.uniform(0, 1.0, (4, 3))
+        a.update_state(step); b.update_state(step)
+        ra = a.execute(pos)
+        b.cv_values = ra["cv_values"].copy(); b.bias_energies = ra["bias_energies"].copy(); b.cv_ready = True
+    sa, sb = a.bias_state[0], b.bias_state[0]
+    assert sa["decisions"] == sb["decisions"]
+    assert any(d >= 0 for d in sa["decisions"]) and any(d == -1 for d in sa["decisions"])
+    nk = int(sa["ist"][0])
+    assert nk == int(sb["ist"][0])
+    assert np.array_equal(sa["centers"][:2 * nk], sb["centers"][:2 * nk])
+    assert np.array_equal(sa["sigmas"][:2 * nk], sb["sigmas"][:2 * nk])
+    assert np.array_equal(sa["logw"][:nk], sb["logw"][:nk])
+    assert sb["dst"][0] == 0.0 and sa["dst"][0] != 0.0
+
+
 def test_deterministic_math_against_libm():
     """gd_exp / gd_log / gd_pow stay within a few ulp of the C library."""
     import ctypes
