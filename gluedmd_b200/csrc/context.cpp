@@ -344,29 +344,8 @@ void Context::buildPlan(const GluedForce& f) {
     G_.items = groupItems_.as<GroupItem>(); G_.numItems = (int)groups.size();
     G_.atoms = gAtoms_.as<int>(); G_.mass = gMass_.as<float>(); G_.ref = gRef_.as<float>();
     G_.ev = gEv_.as<float>(); G_.cmPairs = cmPairs_.as<int2>(); G_.cmParams = cmParams_.as<float4>();
-    // coordination tiling
+    // coordination: tile-major step list over a persistent grid (coord_run.cuh)
     if (!coord.empty()) {
-        const int TA = 8 * coordRA_;
-        long long pairs = 0;
-        for (auto& it : coord) pairs += (long long)it.nA * it.nB;
-        long long target = 148LL * 8;
-        long long perCta = std::max<long long>(1, pairs / target);
-        int bSplit = (int)std::min<long long>(1 << 20, std::max<long long>(128, ((perCta / TA + 127) / 128) * 128));
-        C_.bSplit = bSplit;
-        int blocks = 0, pa = 0, pb = 0, cn = 0, rows = 0;
-        std::vector<int> blockItem;
-        for (size_t i = 0; i < coord.size(); i++) {
-            CoordItem& it = coord[i];
-            it.tilesA = std::max(1, (it.nA + TA - 1) / TA);
-            it.splitsB = std::max(1, (it.nB + bSplit - 1) / bSplit);
-            it.block0 = blocks;
-            it.partA = pa; it.partB = pb; it.cn0 = cn;
-            int nb = it.tilesA * it.splitsB;
-            for (int k = 0; k < nb; k++) blockItem.push_back((int)i);
-            blocks += nb; cn += nb;
-            pa += it.splitsB * it.nA; pb += it.tilesA * it.nB;
-            rows += it.nA + it.nB;
-        }
         // one kernel instantiation per launch: items with different switch kinds
         // fall back to the most general kind present
         coordKind_ = coord[0].kind;
@@ -374,16 +353,32 @@ void Context::buildPlan(const GluedForce& f) {
             if (it.kind != coordKind_) coordKind_ = (coordKind_ == 0 || it.kind == 0) ? 0 : -1;
         if (coordKind_ != 3)
             for (auto& it : coord) it.kind = coordKind_;
+        coordRows_ = buildCoordSteps(coord, 8, {}, coordStepsH_);
+        coordItemsH_ = coord;
+        coordItemsN_ = (int)coord.size();
+        coordAtomsN_ = (int)coordAtoms.size();
         coordItems_.upload(coord);
         coordAtoms_.upload(coordAtoms);
-        coordBlockItem_.upload(blockItem);
-        partA_.alloc(sizeof(float) * 3 * std::max(pa, 1));
-        partB_.alloc(sizeof(float) * 3 * std::max(pb, 1));
-        cnPart_.alloc(sizeof(double) * std::max(cn, 1));
-        C_.items = coordItems_.as<CoordItem>(); C_.numItems = (int)coord.size();
-        C_.atoms = coordAtoms_.as<int>(); C_.blockItem = coordBlockItem_.as<int>();
-        C_.partA = partA_.as<float>(); C_.partB = partB_.as<float>(); C_.cnPart = cnPart_.as<double>();
-        coordBlocks_ = blocks; coordRows_ = rows;
+        coordSlots_.alloc(sizeof(int) * std::max(1, coordAtomsN_));
+        coordSteps_.alloc(sizeof(CoordStep) * coordStepsH_.size());
+        int dev = 0, sms = 0;
+        cudaCheck(cudaGetDevice(&dev), "device");
+        cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
+        coordGrid_ = sms * coordRunOccupancy(coordKind_, periodic_ ? 1 : 0, true);
+        coordGrid_ = std::max(1, std::min(coordGrid_, (int)coordStepsH_.size()));
+        coordBegin_.upload(balanceRanges((int)coordStepsH_.size(), coordGrid_, {}));
+        coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
+        coordCnAcc_.alloc(sizeof(unsigned long long) * coordItemsN_);
+        cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
+        cudaCheck(cudaMemset(coordCnAcc_.p, 0, coordCnAcc_.bytes), "coord acc");
+        R_.items = coordItems_.as<CoordItem>();
+        R_.steps = coordSteps_.as<CoordStep>();
+        R_.begin = coordBegin_.as<int>();
+        R_.slots = coordSlots_.as<int>();
+        R_.sysBox = box_.as<BoxDev>();
+        R_.itemsPerSys = 1 << 30;
+        R_.acc = coordAcc_.as<unsigned long long>();
+        R_.cnAcc = coordCnAcc_.as<unsigned long long>();
     }
 }
 
@@ -549,12 +544,18 @@ void Context::bind(cudaStream_t s, const void* posq, const int* atomIndex, long 
     padded_ = padded;
     bound_ = true;
     invalidateGraphs();
+    if (!coordStepsH_.empty()) {
+        for (auto& st : coordStepsH_) st.posq = posq_;
+        cudaCheck(cudaMemcpy(coordSteps_.p, coordStepsH_.data(), sizeof(CoordStep) * coordStepsH_.size(),
+                             cudaMemcpyHostToDevice), "coordination steps");
+    }
     atomsReordered();
 }
 
 void Context::atomsReordered() {
     requireBound();
     launchInvertIndex(stream_, atomIndex_, u2g_.as<int>(), numParticles_);
+    launchComposeSlots(stream_, coordAtoms_.as<int>(), u2g_.as<int>(), coordSlots_.as<int>(), coordAtomsN_);
     cudaCheck(cudaGetLastError(), "invert index");
 }
 
@@ -571,7 +572,13 @@ void Context::setBox(const double box[9]) {
     b.inv[0] = (float)(1.0 / box[0]); b.inv[1] = (float)(1.0 / box[4]); b.inv[2] = (float)(1.0 / box[8]);
     bool rect = box[1] == 0 && box[2] == 0 && box[3] == 0 && box[5] == 0 && box[6] == 0 && box[7] == 0;
     b.kind = periodic_ ? (rect ? 1 : 2) : 0;
+    if (b.kind != boxHost_.kind) invalidateGraphs();
     boxHost_ = b;
+    if (coordItemsN_ > 0) {
+        bool hi = coordNeedsHi(coordItemsH_, box, periodic_);
+        if (hi != coordHi_) invalidateGraphs();
+        coordHi_ = hi;
+    }
     // The device copy is read by graph-replayed kernels: stage through pinned memory
     // on the same stream so it is ordered before the next launch.
     if (bound_) {
@@ -595,7 +602,7 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
     if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
     if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_);
     if (want(2) || want(3))
-        launchCoord(s, posq_, u2g, C_, coordBlocks_, coordRows_, boxHost_.kind, coordRA_, coordKind_, box, J_, cvv,
+        launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv,
                     onlyPhase < 0 ? 3 : (onlyPhase == 2 ? 1 : 2));
     if (want(4))
         launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
@@ -607,7 +614,7 @@ int Context::kernelsPerExecute(bool includeForces) const {
     int k = 1;  // biases
     if (numSimple_ > 0) k++;
     if (G_.numItems > 0) k++;
-    if (C_.numItems > 0) k += 2;
+    if (coordItemsN_ > 0) k += 2;
     if (includeForces && numRows_ > 0) k++;
     return k;
 }
@@ -632,6 +639,11 @@ std::vector<double> Context::profilePhases(int reps) {
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    // the pair-only repetitions left sums that no finalize cleared
+    if (coordItemsN_ > 0) {
+        cudaCheck(cudaMemsetAsync(coordAcc_.p, 0, coordAcc_.bytes, stream_), "coord acc");
+        cudaCheck(cudaMemsetAsync(coordCnAcc_.p, 0, coordCnAcc_.bytes, stream_), "coord acc");
+    }
     return out;
 }
 

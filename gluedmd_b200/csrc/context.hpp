@@ -114,13 +114,16 @@ private:
     DBuf u2g_, box_, cvv_, dudcv_, energies_, testGrad_;
     DBuf jAtom_, jx_, jy_, jz_, jCv_;
     DBuf simple_, groupItems_, gAtoms_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
-    DBuf coordItems_, coordAtoms_, coordBlockItem_, partA_, partB_, cnPart_;
+    DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnAcc_;
     DBuf biasDev_, mergeFlag_, uprobPartial_;
     JacDev J_{};
     int numSimple_ = 0;
     GroupDev G_{};
-    CoordDev C_{};
-    int coordBlocks_ = 0, coordRows_ = 0, coordRA_ = 8, coordKind_ = 3;
+    std::vector<CoordItem> coordItemsH_;
+    std::vector<CoordStep> coordStepsH_;
+    CoordRunDev R_{};
+    int coordItemsN_ = 0, coordRows_ = 0, coordGrid_ = 0, coordKind_ = 3, coordAtomsN_ = 0;
+    bool coordHi_ = true;
     int nUprobPartial_ = 296;
 
     std::vector<HostBias> biases_;       // addBias order

@@ -1,0 +1,82 @@
+// Host side of the coordination step runs (coord_run.cuh): the tile-major step
+// list of a set of coordination items and the balanced per-CTA ranges.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "kernels.hpp"
+
+namespace glued {
+
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<const float4*>& posqOfItem,
+                    std::vector<CoordStep>& steps) {
+    const int TA = COORD_NW * ra;
+    steps.clear();
+    int rows = 0;
+    for (size_t i = 0; i < items.size(); i++) {
+        CoordItem& it = items[i];
+        it.row0 = rows;
+        it.tilesA = std::max(1, (it.nA + TA - 1) / TA);
+        const int nCh = std::max(1, (it.nB + COORD_CH - 1) / COORD_CH);
+        for (int ta = 0; ta < it.tilesA; ta++) {
+            const int nAv = std::min(TA, it.nA - ta * TA);
+            for (int c = 0; c < nCh; c++) {
+                CoordStep s{};
+                s.posq = posqOfItem.empty() ? nullptr : posqOfItem[i];
+                s.item = (int)i;
+                s.aStart = it.a0 + ta * TA;
+                s.bStart = it.b0 + c * COORD_CH;
+                s.rowA = rows + ta * TA;
+                s.rowB = rows + it.nA + c * COORD_CH;
+                const int nBv = std::min(COORD_CH, it.nB - c * COORD_CH);
+                int fl = (c == 0 ? COORD_F_FIRST : 0) | (c == nCh - 1 ? COORD_F_LAST : 0);
+                s.packed = nAv | (nBv << 8) | (fl << 16);
+                steps.push_back(s);
+            }
+        }
+        rows += it.nA + it.nB;
+    }
+    return rows;
+}
+
+std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost) {
+    std::vector<int> begin(grid + 1, 0);
+    if (grid < 1) return begin;
+    auto share = [&](double T, int b) {
+        double c = b < (int)preCost.size() ? preCost[b] : 0.0;
+        return std::max(0.0, T - c);
+    };
+    // level T with sum_b max(0, T - cost_b) == numSteps (bisection)
+    double lo = 0.0, hi = (double)numSteps + 1.0;
+    for (double c : preCost) hi = std::max(hi, c + (double)numSteps + 1.0);
+    for (int it = 0; it < 100; it++) {
+        double mid = 0.5 * (lo + hi), tot = 0.0;
+        for (int b = 0; b < grid; b++) tot += share(mid, b);
+        if (tot < numSteps) lo = mid; else hi = mid;
+    }
+    double cum = 0.0;
+    for (int b = 0; b < grid; b++) {
+        cum += share(hi, b);
+        begin[b + 1] = std::min(numSteps, (int)std::llround(cum));
+    }
+    begin[grid] = numSteps;
+    for (int b = 1; b <= grid; b++) begin[b] = std::max(begin[b], begin[b - 1]);
+    return begin;
+}
+
+bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic) {
+    if (!periodic) return true;
+    // longest minimum-image distance: half of |a| + |b| + |c| bounds it
+    double la = std::sqrt(box[0] * box[0] + box[1] * box[1] + box[2] * box[2]);
+    double lb = std::sqrt(box[3] * box[3] + box[4] * box[4] + box[5] * box[5]);
+    double lc = std::sqrt(box[6] * box[6] + box[7] * box[7] + box[8] * box[8]);
+    const double dmax = 0.5 * (la + lb + lc);
+    for (const CoordItem& it : items) {
+        if (it.rc2 > 0.0f && (double)it.rc2 < dmax * dmax) return true;
+        const double x = dmax / (double)it.r0;
+        if (x * x >= 0.9e6) return true;
+    }
+    return false;
+}
+
+}  // namespace glued

@@ -1,0 +1,334 @@
+// Coordination pairs as static per-CTA runs of (item, A tile, B chunk) steps.
+//
+// Work decomposition. Every coordination item (one CV of one system) is cut into
+// A tiles of TA = 8*RA atoms and B chunks of CH = 128 atoms; one step is one
+// (tile, chunk) block of TA x CH pairs. The host lists the steps tile-major
+// (CoordStep) and gives every CTA one contiguous range of them, balanced so that
+// each CTA of the persistent grid has the same number of steps (the batched
+// path lowers the share of CTAs that also evaluate hill items). A CTA walks its
+// range once: A atoms stay in registers while consecutive steps belong to the
+// same tile.
+//
+// Data movement. Positions are gathered with 16-byte cp.async copies into
+// shared memory two steps ahead (double buffer), so a step computes while the
+// next one lands; gather indices for step s+2 are loaded into registers before
+// step s computes and the copies are issued after its barrier. Step descriptors
+// of a window of up to WIN steps sit in shared memory.
+//
+// Arithmetic. Coordinates are scaled by 1/r0 (A once per tile, B inside the
+// subtraction FMA), so the pair's squared distance is x^2 directly. For the
+// n = 6, m = 12 switch, f = 1/(1 + x^6) and the gradient factor h = x^4 f^2 need
+// one reciprocal and no square root. The reference's lower bound r^2 >= 1e-20
+// (CommonGluedKernels.cpp:983-987) is compared on every pair; the upper bound
+// x <= 1000 (and the optional cutoff) only where the box admits such distances
+// (template flag HI).
+//
+// Accumulation. Per-pair gradients h*d (scaled units) are summed in FP32 over a
+// step: per lane over its A atoms for B, per warp over lanes for A. Those step
+// sums are converted to 64-bit fixed point (value * 2^32) and added with integer
+// atomics into acc[row][3]; the CN partial of each run piece (FP64 block sum) is
+// added the same way into cnAcc[item]. Integer addition is exact and
+// order-independent, so results are bitwise reproducible run to run and do not
+// depend on the grid. The reader multiplies by the item's scale (-n/r0 for the
+// n = 6, m = 12 switch, 1/r0 otherwise), converts to FP64 and clears the slots.
+#pragma once
+
+#include "devfn.cuh"
+
+namespace glued {
+
+namespace crun {
+constexpr int NW = COORD_NW;   // warps per CTA
+constexpr int RB = 4;          // B atoms per lane per step
+constexpr int CH = 32 * RB;    // B atoms per chunk
+static_assert(CH == COORD_CH, "chunk size");
+constexpr int WIN = 64;        // step descriptors per shared-memory window
+constexpr float FX = 4294967296.0f;   // 2^32
+constexpr double FXD = 4294967296.0;
+constexpr double IFXD = 1.0 / 4294967296.0;
+constexpr int F_FIRST = COORD_F_FIRST, F_LAST = COORD_F_LAST;
+}  // namespace crun
+
+template <int RA>
+struct CoordRunSmem {
+    float4 pos[2][crun::CH];
+    float4 apos[2][crun::NW * RA];
+    float g[2][crun::NW][crun::CH * 3];
+    CoordStep st[crun::WIN];
+    double red[2][crun::NW];
+};
+
+__device__ __forceinline__ unsigned smemU32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// 16-byte global -> shared copy; valid == false writes zeros (nothing is read).
+__device__ __forceinline__ void cpAsync16(void* dst, const void* src, bool valid) {
+    unsigned n = valid ? 16u : 0u;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smemU32(dst)), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ void redAddI64(unsigned long long* p, long long v) {
+    atomicAdd(p, (unsigned long long)v);
+}
+
+// Pair constants of one item in scaled units (coordinates divided by r0).
+struct RunConst {
+    float lo, hi;       // valid pairs: lo <= x^2 < hi
+    float n, m;         // general exponents (kind 0)
+    int ni, mi;         // integer exponents (kind -1)
+    float preRes, preDf, preSec;  // Taylor coefficients at x = 1 (kind 0)
+    float ir0;
+    BoxDev box;         // scaled: a, b, c divided by r0; inv multiplied by r0
+};
+
+__device__ __forceinline__ RunConst runConst(const CoordItem& it, const BoxDev& b) {
+    RunConst k;
+    k.ir0 = 1.0f / it.r0;
+    const float ir0sq = k.ir0 * k.ir0;
+    k.lo = 1e-20f * ir0sq;
+    const float hiX = 1e6f * 1.0000002f;
+    k.hi = it.rc2 > 0.0f ? fminf(it.rc2 * ir0sq, hiX) : hiX;
+    k.n = it.n; k.m = it.m;
+    k.ni = (int)it.n; k.mi = (int)it.m;
+    k.preRes = k.n / k.m;
+    k.preDf = 0.5f * k.n * (k.n - k.m) / k.m;
+    k.preSec = k.n * (k.m * k.m - 3.0f * k.m * (k.n - 1.0f) + k.n * (2.0f * k.n - 3.0f)) / (6.0f * k.m);
+    k.box = b;
+    for (int i = 0; i < 3; i++) {
+        k.box.a[i] = b.a[i] * k.ir0; k.box.b[i] = b.b[i] * k.ir0; k.box.c[i] = b.c[i] * k.ir0;
+        k.box.inv[i] = b.inv[i] * it.r0;
+    }
+    return k;
+}
+
+// Minimum image of a scaled difference (same rounding as imageT in coord_tile.cuh).
+template <int BOX>
+__device__ __forceinline__ void imageS(float& dx, float& dy, float& dz, const BoxDev& b) {
+    constexpr float R = 12582912.0f;
+    if (BOX == 1) {
+        dx = fmaf(-(fmaf(dx, b.inv[0], R) - R), b.a[0], dx);
+        dy = fmaf(-(fmaf(dy, b.inv[1], R) - R), b.b[1], dy);
+        dz = fmaf(-(fmaf(dz, b.inv[2], R) - R), b.c[2], dz);
+    } else if (BOX == 2) {
+        float s3 = fmaf(dz, b.inv[2], R) - R;
+        dx = fmaf(-s3, b.c[0], dx); dy = fmaf(-s3, b.c[1], dy); dz = fmaf(-s3, b.c[2], dz);
+        float s2 = fmaf(dy, b.inv[1], R) - R;
+        dx = fmaf(-s2, b.b[0], dx); dy = fmaf(-s2, b.b[1], dy);
+        float s1 = fmaf(dx, b.inv[0], R) - R;
+        dx = fmaf(-s1, b.a[0], dx);
+    }
+}
+
+// f and h = (df/dx)/x of one pair from x^2 (scaled). For NH > 0 (m = 2n, n = 2NH)
+// the bounds are applied by the caller; for the other kinds `valid` gates the
+// pair and must already include the bounds.
+template <int NH>
+__device__ __forceinline__ void switchX2(float x2, bool valid, const RunConst& k, float& f, float& h) {
+    if (NH > 0) {
+        float p = 1.0f;
+#pragma unroll
+        for (int e = 1; e < NH; e++) p = e == 1 ? x2 : p * x2;
+        float y = valid ? fmaf(p, x2, 1.0f) : __int_as_float(0x7f800000);
+        float ff;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ff) : "f"(y));
+        f = ff;
+        h = (p * ff) * ff;
+    } else if (NH < 0) {
+        float x = sqrtf(x2);
+        float ff, dfdx;
+        ratioSwitch(x, k.ni, k.mi, ff, dfdx);
+        f = valid ? ff : 0.0f;
+        h = valid ? dfdx / x : 0.0f;
+    } else {
+        float x = sqrtf(x2);
+        float ff, dfdx;
+        float dx1 = x - 1.0f;
+        if (fabsf(dx1) < 1e-4f) {
+            ff = k.preRes + dx1 * (k.preDf + 0.5f * dx1 * k.preSec);
+            dfdx = k.preDf + dx1 * k.preSec;
+        } else if (x < 1e-10f) {
+            ff = 1.0f; dfdx = 0.0f;
+        } else {
+            float xn = powf(x, k.n), xm = powf(x, k.m);
+            float den = 1.0f - xm;
+            ff = (1.0f - xn) / den;
+            dfdx = (k.m * (xm / x) - k.n * (xn / x) + (k.n - k.m) * (xn * xm / x)) / (den * den);
+        }
+        f = valid ? ff : 0.0f;
+        h = valid ? dfdx / x : 0.0f;
+    }
+}
+
+// Scale that turns an acc sum into dCN/dx (nm^-1) for the item's switch kind.
+__device__ __host__ __forceinline__ double coordAccScale(const CoordItem& it) {
+    return it.kind > 0 ? -(double)it.n / (double)it.r0 : 1.0 / (double)it.r0;
+}
+
+struct NoPieceHook {
+    __device__ void operator()(int, int) const {}
+};
+
+// Runs steps [s0, s1) of R on this CTA. Hook(item, steps) is called by all
+// threads after a piece (maximal sub-run of one tile) has been fully
+// accumulated; a hook that publishes completion must fence first.
+template <int RA, int BOX, int NH, bool HI, class Hook>
+__device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook) {
+    using namespace crun;
+    constexpr int TA = NW * RA;
+    const int tid = threadIdx.x, lane = tid & 31, ty = tid >> 5;
+    float ax[RA], ay[RA], az[RA], gax[RA], gay[RA], gaz[RA];
+    RunConst K;
+    double cn = 0.0;
+    int pieceSteps = 0;
+    for (int w0 = s0; w0 < s1; w0 += WIN) {
+        const int w1 = min(s1, w0 + WIN);
+        const int nw = w1 - w0;
+        __syncthreads();  // previous window fully consumed
+        {
+            const int4* src = reinterpret_cast<const int4*>(R.steps + w0);
+            int4* dst = reinterpret_cast<int4*>(sm.st);
+            for (int i = tid; i < nw * 2; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
+        __syncthreads();
+        // gather indices of a step: B (threads < CH) and A (threads < TA, first steps only)
+        auto loadIdx = [&](int ls, int& ib, int& ia) {
+            const CoordStep& d = sm.st[ls];
+            const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
+            const bool first = (w0 + ls == s0) || (fl & F_FIRST);
+            ib = (tid < CH && tid < nBv) ? __ldg(R.slots + d.bStart + tid) : -1;
+            ia = (first && tid < TA && tid < nAv) ? __ldg(R.slots + d.aStart + tid) : -1;
+        };
+        auto issue = [&](int ls, int ib, int ia) {
+            const CoordStep& d = sm.st[ls];
+            const int b = (w0 + ls - s0) & 1;
+            const int fl = d.packed >> 16;
+            const bool first = (w0 + ls == s0) || (fl & F_FIRST);
+            if (tid < CH) cpAsync16(&sm.pos[b][tid], d.posq + (ib >= 0 ? ib : 0), ib >= 0);
+            if (first && tid < TA) cpAsync16(&sm.apos[b][tid], d.posq + (ia >= 0 ? ia : 0), ia >= 0);
+            cpAsyncCommit();
+        };
+        int ib0, ia0, ib1 = -1, ia1 = -1;
+        loadIdx(0, ib0, ia0);
+        if (nw > 1) loadIdx(1, ib1, ia1);
+        issue(0, ib0, ia0);
+        if (nw > 1) issue(1, ib1, ia1);
+        cpAsyncWaitAll();
+        __syncthreads();
+        for (int ls = 0; ls < nw; ls++) {
+            const int s = w0 + ls;
+            const int b = (s - s0) & 1;
+            const CoordStep d = sm.st[ls];
+            const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
+            const bool first = (s == s0) || (fl & F_FIRST);
+            const bool last = (s == s1 - 1) || (fl & F_LAST);
+            int ib2 = -1, ia2 = -1;
+            if (ls + 2 < nw) loadIdx(ls + 2, ib2, ia2);
+            if (first) {
+                const CoordItem it = R.items[d.item];
+                K = runConst(it, R.sysBox[d.item / R.itemsPerSys]);
+#pragma unroll
+                for (int k = 0; k < RA; k++) {
+                    const float4 p = sm.apos[b][ty + NW * k];
+                    ax[k] = p.x * K.ir0; ay[k] = p.y * K.ir0; az[k] = p.z * K.ir0;
+                    gax[k] = gay[k] = gaz[k] = 0.0f;
+                }
+                cn = 0.0;
+                pieceSteps = 0;
+            }
+            pieceSteps++;
+            const float nir0 = -K.ir0;
+            float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
+#pragma unroll
+            for (int j = 0; j < RB; j++) {
+                const float4 p = sm.pos[b][lane + 32 * j];
+                bx[j] = p.x; by[j] = p.y; bz[j] = p.z;
+                gbx[j] = gby[j] = gbz[j] = 0.0f;
+            }
+            float cnc = 0.0f;
+            const bool full = nAv == TA && nBv == CH;
+            if (NH > 0 && full) {
+#pragma unroll
+                for (int k = 0; k < RA; k++) {
+#pragma unroll
+                    for (int j = 0; j < RB; j++) {
+                        float dx = fmaf(bx[j], nir0, ax[k]), dy = fmaf(by[j], nir0, ay[k]),
+                              dz = fmaf(bz[j], nir0, az[k]);
+                        imageS<BOX>(dx, dy, dz, K.box);
+                        const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        float f, h;
+                        switchX2<NH>(x2, HI ? (x2 >= K.lo && x2 < K.hi) : (x2 >= K.lo), K, f, h);
+                        cnc += f;
+                        gax[k] = fmaf(h, dx, gax[k]); gay[k] = fmaf(h, dy, gay[k]); gaz[k] = fmaf(h, dz, gaz[k]);
+                        gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < RA; k++) {
+                    const bool av = (ty + NW * k) < nAv;
+#pragma unroll
+                    for (int j = 0; j < RB; j++) {
+                        const bool bv = (lane + 32 * j) < nBv;
+                        float dx = fmaf(bx[j], nir0, ax[k]), dy = fmaf(by[j], nir0, ay[k]),
+                              dz = fmaf(bz[j], nir0, az[k]);
+                        imageS<BOX>(dx, dy, dz, K.box);
+                        const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        float f, h;
+                        switchX2<NH>(x2, av && bv && x2 >= K.lo && x2 < K.hi, K, f, h);
+                        cnc += f;
+                        gax[k] = fmaf(h, dx, gax[k]); gay[k] = fmaf(h, dy, gay[k]); gaz[k] = fmaf(h, dz, gaz[k]);
+                        gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
+                    }
+                }
+            }
+            cn += (double)cnc;
+            // B partials of this warp
+            float* gw = sm.g[b][ty];
+#pragma unroll
+            for (int j = 0; j < RB; j++) {
+                const int o = (lane + 32 * j) * 3;
+                gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
+            }
+            if (last) {
+                // A sums over lanes; lane 3k + c adds component c of atom k
+#pragma unroll
+                for (int k = 0; k < RA; k++) {
+                    const float x = warpSumF(gax[k]), y = warpSumF(gay[k]), z = warpSumF(gaz[k]);
+                    const int i = ty + NW * k;
+                    if (i < nAv) {
+                        unsigned long long* a = R.acc + 3 * (size_t)(d.rowA + i);
+                        if (lane == 3 * k) redAddI64(a, __float2ll_rn(x * FX));
+                        if (lane == 3 * k + 1) redAddI64(a + 1, __float2ll_rn(y * FX));
+                        if (lane == 3 * k + 2) redAddI64(a + 2, __float2ll_rn(z * FX));
+                    }
+                }
+                const double c = warpSum(cn);
+                if (lane == 0) sm.red[b][ty] = c;
+            }
+            cpAsyncWaitAll();
+            __syncthreads();
+            if (ls + 2 < nw) issue(ls + 2, ib2, ia2);
+            // B sums over warps in fixed order
+            for (int v = tid; v < CH * 3; v += blockDim.x) {
+                if (v / 3 < nBv) {
+                    float t = 0.0f;
+#pragma unroll
+                    for (int y = 0; y < NW; y++) t += sm.g[b][y][v];
+                    redAddI64(R.acc + 3 * (size_t)d.rowB + v, __float2ll_rn(t * FX));
+                }
+            }
+            if (last) {
+                if (tid == 0) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int y = 0; y < NW; y++) t += sm.red[b][y];
+                    redAddI64(R.cnAcc + d.item, __double2ll_rn(t * FXD));
+                }
+                hook(d.item, pieceSteps);
+            }
+        }
+    }
+}
+
+}  // namespace glued

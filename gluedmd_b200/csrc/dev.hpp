@@ -79,6 +79,7 @@ struct CoordItem {
     int partA;      // offset (float3 units) of this item's A partials: [splitsB][nA]
     int partB;      // offset of B partials: [tilesA][nB]
     int cn0;        // offset of this item's per-CTA CN partials
+    int row0;       // first fixed-point accumulator row (A rows, then B rows)
 };
 
 struct CoordDev {
@@ -90,6 +91,33 @@ struct CoordDev {
     float* partB;
     double* cnPart;
     int bSplit;            // B atoms per split (multiple of the B chunk)
+};
+
+// Coordination as static per-CTA runs of (A tile, B chunk) steps (coord_run.cuh).
+constexpr int COORD_NW = 8;     // warps per CTA
+constexpr int COORD_CH = 128;   // B atoms per chunk
+constexpr int COORD_F_FIRST = 1, COORD_F_LAST = 2;
+
+// One (tile, chunk) step. 32 bytes.
+struct __align__(16) CoordStep {
+    const float4* posq;  // positions of the item's system (slot order)
+    int item;
+    int aStart;          // index into slots of the tile's first A atom
+    int bStart;          // index into slots of the chunk's first B atom
+    int rowA;            // acc row of the tile's first A atom
+    int rowB;            // acc row of the chunk's first B atom
+    int packed;          // nAv | nBv << 8 | flags << 16 (COORD_F_*)
+};
+
+struct CoordRunDev {
+    const CoordItem* items;
+    const CoordStep* steps;
+    const int* begin;          // [grid + 1]: CTA b runs steps [begin[b], begin[b+1])
+    const int* slots;          // per coordination atom: its row in posq
+    const BoxDev* sysBox;      // box of system item / itemsPerSys
+    int itemsPerSys;
+    unsigned long long* acc;   // [rows][3] fixed-point gradient sums
+    unsigned long long* cnAcc; // [items] fixed-point CN
 };
 
 // Bias records, evaluated in the reference's bias-type order.

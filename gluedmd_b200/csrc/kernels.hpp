@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <vector>
 #include "../../include/glued_b200.h"
 #include "dev.hpp"
 
@@ -14,12 +15,22 @@ void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const Gr
                     double* cvv, const JacDev& J);
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
                      int numAtoms, int mode, double scale, const BoxDev* box);
-// parts: bit 0 = pair kernel, bit 1 = finalize kernel
+// Coordination runs (coord_run.cuh). parts: bit 0 = pair runs, bit 1 = finalize
+// (fixed-point sums -> Jacobian rows and CN values, accumulators cleared).
 // kind: switch kind shared by every item of the launch (3: n = 6, m = 12;
-// -1: other integer exponents; 0: non-integer exponents).
-void launchCoord(cudaStream_t s, const float4* posq, const int* u2g, const CoordDev& C, int numBlocks,
-                 int totalRows, int boxKind, int ra, int kind, const BoxDev* box, const JacDev& J, double* cvv,
-                 int parts = 3);
+// -1: other integer exponents; 0: non-integer exponents); hi: compare the upper
+// pair bound (cutoff or x <= 1000) in the full-tile path.
+void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, int totalRows, int boxKind, int kind,
+                 bool hi, const JacDev& J, double* cvv, int parts = 3);
+void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* slots, int n);
+int coordRunOccupancy(int kind, int boxKind, bool hi);
+// Host planning: steps tile-major (fills row0 / tilesA of the items, returns the
+// accumulator row count); per-CTA ranges of numSteps over grid CTAs with preCost[b]
+// steps' worth of other work on CTA b; whether the upper pair bound can bind.
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<const float4*>& posqOfItem,
+                    std::vector<CoordStep>& steps);
+std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost);
+bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic);
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies);
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
