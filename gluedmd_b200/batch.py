@@ -1,7 +1,7 @@
 """Batched multi-walker evaluation (glued_batch_* of include/glued_b200.h).
 
-All walkers of one GPU are evaluated by a single cooperative persistent launch
-per step. Each walker owns a float4 posq buffer and an int64 fixed-point force
+All walkers of one GPU are evaluated by one graph per step: a persistent
+kernel for the coordination pairs and the hill table, then a finalize kernel. Each walker owns a float4 posq buffer and an int64 fixed-point force
 buffer in device memory (torch tensors here); walkers may have different atom
 counts and boxes but the same CV / bias structure.
 """
@@ -144,27 +144,30 @@ class Batch:
         return v.value
 
     def phase_times(self):
-        """One step with per-CTA timestamps: dict of phase ends (us) and item counts."""
-        out = (c_double * 8)()
+        """One step with each launch bracketed by CUDA events and every CTA
+        time-stamped (microseconds); see glued_batch_phase_times."""
+        out = (c_double * 16)()
         call("glued_batch_phase_times", self._h, out)
-        return dict(phase_a_end_min_us=out[0], phase_a_end_max_us=out[1], barrier_exit_us=out[2],
-                    end_us=out[3], coord_items=int(out[4]), hill_items=int(out[5]),
-                    items_per_cta_max=int(out[6]), items_per_cta_min=int(out[7]))
+        keys = ["runs_us", "finalize_us", "hill_cvs_med_us", "hill_cvs_max_us", "coord_end_min_us",
+                "coord_end_med_us", "coord_end_max_us", "runs_end_med_us", "runs_end_max_us",
+                "fin_cta_med_us", "fin_cta_max_us", "fin_end_max_us", "coord_steps", "grid", "parts",
+                "finalize_grid"]
+        return dict(zip(keys, out[:]))
 
     @property
     def tuning(self):
         t = (c_int * 4)()
         call("glued_batch_get_tuning", self._h, t)
-        return dict(ra=t[0], b_split=t[1], hill_items=t[2], parts=t[3])
+        return dict(ra=t[0], parts=t[1], hill_weight_pct=t[2], hill_chunk=t[3])
 
-    def set_tuning(self, ra=8, b_split=256, hill_items=96, parts=4):
-        t = (c_int * 4)(ra, b_split, hill_items, parts)
+    def set_tuning(self, ra=8, parts=0, hill_weight_pct=150, hill_chunk=0):
+        t = (c_int * 4)(ra, parts, hill_weight_pct, hill_chunk)
         call("glued_batch_set_tuning", self._h, t)
 
     def autotune(self):
         t = (c_int * 4)()
         call("glued_batch_autotune", self._h, t)
-        return dict(ra=t[0], b_split=t[1], hill_items=t[2], parts=t[3])
+        return dict(ra=t[0], parts=t[1], hill_weight_pct=t[2], hill_chunk=t[3])
 
 
 def force_for(cvs, biases, pbc=True):

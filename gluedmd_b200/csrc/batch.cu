@@ -1,31 +1,25 @@
-// Batched multi-walker step: every walker's CVs, biases and force scatter in one
-// cooperative persistent launch per step (captured in a CUDA graph).
+// Batched multi-walker step: every walker's CVs, biases and force scatter in two
+// launches per step, captured in one CUDA graph.
 //
 // The reference steps one OpenMM Context per walker and shares the bias through
 // raw device pointers (tests/test_multiwalker.py:156-158,
 // platforms/common/src/CommonGluedKernels.cpp:5234-5262). Here all walkers of a
-// GPU are one launch:
+// GPU are evaluated together:
 //
-// Phase A (work items pulled from an atomic counter, heavy items first):
-//   - coordination tiles of every walker (coord_tile.cuh: partial gradients and
-//     CN partials, deterministic),
-//   - hill-table items: a chunk of 512 hills is staged into shared memory with a
-//     TMA bulk copy (cp.async.bulk + mbarrier, local memory only) and evaluated
-//     for up to 64 walkers (8 per warp); each item walks the chunks
-//     hill_items apart, so the launch shape does not depend on the hill count.
-//     Sums are FP32 per lane over <= ~16 terms, a fixed xor tree over the warp,
-//     and FP64 across items: a blocked summation with O((16 + 5) eps) error
-//     instead of O(N eps).
-// Grid barrier (bounded spin; on time-out the status word is set and the kernel
-//   returns).
-// Phase B (walker, part) items: the walker's CN (sum of its CTA partials),
-//   distance/angle/dihedral values and Jacobians, the shared hill bias
-//   (sum of item partials), harmonic restraints -> dU/dCV; then the walker's
-//   force rows are reduced from the partials and scattered straight into its
-//   2^32 fixed-point force buffer. No Jacobian table is materialised.
+//   1. Coordination runs (coord_run.cuh, launched through launchCoord): the
+//      (A tile, B chunk) steps of every walker's coordination CVs, walker-major,
+//      in equal static ranges over a persistent grid (SMs x resident CTAs);
+//      gradients accumulate in 64-bit fixed point, CN partials per run piece.
+//   2. k_batch_finalize, walkers x parts CTAs: each part clears and scatters its
+//      share of the walker's coordination rows (dU/dCN needs only CN and the
+//      harmonic terms: the hill bias acts on distance/angle/dihedral CVs) and
+//      evaluates its share of the shared hill table for that walker; the last
+//      part to finish sums the hill partials in part order and completes the
+//      walker (harmonic terms, energy, the distance/angle/dihedral rows).
 //
-// Deposition (updateState at pace): one hill per walker, in walker order, with
-// the well-tempered height from that walker's last hill-bias energy.
+// Every reduction has a fixed order or is an integer sum, so a step is bitwise
+// reproducible. Deposition (updateState at pace): one hill per walker, in walker
+// order, with the well-tempered height from that walker's last hill-bias energy.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,18 +28,20 @@
 
 #include "batch.hpp"
 #include "context.hpp"
-#include "coord_tile.cuh"
+#include "coord_run.cuh"
+#include "kernels.hpp"
 
 namespace glued {
 
 namespace {
-constexpr int HCH = 512;       // hills per staged chunk (float4: c0, c1, h, 0)
-constexpr int WBLK = 64;       // walkers per hill item (8 per warp)
 constexpr int MAXCV = 32;      // CV values per walker
 constexpr int MAXSIMPLE = 16;  // distance/angle/dihedral CVs per walker
 constexpr int MAXHARM = 32;    // harmonic terms per walker
-constexpr int SMEM_BYTES = 16384;
-}
+constexpr int FT = 256;        // threads of a finalize CTA
+constexpr int ROWS_PER_THREAD = 2;   // coordination rows one finalize thread scatters
+constexpr int WBLK = 64;       // walkers per hill item (8 per warp)
+constexpr int HC_MAX = 1024;   // hills per hill item, at most (shared-memory staging)
+}  // namespace
 
 struct BWalker {
     const float4* posq;
@@ -71,50 +67,20 @@ struct BatchDev {
     int W, nCV, nS, nC, nH;
     const BSimple* simple;  // [W][nS]
     const BHarm* harm;      // [W][nH]
-    CoordDev C;             // items [W][nC]
-    int coordBlocks;
-    int hillItems;          // per walker block
-    int nWB;                // walker blocks
-    int parts;
+    const CoordItem* items; // [W][nC]
+    CoordRunDev R;          // coordination step runs over all walkers' items
+    int rowsPerWalker;      // coordination rows of one walker (all its items)
+    int parts;              // finalize CTAs per walker
     BHill hill;
-    double* hillPart;       // [hillItems][W][3]
+    int nWB;                // walker blocks of <= WBLK walkers
+    int hc;                 // hills per hill item (multiple of 32, <= HC_MAX)
+    double* hillPart;       // [ceil(maxHills / hc)][W][3]
     double* cvv;            // [W][nCV]
     double* energy;         // [W]
     double* hillEnergy;     // [W]
-    unsigned int* bar;      // {count, generation}
-    int* work;
-    int* status;
-    unsigned long long spinLimit;
-    unsigned long long* stamps;  // optional [grid][6] phase timestamps (nullptr = off)
+    unsigned long long* stamps;   // profiling (nullptr = off): runs kernel [grid][4]
+    unsigned long long* fstamps;  // profiling (nullptr = off): finalize kernel [W * parts][2]
 };
-
-// ------------------------------------------------------------- grid barrier
-__device__ bool gridBarrier(unsigned int* bar, int* status, unsigned long long limit) {
-    __shared__ int sOk;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = bar + 1;
-        unsigned int gen = *vgen;
-        __threadfence();
-        unsigned int arrived = atomicAdd(bar, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned long long it = 0;
-            while (*vgen == gen) {
-                __nanosleep(100);
-                if (++it > limit) { atomicOr(status, 1); ok = 0; break; }
-            }
-        }
-        __threadfence();
-        sOk = ok;
-    }
-    __syncthreads();
-    return sOk != 0;
-}
 
 __device__ __forceinline__ unsigned long long globalTimer() {
     unsigned long long t;
@@ -122,268 +88,254 @@ __device__ __forceinline__ unsigned long long globalTimer() {
     return t;
 }
 
-// ------------------------------------------------------------- TMA helpers
-__device__ __forceinline__ unsigned smemAddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ double harmonicDU(const BHarm& hm, double v, double& E) {
+    const double TWO_PI = 6.283185307179586;
+    double ds = v - (double)hm.at;
+    if (hm.periodic) ds -= TWO_PI * round(ds / TWO_PI);
+    E += 0.5 * (double)hm.k * ds * ds;
+    return (double)hm.k * ds;
+}
 
-__device__ __forceinline__ bool mbarWait(unsigned mbar, unsigned parity, unsigned long long limit) {
-    unsigned long long it = 0;
-    for (;;) {
-        unsigned done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
-        if (done) return true;
-        if (++it > limit) return false;
-    }
+__device__ __forceinline__ void scatterRow(unsigned long long* F, int P, int atom, double g, float gx, float gy,
+                                           float gz) {
+    const double S = 4294967296.0;
+    atomicAdd(F + atom, (unsigned long long)(long long)(-(g * (double)gx) * S));
+    atomicAdd(F + atom + P, (unsigned long long)(long long)(-(g * (double)gy) * S));
+    atomicAdd(F + atom + 2 * P, (unsigned long long)(long long)(-(g * (double)gz) * S));
 }
 
 // ------------------------------------------------------------- hill items
-__device__ void hillItem(const BatchDev& B, int item, unsigned char* smem, unsigned long long* mbarPtr) {
-    const int h = item % B.hillItems;
-    const int wb = item / B.hillItems;
-    const int w0 = wb * WBLK;
-    const int nw = min(WBLK, B.W - w0);
-    float4* sH = reinterpret_cast<float4*>(smem);                 // HCH hills
-    float* sS = reinterpret_cast<float*>(smem + HCH * 16);         // [WBLK][2]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// One item: hc consecutive hills of the shared table against the <= 64 walkers
+// of one walker block. The walkers' hill-CV values are computed once per CTA
+// (sS, one thread per walker and CV); the chunk is staged in shared memory by
+// plain coalesced loads; warp w takes walkers w, w + 8, ...; lane l takes hills
+// l, l + 32, ...; FP32 sums per lane, a fixed xor tree per walker, one partial
+// per (item, walker), summed by the finalize in item order.
+__device__ void hillCVs(const BatchDev& B, int wb, float* sS) {
+    const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
     const BHill& hb = B.hill;
-    // CV values of this block's walkers the hill bias acts on
-    if (tid < nw) {
-        const int w = w0 + tid;
-        const BWalker& wk = B.walkers[w];
-        for (int d = 0; d < 2; d++) {
-            float v = 0.0f;
-            if (d < hb.D) {
-                for (int s = 0; s < B.nS; s++) {
-                    const BSimple& si = B.simple[w * B.nS + s];
-                    if (si.cv == hb.cv[d]) v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, nullptr);
-                }
+    const int t = threadIdx.x;
+    if (t < 2 * nw) {
+        const int w = w0 + t / 2, d = t % 2;
+        float v = 0.0f;
+        if (d < hb.D) {
+            const BWalker& wk = B.walkers[w];
+            for (int s = 0; s < B.nS; s++) {
+                const BSimple& si = B.simple[w * B.nS + s];
+                if (si.cv == hb.cv[d]) v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, nullptr);
             }
-            sS[tid * 2 + d] = v;
         }
+        sS[t] = v;
     }
-    const unsigned mbar = smemAddr(mbarPtr);
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    float acc[8][3];
-#pragma unroll
-    for (int j = 0; j < 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0f;
+}
+
+__device__ void hillItem(const BatchDev& B, int item, int itemsPerBlock, const float* sS, float4* sH) {
+    const BHill& hb = B.hill;
+    const int c = item % itemsPerBlock, wb = item / itemsPerBlock;
+    const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
     const int count = *hb.count;
-    unsigned parity = 0;
-    bool ok = true;
-    for (int c = h; c * HCH < count; c += B.hillItems) {
-        const int n = min(HCH, count - c * HCH);
-        if (tid == 0) {
-            unsigned bytes = (unsigned)n * 16u;
-            // shared memory may have been written through the generic proxy by an
-            // earlier item of this CTA
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smemAddr(sH)),
-                "l"(hb.mirror + (size_t)c * HCH), "r"(bytes), "r"(mbar)
-                : "memory");
+    const int hc = B.hc;
+    const int k0 = c * hc, n = max(0, min(hc, count - k0));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __syncthreads();  // sH free (previous item read), sS written
+    for (int k = tid; k < hc; k += blockDim.x)
+        sH[k] = k < n ? __ldg(hb.mirror + k0 + k) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    __syncthreads();
+    for (int wl = warp; wl < nw; wl += 8) {
+        const float s0 = sS[wl * 2], s1 = sS[wl * 2 + 1];
+        float V = 0.0f, g0 = 0.0f, g1 = 0.0f;
+#pragma unroll 4
+        for (int q = 0; q < hc / 32; q++) {
+            const float4 hk = sH[lane + 32 * q];   // height 0 past the end of the table
+            float dx = s0 - hk.x, dy = s1 - hk.y;
+            if (hb.period[0] > 0.0f) dx -= hb.period[0] * rintf(dx * hb.iperiod[0]);
+            if (hb.period[1] > 0.0f) dy -= hb.period[1] * rintf(dy * hb.iperiod[1]);
+            const float ex = dx * dx * hb.a[0] + dy * dy * hb.a[1];
+            const float g = ex <= 8.0f ? hk.z * __expf(-ex) : 0.0f;
+            V += g; g0 += g * dx; g1 += g * dy;
         }
-        // one thread waits (bounded) and the result is broadcast, so every
-        // thread takes the same path through the block barriers below
-        if (tid == 0) {
-            int got = mbarWait(mbar, parity, B.spinLimit) ? 1 : 0;
-            if (!got) atomicOr(B.status, 2);
-            *reinterpret_cast<volatile int*>(sS + 2 * WBLK) = got;
-        }
-        __syncthreads();
-        if (!*reinterpret_cast<volatile int*>(sS + 2 * WBLK)) { ok = false; break; }
-        parity ^= 1u;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int wl = warp + 8 * j;
-            if (wl < nw) {
-                const float s0 = sS[wl * 2], s1 = sS[wl * 2 + 1];
-                float V = 0.0f, g0 = 0.0f, g1 = 0.0f;
-                for (int k = lane; k < n; k += 32) {
-                    const float4 hk = sH[k];
-                    float dx = s0 - hk.x, dy = s1 - hk.y;
-                    if (hb.period[0] > 0.0f) dx -= hb.period[0] * rintf(dx * hb.iperiod[0]);
-                    if (hb.period[1] > 0.0f) dy -= hb.period[1] * rintf(dy * hb.iperiod[1]);
-                    const float ex = dx * dx * hb.a[0] + dy * dy * hb.a[1];
-                    const float g = ex <= 8.0f ? hk.z * __expf(-ex) : 0.0f;
-                    V += g; g0 += g * dx; g1 += g * dy;
-                }
-                acc[j][0] += V; acc[j][1] += g0; acc[j][2] += g1;
-            }
-        }
-        __syncthreads();  // chunk fully read before it is overwritten
-    }
-    if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
-    if (!ok) return;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const int wl = warp + 8 * j;
-        float V = warpSumF(acc[j][0]), g0 = warpSumF(acc[j][1]), g1 = warpSumF(acc[j][2]);
-        if (lane == 0 && wl < nw) {
-            double* out = B.hillPart + 3 * ((size_t)h * B.W + w0 + wl);
+        V = warpSumF(V); g0 = warpSumF(g0); g1 = warpSumF(g1);
+        if (lane == 0) {
+            double* out = B.hillPart + 3 * ((size_t)c * B.W + w0 + wl);
             out[0] = V;
             out[1] = -(double)g0 * hb.isig2[0];
             out[2] = -(double)g1 * hb.isig2[1];
         }
     }
-    __syncthreads();
+}
+
+// ------------------------------------------------------------- the runs
+// Persistent CTAs (grid = SMs x resident CTAs): CTA b runs its static range of
+// coordination steps, then its hill items b, b + grid, ... (ranges balanced so
+// that CTAs with more hill items get fewer steps).
+template <int RA, int BOX, int NH, bool HI>
+__global__ void __launch_bounds__(256, 2) k_batch_runs(BatchDev B) {
+    __shared__ CoordRunSmem<RA> sm;
+    __shared__ float sS[WBLK * 2];
+    const int numHill = B.hill.present ? ((*B.hill.count + B.hc - 1) / B.hc) * B.nWB : 0;
+    int wbHave = -1;
+    unsigned long long* st = B.stamps ? B.stamps + 4 * (size_t)blockIdx.x : nullptr;
+    if (st && threadIdx.x == 0) st[0] = globalTimer();
+    const int perBlock = numHill / max(B.nWB, 1);
+    if ((int)blockIdx.x < numHill) {
+        wbHave = blockIdx.x / perBlock;
+        hillCVs(B, wbHave, sS);
+    }
+    if (st) { __syncthreads(); if (threadIdx.x == 0) st[1] = globalTimer(); }
+    const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
+    if (s0 < s1) coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
+    if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
+    float4* sH = reinterpret_cast<float4*>(&sm.g[0][0][0]);
+    for (int item = blockIdx.x; item < numHill; item += gridDim.x) {
+        const int wb = item / perBlock;
+        if (wb != wbHave) {
+            __syncthreads();
+            hillCVs(B, wb, sS);
+            wbHave = wb;
+        }
+        hillItem(B, item, perBlock, sS, sH);
+    }
+    if (st) { __syncthreads(); if (threadIdx.x == 0) st[3] = globalTimer(); }
 }
 
 // ------------------------------------------------------------- finalize
-__device__ void finalizeWalker(const BatchDev& B, int w, int part, unsigned char* smem) {
-    double* sCV = reinterpret_cast<double*>(smem);           // [MAXCV]
-    double* sdU = sCV + MAXCV;                               // [MAXCV]
-    double* sScal = sdU + MAXCV;                             // [4]
-    F3* sJac = reinterpret_cast<F3*>(sScal + 4);             // [MAXSIMPLE][4]
+// CTA (walker w, part p) after the runs. Every part clears and scatters its share
+// of the walker's coordination rows (at most ROWS_PER_THREAD per thread) with
+// dU/dCN, which needs only CN (the walker's run-piece partials in step order)
+// and the harmonic terms: the hill bias acts only on distance/angle/dihedral
+// CVs. Part 0 also computes those CVs and their Jacobians, sums the hill
+// partials in item order (fixed tree), evaluates the harmonic terms and the hill
+// bias, writes CVs and energies and scatters the distance/angle/dihedral rows.
+__global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
+    __shared__ double sCV[MAXCV], sdU[MAXCV];
+    __shared__ F3 sJac[MAXSIMPLE * 4];
+    __shared__ double red[32 * 3];
+    const int w = blockIdx.x / B.parts, part = blockIdx.x % B.parts;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long* st = B.fstamps ? B.fstamps + 2 * (size_t)blockIdx.x : nullptr;
+    if (st && tid == 0) st[0] = globalTimer();
     const BWalker& wk = B.walkers[w];
+    // First what does not depend on the runs kernel's results: the rows'
+    // accumulator slots and atoms, the distance/angle/dihedral values and
+    // Jacobians; then the fixed-point row sums (cleared as read), CN, hill partials.
+    const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
+    const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
+    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD], rRow[ROWS_PER_THREAD];
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        const int r = r0 + tid + FT * q;
+        rItem[q] = -1; rAtom[q] = 0; rRow[q] = 0;
+        if (r < r1) {
+            // the walker's rows: item 0's A and B rows, then item 1's, ...
+            int c = 0, base = 0;
+            while (c < B.nC - 1 && r >= base + B.items[w * B.nC + c].nA + B.items[w * B.nC + c].nB) {
+                base += B.items[w * B.nC + c].nA + B.items[w * B.nC + c].nB;
+                c++;
+            }
+            const CoordItem& it = B.items[w * B.nC + c];
+            const int i = r - base;
+            rItem[q] = c;
+            rRow[q] = it.row0 + i;
+            rAtom[q] = B.R.slots[i < it.nA ? it.a0 + i : it.b0 + (i - it.nA)];
+        }
+    }
     if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
     __syncthreads();
-    if (tid < B.nS) {
+    if (part == 0 && tid < B.nS) {
         const BSimple& si = B.simple[w * B.nS + tid];
         F3 jac[4];
-        float v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, jac);
+        const float v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, jac);
         for (int k = 0; k < 4; k++) sJac[tid * 4 + k] = jac[k];
         sCV[si.cv] = (double)v;
     }
+    long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        vx[q] = vy[q] = vz[q] = 0;
+        if (rItem[q] >= 0) {
+            unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
+            vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
+            a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
+        }
+    }
     if (warp == 1) {
         for (int c = 0; c < B.nC; c++) {
-            const CoordItem& it = B.C.items[w * B.nC + c];
-            int nb = it.tilesA * it.splitsB;
-            double s = 0;
-            for (int k = lane; k < nb; k += 32) s += B.C.cnPart[it.cn0 + k];
-            s = warpSum(s);
-            if (lane == 0) sCV[it.cv] = s;
+            const int ii = w * B.nC + c;
+            double t = 0.0;
+            // pieces in step order: lane k takes pieces k, k + 32, ...; fixed tree
+            for (int k = B.R.pieceBegin[ii] + lane; k < B.R.pieceBegin[ii + 1]; k += 32)
+                t += __ldcg(B.R.cnPiece + B.R.pieceStep[k]);
+            t = warpSum(t);
+            if (lane == 0) sCV[B.items[ii].cv] = t;
         }
     }
-    if (warp == 2 && B.hill.present) {
-        double v[3] = {0, 0, 0};
-        for (int h = lane; h < B.hillItems; h += 32) {
-            const double* p = B.hillPart + 3 * ((size_t)h * B.W + w);
-            v[0] += p[0]; v[1] += p[1]; v[2] += p[2];
+    double hv[3] = {0.0, 0.0, 0.0};
+    if (part == 0 && B.hill.present) {
+        const int items = (*B.hill.count + B.hc - 1) / B.hc;
+        for (int c = tid; c < items; c += FT) {
+            const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
+            hv[0] += __ldcg(q); hv[1] += __ldcg(q + 1); hv[2] += __ldcg(q + 2);
         }
-        for (int k = 0; k < 3; k++) v[k] = warpSum(v[k]);
-        if (lane == 0) { sScal[0] = v[0]; sScal[1] = v[1]; sScal[2] = v[2]; }
     }
-    __syncthreads();
+    if (part == 0) blockSum<3>(hv, red);   // part-uniform: every thread of part 0 takes part
+    else __syncthreads();
+    // dU/dCV: part 0 everything, the other parts the coordination CVs only
     if (tid == 0) {
-        const double TWO_PI = 6.283185307179586;
         double E = 0.0;
         for (int k = 0; k < B.nH; k++) {
             const BHarm& hm = B.harm[w * B.nH + k];
-            double ds = sCV[hm.cv] - (double)hm.at;
-            if (hm.periodic) ds -= TWO_PI * round(ds / TWO_PI);
-            E += 0.5 * (double)hm.k * ds * ds;
-            sdU[hm.cv] += (double)hm.k * ds;
-        }
-        if (B.hill.present) {
-            E += sScal[0];
-            sdU[B.hill.cv[0]] += sScal[1];
-            if (B.hill.D > 1) sdU[B.hill.cv[1]] += sScal[2];
+            bool coordCv = false;
+            for (int c = 0; c < B.nC; c++) coordCv = coordCv || B.items[w * B.nC + c].cv == hm.cv;
+            if (part == 0 || coordCv) sdU[hm.cv] += harmonicDU(hm, sCV[hm.cv], E);
         }
         if (part == 0) {
+            if (B.hill.present) {
+                E += hv[0];
+                sdU[B.hill.cv[0]] += hv[1];
+                if (B.hill.D > 1) sdU[B.hill.cv[1]] += hv[2];
+            }
             for (int k = 0; k < B.nCV; k++) B.cvv[(size_t)w * B.nCV + k] = sCV[k];
             B.energy[w] = E;
-            B.hillEnergy[w] = B.hill.present ? sScal[0] : 0.0;
+            B.hillEnergy[w] = B.hill.present ? hv[0] : 0.0;
         }
     }
     __syncthreads();
-    const double S = 4294967296.0;
     unsigned long long* F = wk.force;
     const int P = wk.padded;
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        if (rItem[q] < 0) continue;
+        const CoordItem& it = B.items[w * B.nC + rItem[q]];
+        const double g = sdU[it.cv];
+        if (g == 0.0) continue;
+        const double sc = coordAccScale(it) * crun::IFXD;
+        scatterRow(F, P, rAtom[q], g, (float)((double)vx[q] * sc), (float)((double)vy[q] * sc),
+                   (float)((double)vz[q] * sc));
+    }
     if (part == 0 && tid < B.nS * 4) {
         const BSimple& si = B.simple[w * B.nS + tid / 4];
         const int k = tid % 4;
         const int na = si.type == 1 ? 2 : si.type == 2 ? 3 : 4;
         const double g = sdU[si.cv];
         if (k < na && g != 0.0) {
-            F3 j = sJac[tid];
-            int a = si.atoms[k];
-            atomicAdd(F + a, (unsigned long long)(long long)(-(g * (double)j.x) * S));
-            atomicAdd(F + a + P, (unsigned long long)(long long)(-(g * (double)j.y) * S));
-            atomicAdd(F + a + 2 * P, (unsigned long long)(long long)(-(g * (double)j.z) * S));
+            const F3 j = sJac[tid];
+            scatterRow(F, P, si.atoms[k], g, j.x, j.y, j.z);
         }
     }
-    for (int c = 0; c < B.nC; c++) {
-        const CoordItem& it = B.C.items[w * B.nC + c];
-        const double g = sdU[it.cv];
-        if (g == 0.0) continue;
-        const int R = it.nA + it.nB;
-        const int r0 = (int)((long long)R * part / B.parts), r1 = (int)((long long)R * (part + 1) / B.parts);
-        for (int i = r0 + tid; i < r1; i += blockDim.x) {
-            double x = 0, y = 0, z = 0;
-            int atom;
-            if (i < it.nA) {
-                const float* p = B.C.partA + 3 * ((size_t)it.partA + i);
-                for (int sb = 0; sb < it.splitsB; sb++) {
-                    const float* q = p + 3 * (size_t)sb * it.nA;
-                    x += q[0]; y += q[1]; z += q[2];
-                }
-                atom = B.C.atoms[it.a0 + i];
-            } else {
-                const int b = i - it.nA;
-                const float* p = B.C.partB + 3 * ((size_t)it.partB + b);
-                for (int ta = 0; ta < it.tilesA; ta++) {
-                    const float* q = p + 3 * (size_t)ta * it.nB;
-                    x += q[0]; y += q[1]; z += q[2];
-                }
-                atom = B.C.atoms[it.b0 + b];
-            }
-            // Same rounding as the per-context path: the gradient is stored as float.
-            const float gx = (float)x, gy = (float)y, gz = (float)z;
-            atomicAdd(F + atom, (unsigned long long)(long long)(-(g * (double)gx) * S));
-            atomicAdd(F + atom + P, (unsigned long long)(long long)(-(g * (double)gy) * S));
-            atomicAdd(F + atom + 2 * P, (unsigned long long)(long long)(-(g * (double)gz) * S));
-        }
-    }
-    __syncthreads();
+    if (st) { __syncthreads(); if (tid == 0) st[1] = globalTimer(); }
 }
 
-// ------------------------------------------------------------- the step
-template <int RA, int BOX, int NH>
-__global__ void __launch_bounds__(256, 2) k_batch_step(BatchDev B) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ int sItem;
-    __shared__ double red[32];
-    __shared__ __align__(8) unsigned long long mbar;
-    const int tid = threadIdx.x;
-    const int numA = B.coordBlocks + B.hillItems * B.nWB;
-    unsigned long long* stamp = B.stamps ? B.stamps + 6 * (size_t)blockIdx.x : nullptr;
-    int nCoord = 0, nHill = 0;
-    if (stamp && tid == 0) stamp[0] = globalTimer();
-    for (;;) {
-        if (tid == 0) sItem = atomicAdd(B.work, 1);
-        __syncthreads();
-        const int item = sItem;
-        __syncthreads();
-        if (item >= numA) break;
-        if (item < B.coordBlocks) {
-            const int ci = B.C.blockItem[item];
-            const CoordItem it = B.C.items[ci];
-            const BWalker& wk = B.walkers[ci / B.nC];
-            const BoxDev box = wk.box;
-            const int local = item - it.block0;
-            const int ta = local / it.splitsB, sb = local % it.splitsB;
-            float (*sB)[TB * 3] = reinterpret_cast<float (*)[TB * 3]>(smem);
-            coordTile<RA, BOX, NH>(wk.posq, nullptr, B.C, it, ta, sb, box, sB, red);
-            __syncthreads();
-            nCoord++;
-        } else {
-            hillItem(B, item - B.coordBlocks, smem, &mbar);
-            nHill++;
-        }
-    }
-    if (stamp && tid == 0) { stamp[1] = globalTimer(); stamp[4] = nCoord; stamp[5] = nHill; }
-    if (!gridBarrier(B.bar, B.status, B.spinLimit)) return;
-    if (stamp && tid == 0) stamp[2] = globalTimer();
-    if (blockIdx.x == 0 && tid == 0) *B.work = 0;
-    for (int p = blockIdx.x; p < B.W * B.parts; p += gridDim.x) finalizeWalker(B, p / B.parts, p % B.parts, smem);
-    if (stamp && tid == 0) stamp[3] = globalTimer();
+typedef void (*RunsFn)(BatchDev);
+
+template <int NH>
+RunsFn runsKernelB(int box, bool hi) {
+    if (box == 0) return k_batch_runs<8, 0, NH, true>;
+    if (box == 1) return hi ? k_batch_runs<8, 1, NH, true> : k_batch_runs<8, 1, NH, false>;
+    return hi ? k_batch_runs<8, 2, NH, true> : k_batch_runs<8, 2, NH, false>;
+}
+
+RunsFn runsKernel(int box, int kind, bool hi) {
+    return kind == 3 ? runsKernelB<3>(box, hi) : kind == -1 ? runsKernelB<-1>(box, true) : runsKernelB<0>(box, true);
 }
 
 __global__ void k_batch_deposit(BatchDev B) {
@@ -407,112 +359,143 @@ __global__ void k_batch_deposit(BatchDev B) {
     if (threadIdx.x == 0) *hb.count = min(hb.maxH, n0 + B.W);
 }
 
-typedef void (*StepFn)(BatchDev);
-
-template <int RA, int NH>
-StepFn stepKernelB(int box) {
-    return box == 0 ? k_batch_step<RA, 0, NH> : box == 1 ? k_batch_step<RA, 1, NH> : k_batch_step<RA, 2, NH>;
-}
-
-template <int RA>
-StepFn stepKernelK(int box, int kind) {
-    return kind == 3 ? stepKernelB<RA, 3>(box) : kind == -1 ? stepKernelB<RA, -1>(box) : stepKernelB<RA, 0>(box);
-}
-
-StepFn stepKernel(int ra, int box, int kind) {
-    return ra == 4 ? stepKernelK<4>(box, kind) : stepKernelK<8>(box, kind);
-}
-
 // ================================================================== host
 struct Batch::Impl {
     int W = 0, nCV = 0, nS = 0, nC = 0, nH = 0, boxKind = 1, kind = 3;
     std::vector<BWalker> walkersH;
     std::vector<CoordItem> items;
     std::vector<int> coordAtoms;
-    DBuf walkersD, simpleD, harmD, itemsD, atomsD, blockItemD, partA, partB, cnPart, hillPart;
-    DBuf cvv, energy, hillEnergy, bar, work, status, scratchForce;
+    std::vector<CoordStep> steps;
+    DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, acc, cnPiece, pieceStepD, pieceBeginD;
+    DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
     DBuf hMirror, hCenters, hHeights, hCount;
     BHill hill{};
     BatchTuning tune;
     BatchDev dev{};
-    int grid = 0;
+    int grid = 0;        // coordination runs: SMs x resident CTAs
+    int rows = 0;        // coordination rows of one walker
+    int parts = 1;       // finalize CTAs per walker
+    int nWB = 1;         // walker blocks of the hill items
+    int hillCountHost = 0;   // host mirror of the hill count (set_hills + deposits)
+    int balancedItems = -1;  // hill items the current ranges were balanced for
+    bool hi = true;
     cudaStream_t stream = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t graph = nullptr;
     long long launches = 0;
     int lastUpdateStep = -1;
     bool ready = false;
-    bool useGraph = true;
     float lastMs = 0;
 
     void destroyGraph() {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
     }
 
+    RunsFn runs() const { return runsKernel(boxKind, kind, hi); }
+    int hcHill() const { return tune.hillChunk > 0 ? tune.hillChunk : 512; }
+
+    // Per-CTA step ranges: CTA b also evaluates hill items b, b + grid, ...,
+    // charged hillWeightPct percent of a step each; piece table to match.
+    void balance() {
+        const int nItems = hill.present ? ((hillCountHost + hcHill() - 1) / hcHill()) * ((W + WBLK - 1) / WBLK) : 0;
+        std::vector<double> pre(grid, 0.0);
+        for (int h = 0; h < nItems; h++) pre[h % grid] += tune.hillWeightPct / 100.0;
+        std::vector<int> begin = balanceRanges((int)steps.size(), grid, pre);
+        std::vector<int> pieceStep, pieceBegin;
+        buildCoordPieces(steps, begin, (int)items.size(), pieceStep, pieceBegin);
+        if (pieceStep.empty()) pieceStep.push_back(0);
+        // same buffers across rebalances: a captured graph keeps their addresses
+        auto put = [&](DBuf& d, const std::vector<int>& v) {
+            if (d.bytes < sizeof(int) * v.size()) {
+                d.alloc(sizeof(int) * std::max(v.size(), (size_t)grid + 1 + pieceStep.size()));
+                destroyGraph();
+            }
+            cudaCheck(cudaMemcpy(d.p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice), "ranges");
+        };
+        put(beginD, begin);
+        put(pieceStepD, pieceStep);
+        put(pieceBeginD, pieceBegin);
+        balancedItems = nItems;
+        dev.R.begin = beginD.as<int>();
+        dev.R.pieceStep = pieceStepD.as<int>();
+        dev.R.pieceBegin = pieceBeginD.as<int>();
+    }
+
+    int minParts() const { return std::max(1, (rows + FT * ROWS_PER_THREAD - 1) / (FT * ROWS_PER_THREAD)); }
+
     void plan() {
-        const int TA = 8 * tune.ra;
-        int blocks = 0, pa = 0, pb = 0, cn = 0;
-        std::vector<int> blockItem;
-        for (size_t i = 0; i < items.size(); i++) {
-            CoordItem& it = items[i];
-            it.tilesA = std::max(1, (it.nA + TA - 1) / TA);
-            it.splitsB = std::max(1, (it.nB + tune.bSplit - 1) / tune.bSplit);
-            it.block0 = blocks;
-            it.partA = pa; it.partB = pb; it.cn0 = cn;
-            const int nb = it.tilesA * it.splitsB;
-            blocks += nb; cn += nb;
-            pa += it.splitsB * it.nA; pb += it.tilesA * it.nB;
-        }
-        // heavy items first: order the coordination blocks walker-interleaved
-        blockItem.resize(blocks);
-        for (size_t i = 0; i < items.size(); i++)
-            for (int k = 0; k < items[i].tilesA * items[i].splitsB; k++) blockItem[items[i].block0 + k] = (int)i;
+        // coordination steps over all walkers' items (walker-major)
+        std::vector<const float4*> posqOf(items.size());
+        for (size_t i = 0; i < items.size(); i++) posqOf[i] = walkersH[i / std::max(nC, 1)].posq;
+        buildCoordSteps(items, 8, posqOf, steps);
+        rows = 0;
+        for (int c = 0; c < nC; c++) rows += items[c].nA + items[c].nB;
         itemsD.upload(items);
-        blockItemD.upload(blockItem);
-        if (partA.bytes < sizeof(float) * 3 * (size_t)std::max(pa, 1)) partA.alloc(sizeof(float) * 3 * std::max(pa, 1));
-        if (partB.bytes < sizeof(float) * 3 * (size_t)std::max(pb, 1)) partB.alloc(sizeof(float) * 3 * std::max(pb, 1));
-        if (cnPart.bytes < sizeof(double) * (size_t)std::max(cn, 1)) cnPart.alloc(sizeof(double) * std::max(cn, 1));
-        const int nWB = (W + WBLK - 1) / WBLK;
-        size_t hp = sizeof(double) * 3 * (size_t)tune.hillItems * W;
-        if (hillPart.bytes < hp) hillPart.alloc(hp);
+        stepsD.upload(steps);
+        const size_t accRows = (size_t)std::max(1, rows) * W;
+        if (acc.bytes < sizeof(unsigned long long) * 3 * accRows) acc.alloc(sizeof(unsigned long long) * 3 * accRows);
+        cudaCheck(cudaMemset(acc.p, 0, acc.bytes), "reset");
+        cnPiece.alloc(sizeof(double) * std::max((size_t)1, steps.size()));
+        std::vector<BoxDev> boxes(W);
+        for (int w = 0; w < W; w++) boxes[w] = walkersH[w].box;
+        boxesD.upload(boxes);
+        hi = false;
+        for (int w = 0; w < W && nC > 0; w++) {
+            const BoxDev& b = walkersH[w].box;
+            double box9[9] = {b.a[0], b.a[1], b.a[2], b.b[0], b.b[1], b.b[2], b.c[0], b.c[1], b.c[2]};
+            std::vector<CoordItem> mine(items.begin() + w * nC, items.begin() + (w + 1) * nC);
+            if (coordNeedsHi(mine, box9, boxKind != 0)) hi = true;
+        }
+        int dev_ = 0, sms = 0;
+        cudaCheck(cudaGetDevice(&dev_), "device");
+        cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_), "attr");
+        cudaCheck(cudaFuncSetAttribute((const void*)runs(), cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared), "carveout");
+        int perSM = 0;
+        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)runs(), 256, 0), "occupancy");
+        if (perSM < 1) throw Error(GLUED_E_CUDA, "batched runs kernel cannot be resident");
+        grid = sms * perSM;
+        balance();
+        parts = tune.parts > 0 ? std::max(minParts(), tune.parts) : minParts();
+        nWB = (W + WBLK - 1) / WBLK;
+        if (hill.present) hillPart.alloc(sizeof(double) * 3 * (size_t)W * ((hill.maxH + hcHill() - 1) / hcHill()));
         dev.walkers = walkersD.as<BWalker>();
         dev.W = W; dev.nCV = nCV; dev.nS = nS; dev.nC = nC; dev.nH = nH;
         dev.simple = simpleD.as<BSimple>();
         dev.harm = harmD.as<BHarm>();
-        dev.C.items = itemsD.as<CoordItem>();
-        dev.C.numItems = (int)items.size();
-        dev.C.atoms = atomsD.as<int>();
-        dev.C.blockItem = blockItemD.as<int>();
-        dev.C.partA = partA.as<float>(); dev.C.partB = partB.as<float>(); dev.C.cnPart = cnPart.as<double>();
-        dev.C.bSplit = tune.bSplit;
-        dev.coordBlocks = blocks;
-        dev.hillItems = hill.present ? tune.hillItems : 0;
-        dev.nWB = hill.present ? nWB : 0;
-        dev.parts = tune.parts;
+        dev.items = itemsD.as<CoordItem>();
+        dev.R.items = itemsD.as<CoordItem>();
+        dev.R.steps = stepsD.as<CoordStep>();
+        dev.R.slots = atomsD.as<int>();
+        dev.R.sysBox = boxesD.as<BoxDev>();
+        dev.R.itemsPerSys = std::max(nC, 1);
+        dev.R.acc = acc.as<unsigned long long>();
+        dev.R.cnPiece = cnPiece.as<double>();
+        dev.rowsPerWalker = rows;
+        dev.parts = parts;
         dev.hill = hill;
         dev.hillPart = hillPart.as<double>();
+        dev.nWB = nWB;
+        dev.hc = hcHill();
         dev.cvv = cvv.as<double>(); dev.energy = energy.as<double>(); dev.hillEnergy = hillEnergy.as<double>();
-        dev.bar = bar.as<unsigned int>(); dev.work = work.as<int>(); dev.status = status.as<int>();
-        dev.spinLimit = 1ull << 24;
-        cudaCheck(cudaMemset(bar.p, 0, bar.bytes), "reset");
-        cudaCheck(cudaMemset(work.p, 0, work.bytes), "reset");
-        cudaCheck(cudaMemset(status.p, 0, status.bytes), "reset");
-        StepFn fn = stepKernel(tune.ra, boxKind, kind);
-        int dev_ = 0, sms = 0, perSM = 0;
-        cudaCheck(cudaGetDevice(&dev_), "device");
-        cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_), "attr");
-        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)fn, 256, SMEM_BYTES), "occupancy");
-        if (perSM < 1) throw Error(GLUED_E_CUDA, "batched step kernel cannot be resident");
-        grid = sms * perSM;
         destroyGraph();
     }
 
-    void launch(cudaStream_t s) {
-        StepFn fn = stepKernel(tune.ra, boxKind, kind);
+    void launchRuns(cudaStream_t s) {
         void* args[] = {&dev};
-        cudaCheck(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(256), args, SMEM_BYTES, s),
-                  "cooperative launch");
+        cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(256), args, 0, s), "runs");
     }
+    void launchFinalize(cudaStream_t s) {
+        void* args[] = {&dev};
+        cudaCheck(cudaLaunchKernel((const void*)k_batch_finalize, dim3(W * parts), dim3(FT), args, 0, s), "finalize");
+    }
+    // The step's launches on stream s: coordination runs, then the finalize.
+    void launch(cudaStream_t s) {
+        launchRuns(s);
+        launchFinalize(s);
+        cudaCheck(cudaGetLastError(), "step launch");
+    }
+    int launchesPerStep() const { return 2; }
 };
 
 Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_desc* walkers) : impl_(new Impl()) {
@@ -673,14 +656,8 @@ Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_de
     I.cvv.alloc(sizeof(double) * (size_t)I.W * std::max(I.nCV, 1));
     I.energy.alloc(sizeof(double) * I.W);
     I.hillEnergy.alloc(sizeof(double) * I.W);
-    I.bar.alloc(sizeof(unsigned int) * 4);
-    I.work.alloc(sizeof(int) * 4);
     I.status.alloc(sizeof(int) * 4);
     cudaCheck(cudaStreamCreateWithFlags(&I.cap, cudaStreamNonBlocking), "stream");
-    for (int r : {4, 8}) {
-        StepFn fn = stepKernel(r, I.boxKind, I.kind);
-        cudaCheck(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES), "attr");
-    }
     I.plan();
 }
 
@@ -697,9 +674,12 @@ void Batch::setStream(cudaStream_t s) {
 }
 
 void Batch::setTuning(const BatchTuning& t) {
-    if (t.ra != 4 && t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 4 or 8");
-    if (t.bSplit < 128 || t.bSplit % 128) throw Error(GLUED_E_INVALID, "batch tuning: bSplit must be a multiple of 128");
-    if (t.hillItems < 1 || t.parts < 1) throw Error(GLUED_E_INVALID, "batch tuning: hillItems and parts must be >= 1");
+    if (t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 8");
+    if (t.parts < 0 || t.parts > 4096) throw Error(GLUED_E_INVALID, "batch tuning: finalize parts must be 0..4096");
+    if (t.hillWeightPct < 0 || t.hillWeightPct > 10000)
+        throw Error(GLUED_E_INVALID, "batch tuning: hill weight must be 0..10000 percent of a step");
+    if (t.hillChunk != 0 && (t.hillChunk < 128 || t.hillChunk > HC_MAX || t.hillChunk % 128))
+        throw Error(GLUED_E_INVALID, "batch tuning: hill chunk must be 0 or a multiple of 128 up to 1024");
     cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
     impl_->tune = t;
     impl_->plan();
@@ -709,34 +689,29 @@ BatchTuning Batch::tuning() const { return impl_->tune; }
 
 void Batch::execute() {
     Impl& I = *impl_;
-    if (!I.graph && I.useGraph) {
+    if (!I.graph) {
         cudaGraph_t g = nullptr;
-        bool ok = cudaStreamBeginCapture(I.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-        if (ok) {
-            StepFn fn = stepKernel(I.tune.ra, I.boxKind, I.kind);
-            void* args[] = {&I.dev};
-            cudaError_t le = cudaLaunchCooperativeKernel((const void*)fn, dim3(I.grid), dim3(256), args, SMEM_BYTES, I.cap);
-            cudaError_t ce = cudaStreamEndCapture(I.cap, &g);
-            ok = le == cudaSuccess && ce == cudaSuccess && g &&
-                 cudaGraphInstantiate(&I.graph, g, 0) == cudaSuccess;
+        cudaCheck(cudaStreamBeginCapture(I.cap, cudaStreamCaptureModeThreadLocal), "capture begin");
+        try {
+            I.launch(I.cap);
+        } catch (...) {
+            cudaStreamEndCapture(I.cap, &g);
             if (g) cudaGraphDestroy(g);
+            throw;
         }
-        if (!ok) {
-            // cooperative launches are not capturable here: launch directly
-            cudaGetLastError();
-            I.graph = nullptr;
-            I.useGraph = false;
-        }
+        cudaCheck(cudaStreamEndCapture(I.cap, &g), "capture end");
+        cudaError_t ie = cudaGraphInstantiate(&I.graph, g, 0);
+        cudaGraphDestroy(g);
+        cudaCheck(ie, "graph instantiate");
     }
-    if (I.graph) cudaCheck(cudaGraphLaunch(I.graph, I.stream), "graph launch");
-    else I.launch(I.stream);
-    I.launches++;
+    cudaCheck(cudaGraphLaunch(I.graph, I.stream), "graph launch");
+    I.launches += I.launchesPerStep();
     I.ready = true;
 }
 
-// Autotuner: tile shape, B split, hill items and finalize parts are timed on
-// the live walkers with CUDA events (forces go to a scratch buffer) and the
-// fastest combination is kept.
+// Autotuner: finalize CTAs per walker and the weight of a hill item in the range
+// balance are timed on the live walkers with CUDA events (forces go to a scratch
+// buffer) and the fastest combination is kept.
 BatchTuning Batch::autotune() {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
@@ -752,26 +727,27 @@ BatchTuning Batch::autotune() {
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
     const BatchTuning saved = I.tune;
-    for (int ra : {4, 8})
-        for (int bs : {128, 256, 512})
-            for (int hi : {32, 64, 128, 256})
-                for (int parts : {2, 4, 8}) {
-                    BatchTuning t;
-                    t.ra = ra; t.bSplit = bs; t.hillItems = hi; t.parts = parts;
-                    I.tune = t;
-                    I.plan();
-                    for (int r = 0; r < 2; r++) I.launch(I.stream);
-                    cudaCheck(cudaEventRecord(a, I.stream), "event");
-                    const int reps = 8;
-                    for (int r = 0; r < reps; r++) I.launch(I.stream);
-                    cudaCheck(cudaEventRecord(b, I.stream), "event");
-                    cudaCheck(cudaEventSynchronize(b), "event");
-                    float ms = 0;
-                    cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
-                    ms /= reps;
-                    I.launches += reps + 2;
-                    if (ms < bestMs) { bestMs = ms; best = t; }
-                }
+    const int base = I.minParts();
+    for (int hc : {256, 512, 1024})
+        for (int pct : {100, 150, 200, 300})
+            for (int mul : {1, 2}) {
+                if (!I.hill.present && (hc != 512 || pct != 150)) continue;
+                BatchTuning t;
+                t.ra = 8; t.parts = base * mul; t.hillWeightPct = pct; t.hillChunk = hc;
+                I.tune = t;
+                I.plan();
+                for (int r = 0; r < 2; r++) I.launch(I.stream);
+                cudaCheck(cudaEventRecord(a, I.stream), "event");
+                const int reps = 8;
+                for (int r = 0; r < reps; r++) I.launch(I.stream);
+                cudaCheck(cudaEventRecord(b, I.stream), "event");
+                cudaCheck(cudaEventSynchronize(b), "event");
+                float ms = 0;
+                cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
+                ms /= reps;
+                I.launches += (long long)(reps + 2) * I.launchesPerStep();
+                if (ms < bestMs) { bestMs = ms; best = t; }
+            }
     (void)saved;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -789,35 +765,61 @@ BatchTuning Batch::autotune() {
 // coordination / hill items it processed. out[0..7]: phase-A end (earliest,
 // latest CTA), barrier exit (latest), exit (latest) in microseconds after the
 // earliest entry; coordination items, hill items, most and fewest items per CTA.
+// Percentile p (0..100) of v (sorted in place).
+static double pct(std::vector<double>& v, double p) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    size_t i = (size_t)std::min((double)v.size() - 1, std::floor(p / 100.0 * (double)(v.size() - 1) + 0.5));
+    return v[i];
+}
+
 void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
+    const int fg = I.W * I.parts;
     DBuf st;
-    st.alloc(sizeof(unsigned long long) * 6 * (size_t)I.grid);
+    st.alloc(sizeof(unsigned long long) * (4 * (size_t)I.grid + 2 * (size_t)fg));
     cudaCheck(cudaMemsetAsync(st.p, 0, st.bytes, I.stream), "stamps");
     I.dev.stamps = st.as<unsigned long long>();
-    I.launch(I.stream);
+    I.dev.fstamps = st.as<unsigned long long>() + 4 * (size_t)I.grid;
+    cudaEvent_t e[3];
+    for (auto& x : e) cudaCheck(cudaEventCreate(&x), "event");
+    cudaCheck(cudaEventRecord(e[0], I.stream), "event");
+    I.launchRuns(I.stream);
+    cudaCheck(cudaEventRecord(e[1], I.stream), "event");
+    I.launchFinalize(I.stream);
+    cudaCheck(cudaEventRecord(e[2], I.stream), "event");
     I.dev.stamps = nullptr;
-    I.launches++;
+    I.dev.fstamps = nullptr;
+    cudaCheck(cudaEventSynchronize(e[2]), "event");
+    float a = 0, b = 0;
+    cudaCheck(cudaEventElapsedTime(&a, e[0], e[1]), "event");
+    cudaCheck(cudaEventElapsedTime(&b, e[1], e[2]), "event");
+    for (auto& x : e) cudaEventDestroy(x);
+    I.launches += I.launchesPerStep();
     I.ready = true;
-    std::vector<unsigned long long> h(6 * (size_t)I.grid);
-    cudaCheck(cudaStreamSynchronize(I.stream), "sync");
+    std::vector<unsigned long long> h(st.bytes / sizeof(unsigned long long));
     cudaCheck(cudaMemcpy(h.data(), st.p, st.bytes, cudaMemcpyDeviceToHost), "stamps");
-    unsigned long long t0 = ~0ull, aMin = ~0ull, aMax = 0, bMax = 0, eMax = 0;
-    long long nc = 0, nh = 0, most = 0, fewest = 1ll << 40;
+    unsigned long long t0 = ~0ull, f0 = ~0ull;
+    for (int g = 0; g < I.grid; g++) t0 = std::min(t0, h[4 * (size_t)g]);
+    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[4 * (size_t)I.grid + 2 * (size_t)g]);
+    std::vector<double> cvs, coord, end, fdur, fend;
     for (int g = 0; g < I.grid; g++) {
-        const unsigned long long* r = h.data() + 6 * (size_t)g;
-        t0 = std::min(t0, r[0]);
-        aMin = std::min(aMin, r[1]); aMax = std::max(aMax, r[1]);
-        bMax = std::max(bMax, r[2]); eMax = std::max(eMax, r[3]);
-        nc += (long long)r[4]; nh += (long long)r[5];
-        most = std::max(most, (long long)(r[4] + r[5]));
-        fewest = std::min(fewest, (long long)(r[4] + r[5]));
+        const unsigned long long* r = h.data() + 4 * (size_t)g;
+        cvs.push_back((r[1] - r[0]) * 1e-3);
+        coord.push_back((r[2] - t0) * 1e-3);
+        end.push_back((r[3] - t0) * 1e-3);
     }
-    out[0] = (aMin - t0) * 1e-3; out[1] = (aMax - t0) * 1e-3;
-    out[2] = (bMax - t0) * 1e-3; out[3] = (eMax - t0) * 1e-3;
-    out[4] = (double)nc; out[5] = (double)nh; out[6] = (double)most; out[7] = (double)fewest;
-    int s = status();
-    if (s) throw Error(GLUED_E_TIMEOUT, "batch: bounded wait gave up (status " + std::to_string(s) + ")");
+    for (int g = 0; g < fg; g++) {
+        const unsigned long long* r = h.data() + 4 * (size_t)I.grid + 2 * (size_t)g;
+        fdur.push_back((r[1] - r[0]) * 1e-3);
+        fend.push_back((r[1] - f0) * 1e-3);
+    }
+    out[0] = a * 1e3; out[1] = b * 1e3;
+    out[2] = pct(cvs, 50); out[3] = pct(cvs, 100);
+    out[4] = pct(coord, 0); out[5] = pct(coord, 50); out[6] = pct(coord, 100);
+    out[7] = pct(end, 50); out[8] = pct(end, 100);
+    out[9] = pct(fdur, 50); out[10] = pct(fdur, 100); out[11] = pct(fend, 100);
+    out[12] = (double)I.steps.size(); out[13] = (double)I.grid; out[14] = (double)I.parts; out[15] = (double)fg;
 }
 
 void Batch::updateState(int step) {
@@ -829,6 +831,9 @@ void Batch::updateState(int step) {
     k_batch_deposit<<<1, 256, 0, I.stream>>>(I.dev);
     cudaCheck(cudaGetLastError(), "deposit");
     I.launches++;
+    I.hillCountHost = std::min(I.hill.maxH, I.hillCountHost + I.W);
+    const int nItems = ((I.hillCountHost + I.hcHill() - 1) / I.hcHill()) * ((I.W + WBLK - 1) / WBLK);
+    if (nItems != I.balancedItems) I.balance();
 }
 
 void Batch::energies(double* out) {
@@ -867,6 +872,8 @@ void Batch::setHills(const double* centers, const double* heights, int n) {
         cudaCheck(cudaMemcpy(I.hill.mirror, m.data(), sizeof(float4) * n, cudaMemcpyHostToDevice), "hills");
     }
     cudaCheck(cudaMemcpy(I.hill.count, &n, sizeof(int), cudaMemcpyHostToDevice), "hills");
+    I.hillCountHost = n;
+    I.balance();
 }
 
 void Batch::getHills(double* centers, double* heights, int n) {

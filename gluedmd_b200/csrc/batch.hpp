@@ -1,5 +1,5 @@
 // Batched multi-walker evaluation: many walkers with the same CV / bias
-// structure evaluated by one cooperative persistent launch per step.
+// structure evaluated by one graph of two launches per step.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,10 +11,10 @@
 namespace glued {
 
 struct BatchTuning {
-    int ra = 8;        // A atoms per thread in the coordination tile (TA = 8 * ra)
-    int bSplit = 256;  // B atoms per coordination CTA item
-    int hillItems = 96;  // hill-table work items (each walks chunks hillItems apart)
-    int parts = 4;     // finalize items per walker
+    int ra = 8;               // A atoms per thread in the coordination tile (TA = 8 * ra)
+    int parts = 0;            // finalize CTAs per walker (0: the fewest that cover its rows)
+    int hillWeightPct = 150;  // cost of one hill item in the range balance, percent of a step
+    int hillChunk = 0;        // hills per hill item (multiple of 128, <= 1024; 0: 512)
 };
 
 class Batch {

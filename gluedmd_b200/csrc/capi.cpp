@@ -360,7 +360,7 @@ int glued_batch_set_tuning(glued_batch* b, const int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t;
-        t.ra = tune[0]; t.bSplit = tune[1]; t.hillItems = tune[2]; t.parts = tune[3];
+        t.ra = tune[0]; t.parts = tune[1]; t.hillWeightPct = tune[2]; t.hillChunk = tune[3];
         b->b->setTuning(t);
     });
 }
@@ -368,14 +368,14 @@ int glued_batch_get_tuning(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t = b->b->tuning();
-        tune[0] = t.ra; tune[1] = t.bSplit; tune[2] = t.hillItems; tune[3] = t.parts;
+        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.hillWeightPct; tune[3] = t.hillChunk;
     });
 }
 int glued_batch_autotune(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch");
         glued::BatchTuning t = b->b->autotune();
-        if (tune) { tune[0] = t.ra; tune[1] = t.bSplit; tune[2] = t.hillItems; tune[3] = t.parts; }
+        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.hillWeightPct; tune[3] = t.hillChunk; }
     });
 }
 int glued_batch_execute(glued_batch* b) {

@@ -366,11 +366,15 @@ void Context::buildPlan(const GluedForce& f) {
         cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
         coordGrid_ = sms * coordRunOccupancy(coordKind_, periodic_ ? 1 : 0, true);
         coordGrid_ = std::max(1, std::min(coordGrid_, (int)coordStepsH_.size()));
-        coordBegin_.upload(balanceRanges((int)coordStepsH_.size(), coordGrid_, {}));
+        std::vector<int> begin = balanceRanges((int)coordStepsH_.size(), coordGrid_, {});
+        std::vector<int> pieceStep, pieceBegin;
+        buildCoordPieces(coordStepsH_, begin, coordItemsN_, pieceStep, pieceBegin);
+        coordBegin_.upload(begin);
+        coordPieceStep_.upload(pieceStep);
+        coordPieceBegin_.upload(pieceBegin);
         coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
-        coordCnAcc_.alloc(sizeof(unsigned long long) * coordItemsN_);
+        coordCnPiece_.alloc(sizeof(double) * coordStepsH_.size());
         cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
-        cudaCheck(cudaMemset(coordCnAcc_.p, 0, coordCnAcc_.bytes), "coord acc");
         R_.items = coordItems_.as<CoordItem>();
         R_.steps = coordSteps_.as<CoordStep>();
         R_.begin = coordBegin_.as<int>();
@@ -378,7 +382,9 @@ void Context::buildPlan(const GluedForce& f) {
         R_.sysBox = box_.as<BoxDev>();
         R_.itemsPerSys = 1 << 30;
         R_.acc = coordAcc_.as<unsigned long long>();
-        R_.cnAcc = coordCnAcc_.as<unsigned long long>();
+        R_.cnPiece = coordCnPiece_.as<double>();
+        R_.pieceStep = coordPieceStep_.as<int>();
+        R_.pieceBegin = coordPieceBegin_.as<int>();
     }
 }
 
@@ -642,7 +648,6 @@ std::vector<double> Context::profilePhases(int reps) {
     // the pair-only repetitions left sums that no finalize cleared
     if (coordItemsN_ > 0) {
         cudaCheck(cudaMemsetAsync(coordAcc_.p, 0, coordAcc_.bytes, stream_), "coord acc");
-        cudaCheck(cudaMemsetAsync(coordCnAcc_.p, 0, coordCnAcc_.bytes, stream_), "coord acc");
     }
     return out;
 }

@@ -114,7 +114,8 @@ private:
     DBuf u2g_, box_, cvv_, dudcv_, energies_, testGrad_;
     DBuf jAtom_, jx_, jy_, jz_, jCv_;
     DBuf simple_, groupItems_, gAtoms_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
-    DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnAcc_;
+    DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnPiece_;
+    DBuf coordPieceStep_, coordPieceBegin_;
     DBuf biasDev_, mergeFlag_, uprobPartial_;
     JacDev J_{};
     int numSimple_ = 0;

@@ -36,8 +36,9 @@ __global__ void __launch_bounds__(256, 2) k_coord_run(CoordRunDev R) {
     if (s0 < s1) coordRun<RA, BOX, NH, HI>(R, s0, s1, sm, NoPieceHook());
 }
 
-// Fixed-point sums -> float Jacobian rows (one thread per row and component) and
-// CN values; every accumulator read is cleared.
+// Fixed-point sums -> float Jacobian rows (one thread per row and component),
+// every accumulator read is cleared; CN values = sums of the run pieces' partials
+// in step order.
 __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* __restrict__ cvv, int totalRows) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid < 3 * totalRows) {
@@ -56,10 +57,14 @@ __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* 
         out[it.jac0 + (row - base)] = (float)((double)v * crun::IFXD * coordAccScale(it));
     }
     if (blockIdx.x == 0) {
-        for (int i = threadIdx.x; i < numItems; i += blockDim.x) {
-            unsigned long long* c = R.cnAcc + i;
-            cvv[R.items[i].cv] = (double)(long long)*c * crun::IFXD;
-            *c = 0ull;
+        // one warp per item: lane l sums pieces l, l + 32, ... in step order, then
+        // a fixed xor tree
+        const int lane = threadIdx.x & 31;
+        for (int i = threadIdx.x >> 5; i < numItems; i += blockDim.x >> 5) {
+            double t = 0.0;
+            for (int k = R.pieceBegin[i] + lane; k < R.pieceBegin[i + 1]; k += 32) t += R.cnPiece[R.pieceStep[k]];
+            t = warpSum(t);
+            if (lane == 0) cvv[R.items[i].cv] = t;
         }
     }
 }
@@ -76,17 +81,34 @@ void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* s
     if (n > 0) k_compose_slots<<<(n + 255) / 256, 256, 0, s>>>(atoms, u2g, slots, n);
 }
 
-template <int RA, int BOX, int NH>
-static void launchRunH(cudaStream_t s, int grid, bool hi, const CoordRunDev& R) {
-    if (hi) k_coord_run<RA, BOX, NH, true><<<grid, 256, 0, s>>>(R);
-    else k_coord_run<RA, BOX, NH, false><<<grid, 256, 0, s>>>(R);
+// Two 33 KB CTAs per SM need the shared-memory carveout at its maximum; the
+// default split may leave room for one, which halves the resident grid.
+template <class K>
+static void maxSharedCarveout(K* fn) {
+    static bool done = false;
+    if (!done) {
+        cudaCheck(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared), "carveout");
+        done = true;
+    }
+}
+
+template <int RA, int BOX, int NH, bool HI>
+static void launchRun(cudaStream_t s, int grid, const CoordRunDev& R) {
+    maxSharedCarveout(k_coord_run<RA, BOX, NH, HI>);
+    k_coord_run<RA, BOX, NH, HI><<<grid, 256, 0, s>>>(R);
 }
 
 template <int BOX>
 static void launchRunB(cudaStream_t s, int grid, int kind, bool hi, const CoordRunDev& R) {
-    if (kind == 3) launchRunH<8, BOX, 3>(s, grid, hi, R);
-    else if (kind == -1) k_coord_run<8, BOX, -1, true><<<grid, 256, 0, s>>>(R);
-    else k_coord_run<8, BOX, 0, true><<<grid, 256, 0, s>>>(R);
+    if (kind == 3) {
+        if (hi) launchRun<8, BOX, 3, true>(s, grid, R);
+        else launchRun<8, BOX, 3, false>(s, grid, R);
+    } else if (kind == -1) {
+        launchRun<8, BOX, -1, true>(s, grid, R);
+    } else {
+        launchRun<8, BOX, 0, true>(s, grid, R);
+    }
 }
 
 void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, int totalRows, int boxKind, int kind,
@@ -116,6 +138,8 @@ int coordRunOccupancy(int kind, int boxKind, bool hi) {
         fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 0, true>
              : boxKind == 1 ? (const void*)k_coord_run<8, 1, 0, true> : (const void*)k_coord_run<8, 2, 0, true>;
     }
+    cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared), "carveout");
     int perSM = 0;
     cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 256, 0), "occupancy");
     return std::max(1, perSM);

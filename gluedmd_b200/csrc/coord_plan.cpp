@@ -64,6 +64,24 @@ std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>
     return begin;
 }
 
+void buildCoordPieces(const std::vector<CoordStep>& steps, const std::vector<int>& begin, int numItems,
+                      std::vector<int>& pieceStep, std::vector<int>& pieceBegin) {
+    std::vector<std::vector<int>> per(numItems);
+    for (size_t b = 0; b + 1 < begin.size(); b++)
+        for (int s = begin[b]; s < begin[b + 1]; s++) {
+            const int fl = steps[s].packed >> 16;
+            if (s == begin[b + 1] - 1 || (fl & COORD_F_LAST)) per[steps[s].item].push_back(s);
+        }
+    pieceStep.clear();
+    pieceBegin.assign(numItems + 1, 0);
+    for (int i = 0; i < numItems; i++) {
+        std::sort(per[i].begin(), per[i].end());
+        pieceBegin[i] = (int)pieceStep.size();
+        pieceStep.insert(pieceStep.end(), per[i].begin(), per[i].end());
+    }
+    pieceBegin[numItems] = (int)pieceStep.size();
+}
+
 bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic) {
     if (!periodic) return true;
     // longest minimum-image distance: half of |a| + |b| + |c| bounds it

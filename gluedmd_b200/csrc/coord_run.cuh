@@ -15,8 +15,8 @@
 // step s computes and the copies are issued after its barrier. Step descriptors
 // of a window of up to WIN steps sit in shared memory.
 //
-// Arithmetic. Coordinates are scaled by 1/r0 (A once per tile, B inside the
-// subtraction FMA), so the pair's squared distance is x^2 directly. For the
+// Arithmetic. Coordinates are scaled by 1/r0 (A once per tile, B once per step,
+// both rounded the same way), so the pair's squared distance is x^2 directly. For the
 // n = 6, m = 12 switch, f = 1/(1 + x^6) and the gradient factor h = x^4 f^2 need
 // one reciprocal and no square root. The reference's lower bound r^2 >= 1e-20
 // (CommonGluedKernels.cpp:983-987) is compared on every pair; the upper bound
@@ -26,11 +26,13 @@
 // Accumulation. Per-pair gradients h*d (scaled units) are summed in FP32 over a
 // step: per lane over its A atoms for B, per warp over lanes for A. Those step
 // sums are converted to 64-bit fixed point (value * 2^32) and added with integer
-// atomics into acc[row][3]; the CN partial of each run piece (FP64 block sum) is
-// added the same way into cnAcc[item]. Integer addition is exact and
-// order-independent, so results are bitwise reproducible run to run and do not
-// depend on the grid. The reader multiplies by the item's scale (-n/r0 for the
-// n = 6, m = 12 switch, 1/r0 otherwise), converts to FP64 and clears the slots.
+// atomics into acc[row][3] (integer addition is exact and order-independent, so
+// the sums are bitwise reproducible and do not depend on the grid); the reader
+// multiplies by the item's scale (-n/r0 for the n = 6, m = 12 switch, 1/r0
+// otherwise), converts to FP64 and clears the rows. The CN partial of each run
+// piece (a maximal sub-run of one tile on one CTA; FP64 block sum) goes to the
+// slot of the piece's last step, cnPiece[step]; the reader sums an item's pieces
+// in step order from a host-built table, so nothing needs clearing.
 #pragma once
 
 #include "devfn.cuh"
@@ -77,7 +79,6 @@ struct RunConst {
     float lo, hi;       // valid pairs: lo <= x^2 < hi
     float n, m;         // general exponents (kind 0)
     int ni, mi;         // integer exponents (kind -1)
-    float preRes, preDf, preSec;  // Taylor coefficients at x = 1 (kind 0)
     float ir0;
     BoxDev box;         // scaled: a, b, c divided by r0; inv multiplied by r0
 };
@@ -91,9 +92,6 @@ __device__ __forceinline__ RunConst runConst(const CoordItem& it, const BoxDev& 
     k.hi = it.rc2 > 0.0f ? fminf(it.rc2 * ir0sq, hiX) : hiX;
     k.n = it.n; k.m = it.m;
     k.ni = (int)it.n; k.mi = (int)it.m;
-    k.preRes = k.n / k.m;
-    k.preDf = 0.5f * k.n * (k.n - k.m) / k.m;
-    k.preSec = k.n * (k.m * k.m - 3.0f * k.m * (k.n - 1.0f) + k.n * (2.0f * k.n - 3.0f)) / (6.0f * k.m);
     k.box = b;
     for (int i = 0; i < 3; i++) {
         k.box.a[i] = b.a[i] * k.ir0; k.box.b[i] = b.b[i] * k.ir0; k.box.c[i] = b.c[i] * k.ir0;
@@ -141,22 +139,29 @@ __device__ __forceinline__ void switchX2(float x2, bool valid, const RunConst& k
         f = valid ? ff : 0.0f;
         h = valid ? dfdx / x : 0.0f;
     } else {
-        float x = sqrtf(x2);
-        float ff, dfdx;
-        float dx1 = x - 1.0f;
-        if (fabsf(dx1) < 1e-4f) {
-            ff = k.preRes + dx1 * (k.preDf + 0.5f * dx1 * k.preSec);
-            dfdx = k.preDf + dx1 * k.preSec;
-        } else if (x < 1e-10f) {
-            ff = 1.0f; dfdx = 0.0f;
+        // Non-integer exponents: the reference formula (Taylor branch within
+        // 1e-4 of x = 1, CommonGluedKernels.cpp:983-1003) evaluated in FP64; in
+        // FP32 the quotient (1 - x^n)/(1 - x^m) loses up to ~1e-2 relative force
+        // accuracy through cancellation just outside the Taylor window.
+        const double x = sqrt((double)x2);
+        const double n = k.n, m = k.m;
+        double ff, dfdx;
+        const double dx1 = x - 1.0;
+        if (fabs(dx1) < 1e-4) {
+            const double pre = n / m, df = 0.5 * n * (n - m) / m;
+            const double sec = n * (m * m - 3.0 * m * (n - 1.0) + n * (2.0 * n - 3.0)) / (6.0 * m);
+            ff = pre + dx1 * (df + 0.5 * dx1 * sec);
+            dfdx = df + dx1 * sec;
+        } else if (x < 1e-10) {
+            ff = 1.0; dfdx = 0.0;
         } else {
-            float xn = powf(x, k.n), xm = powf(x, k.m);
-            float den = 1.0f - xm;
-            ff = (1.0f - xn) / den;
-            dfdx = (k.m * (xm / x) - k.n * (xn / x) + (k.n - k.m) * (xn * xm / x)) / (den * den);
+            const double xn = pow(x, n), xm = pow(x, m);
+            const double den = 1.0 - xm;
+            ff = (1.0 - xn) / den;
+            dfdx = (m * (xm / x) - n * (xn / x) + (n - m) * (xn * xm / x)) / (den * den);
         }
-        f = valid ? ff : 0.0f;
-        h = valid ? dfdx / x : 0.0f;
+        f = valid ? (float)ff : 0.0f;
+        h = valid ? (float)(dfdx / x) : 0.0f;
     }
 }
 
@@ -237,12 +242,13 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                 pieceSteps = 0;
             }
             pieceSteps++;
-            const float nir0 = -K.ir0;
+            // B scaled exactly as A, so that an atom present in both groups gives
+            // a difference of exactly zero (excluded by the lower bound)
             float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
 #pragma unroll
             for (int j = 0; j < RB; j++) {
                 const float4 p = sm.pos[b][lane + 32 * j];
-                bx[j] = p.x; by[j] = p.y; bz[j] = p.z;
+                bx[j] = p.x * K.ir0; by[j] = p.y * K.ir0; bz[j] = p.z * K.ir0;
                 gbx[j] = gby[j] = gbz[j] = 0.0f;
             }
             float cnc = 0.0f;
@@ -252,8 +258,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                 for (int k = 0; k < RA; k++) {
 #pragma unroll
                     for (int j = 0; j < RB; j++) {
-                        float dx = fmaf(bx[j], nir0, ax[k]), dy = fmaf(by[j], nir0, ay[k]),
-                              dz = fmaf(bz[j], nir0, az[k]);
+                        float dx = ax[k] - bx[j], dy = ay[k] - by[j], dz = az[k] - bz[j];
                         imageS<BOX>(dx, dy, dz, K.box);
                         const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                         float f, h;
@@ -270,8 +275,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
 #pragma unroll
                     for (int j = 0; j < RB; j++) {
                         const bool bv = (lane + 32 * j) < nBv;
-                        float dx = fmaf(bx[j], nir0, ax[k]), dy = fmaf(by[j], nir0, ay[k]),
-                              dz = fmaf(bz[j], nir0, az[k]);
+                        float dx = ax[k] - bx[j], dy = ay[k] - by[j], dz = az[k] - bz[j];
                         imageS<BOX>(dx, dy, dz, K.box);
                         const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                         float f, h;
@@ -323,7 +327,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                     double t = 0.0;
 #pragma unroll
                     for (int y = 0; y < NW; y++) t += sm.red[b][y];
-                    redAddI64(R.cnAcc + d.item, __double2ll_rn(t * FXD));
+                    R.cnPiece[s] = t;
                 }
                 hook(d.item, pieceSteps);
             }

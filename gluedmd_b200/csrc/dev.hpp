@@ -117,7 +117,9 @@ struct CoordRunDev {
     const BoxDev* sysBox;      // box of system item / itemsPerSys
     int itemsPerSys;
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
-    unsigned long long* cnAcc; // [items] fixed-point CN
+    double* cnPiece;           // [steps]: CN partial of the piece ending at the step
+    const int* pieceStep;      // last steps of the pieces, grouped by item, step order
+    const int* pieceBegin;     // [items + 1] into pieceStep
 };
 
 // Bias records, evaluated in the reference's bias-type order.

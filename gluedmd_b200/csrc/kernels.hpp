@@ -30,6 +30,10 @@ int coordRunOccupancy(int kind, int boxKind, bool hi);
 int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<const float4*>& posqOfItem,
                     std::vector<CoordStep>& steps);
 std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost);
+// Last step of every run piece (maximal sub-run of one tile on one CTA), grouped
+// by item in step order: the slots of cnPiece the reader sums.
+void buildCoordPieces(const std::vector<CoordStep>& steps, const std::vector<int>& begin, int numItems,
+                      std::vector<int>& pieceStep, std::vector<int>& pieceBegin);
 bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic);
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies);

@@ -228,7 +228,8 @@ int glued_coordination_noalloc(void* stream, const void* posq, const int* group_
                                double* cn_out, float* grad_out);
 
 /* ----------------------------------------------------------------------- batch
- * Many walkers on one GPU evaluated by one cooperative persistent launch per step
+ * Many walkers on one GPU evaluated by one graph per step (a persistent
+ * kernel for the coordination pairs and the hill table, then a finalize kernel)
  * (no reference counterpart as a kernel: it replaces the reference's
  * one-Context-per-walker stepping, tests/test_multiwalker.py:156-158, and its
  * shared-bias pointer aliasing, CommonGluedKernels.cpp:5234-5262).
@@ -250,10 +251,13 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
                        glued_batch** out);
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
-/* Tiling of the persistent launch: tune[4] = {ra (4|8), b_split (multiple of
- * 128), hill_items, parts}. autotune times every candidate on the live walkers
- * (forces of the trial launches go to a scratch buffer), keeps the fastest and
- * returns it in tune (synchronizing).                                          */
+/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
+ * fewest that cover the walker's coordination rows), hill_weight_pct (cost the
+ * balance of the coordination ranges charges per hill item, percent of a step,
+ * 0..10000), hill_chunk (hills per hill item: 0 = 512, else a multiple of 128 up
+ * to 1024)}. autotune times every candidate on the live walkers (forces of the
+ * trial launches go to a scratch buffer), keeps the fastest and returns it in
+ * tune (synchronizing).                                                        */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);
@@ -271,14 +275,18 @@ int glued_batch_num_cvs(glued_batch* b, int* n);
 int glued_batch_num_hills(glued_batch* b, int* n);
 int glued_batch_set_hills(glued_batch* b, const double* centers, const double* heights, int n);
 int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int n);
-/* Status word of the bounded waits (0 = ok; bit 0 grid barrier, bit 1 bulk copy). */
+/* Status word of the step's device checks (0 = ok; no bounded wait remains in
+ * the current kernels, so it stays 0).                                         */
 int glued_batch_status(glued_batch* b, int* status);
 int glued_batch_launch_count(glued_batch* b, long long* count);
-/* Profiling: runs one regular step (forces are accumulated as by execute) with
- * per-CTA timestamps. out[8]: end of the work-item phase on the earliest and the
- * latest CTA, grid-barrier exit and kernel exit on the latest CTA (microseconds
- * after the earliest CTA started), coordination items, hill items, and the most
- * and fewest items one CTA processed. No reference counterpart.             */
+/* Profiling: runs one regular step (forces are accumulated as by execute), each
+ * launch bracketed by CUDA events and every CTA time-stamped. out[16], times in
+ * microseconds: {runs kernel, finalize kernel (events); hill-CV prologue of a
+ * runs CTA (median, max); end of a CTA's coordination steps after the first runs
+ * CTA started (min, median, max); end of a runs CTA incl. its hill items (median,
+ * max); finalize CTA duration (median, max); last finalize CTA end after the
+ * first one started; coordination steps, runs grid, finalize CTAs per walker,
+ * finalize grid}. No reference counterpart.                                   */
 int glued_batch_phase_times(glued_batch* b, double* out);
 
 #ifdef __cplusplus

@@ -83,7 +83,7 @@ def test_batch_repeatable_and_autotuned():
     for a, c in zip(f1, f2):
         assert np.array_equal(a, c)  # deterministic reductions: bitwise repeatable
     t = b.autotune()
-    assert t["ra"] in (4, 8) and t["b_split"] % 128 == 0
+    assert t["ra"] == 8 and t["parts"] >= 1
     for wk in walkers:
         wk.force.zero_()
     b.execute()

@@ -44,6 +44,29 @@ def test_random_systems_vs_fp64_oracle(seed, periodic):
     assert O.max_rel_force_err(res["forces"], ref["forces"]) < FORCE_TOL
 
 
+@pytest.mark.parametrize("nm", [(6, 12), (8, 14), (4.5, 9.5)])
+@pytest.mark.parametrize("periodic", [False, True])
+def test_coordination_overlapping_groups_multi_tile(nm, periodic):
+    """Groups sharing atoms (self pairs are excluded by the reference's r^2 >= 1e-20
+    bound), ragged sizes that leave partial A tiles and B chunks, and two
+    coordination CVs in one launch."""
+    rng = np.random.default_rng(21)
+    n, L = 1500, 2.5
+    pos = rng.uniform(0, L, (n, 3))
+    A = rng.choice(n, 203, replace=False)
+    B = np.concatenate([A[:50], rng.choice(n, 331, replace=False)])
+    A2 = rng.choice(n, 64, replace=False)
+    B2 = rng.choice(n, 128, replace=False)
+    cvs = [(O.CV_COORDINATION, [len(A)] + [int(x) for x in A] + [int(x) for x in B], [0.3, nm[0], nm[1]]),
+           (O.CV_COORDINATION, [len(A2)] + [int(x) for x in A2] + [int(x) for x in B2], [0.25, nm[0], nm[1]])]
+    g = [0.7, -1.3]
+    box = np.diag([L, L, L]).ravel()
+    ref = O.OracleSystem(cvs, periodic=periodic, mode="f64", test_bias_gradients=g, num_particles=n).execute(pos, box)
+    res = _gpu().run(pos, cvs, pbc=periodic, box=box.reshape(3, 3), grad=g)
+    np.testing.assert_allclose(res["cv_values"], ref["cv_values"], rtol=1e-5, atol=1e-5)
+    assert O.max_rel_force_err(res["forces"], ref["forces"]) < FORCE_TOL
+
+
 def test_atom_reorder_gives_identical_forces():
     """OpenMM's GPU-slot reordering must not change anything (fixed-point sums are
     order independent): forces bit-identical with and without a permutation."""
