@@ -206,68 +206,74 @@ __global__ void __launch_bounds__(256, 2) k_batch_runs(BatchDev B) {
 // CVs. Part 0 also computes those CVs and their Jacobians, sums the hill
 // partials in item order (fixed tree), evaluates the harmonic terms and the hill
 // bias, writes CVs and energies and scatters the distance/angle/dihedral rows.
+// Copies n bytes (multiple of 4) from global to shared memory, all threads.
+__device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
+    const int* s = static_cast<const int*>(src);
+    int* d = static_cast<int*>(dst);
+    for (int i = threadIdx.x; i < n / 4; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+constexpr int MAXCOORD = 8;   // coordination CVs per walker
+
 __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     __shared__ double sCV[MAXCV], sdU[MAXCV];
     __shared__ F3 sJac[MAXSIMPLE * 4];
     __shared__ double red[32 * 3];
+    // the walker's record: one round of independent loads
+    __shared__ BWalker sW;
+    __shared__ BSimple sSimple[MAXSIMPLE];
+    __shared__ BHarm sHarm[MAXHARM];
+    __shared__ CoordItem sItem[MAXCOORD];
     const int w = blockIdx.x / B.parts, part = blockIdx.x % B.parts;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long* st = B.fstamps ? B.fstamps + 2 * (size_t)blockIdx.x : nullptr;
     if (st && tid == 0) st[0] = globalTimer();
-    const BWalker& wk = B.walkers[w];
-    // First what does not depend on the runs kernel's results: the rows'
-    // accumulator slots and atoms, the distance/angle/dihedral values and
-    // Jacobians; then the fixed-point row sums (cleared as read), CN, hill partials.
+    copyWords(&sW, B.walkers + w, sizeof(BWalker));
+    copyWords(sSimple, B.simple + (size_t)w * B.nS, sizeof(BSimple) * B.nS);
+    copyWords(sHarm, B.harm + (size_t)w * B.nH, sizeof(BHarm) * B.nH);
+    copyWords(sItem, B.items + (size_t)w * B.nC, sizeof(CoordItem) * B.nC);
+    if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
+    __syncthreads();
+    // part 0: distance/angle/dihedral values and Jacobians (positions: one round)
+    if (part == 0 && tid < B.nS) {
+        F3 jac[4];
+        const float v = simpleCV(sSimple[tid].type, sSimple[tid].atoms, sW.posq, nullptr, sW.box, jac);
+        for (int k = 0; k < 4; k++) sJac[tid * 4 + k] = jac[k];
+        sCV[sSimple[tid].cv] = (double)v;
+    }
+    // the rows of this part: fixed-point sums (cleared as read) and their atoms
     const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
     const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
-    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD], rRow[ROWS_PER_THREAD];
+    long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
+    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD];
 #pragma unroll
     for (int q = 0; q < ROWS_PER_THREAD; q++) {
         const int r = r0 + tid + FT * q;
-        rItem[q] = -1; rAtom[q] = 0; rRow[q] = 0;
+        rItem[q] = -1; rAtom[q] = 0;
+        vx[q] = vy[q] = vz[q] = 0;
         if (r < r1) {
             // the walker's rows: item 0's A and B rows, then item 1's, ...
             int c = 0, base = 0;
-            while (c < B.nC - 1 && r >= base + B.items[w * B.nC + c].nA + B.items[w * B.nC + c].nB) {
-                base += B.items[w * B.nC + c].nA + B.items[w * B.nC + c].nB;
+            while (c < B.nC - 1 && r >= base + sItem[c].nA + sItem[c].nB) {
+                base += sItem[c].nA + sItem[c].nB;
                 c++;
             }
-            const CoordItem& it = B.items[w * B.nC + c];
+            const CoordItem& it = sItem[c];
             const int i = r - base;
+            unsigned long long* a = B.R.acc + 3 * (size_t)(it.row0 + i);
+            vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
+            a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
             rItem[q] = c;
-            rRow[q] = it.row0 + i;
             rAtom[q] = B.R.slots[i < it.nA ? it.a0 + i : it.b0 + (i - it.nA)];
         }
     }
-    if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
-    __syncthreads();
-    if (part == 0 && tid < B.nS) {
-        const BSimple& si = B.simple[w * B.nS + tid];
-        F3 jac[4];
-        const float v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, jac);
-        for (int k = 0; k < 4; k++) sJac[tid * 4 + k] = jac[k];
-        sCV[si.cv] = (double)v;
-    }
-    long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
-#pragma unroll
-    for (int q = 0; q < ROWS_PER_THREAD; q++) {
-        vx[q] = vy[q] = vz[q] = 0;
-        if (rItem[q] >= 0) {
-            unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
-            vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
-            a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
-        }
-    }
-    if (warp == 1) {
-        for (int c = 0; c < B.nC; c++) {
-            const int ii = w * B.nC + c;
-            double t = 0.0;
-            // pieces in step order: lane k takes pieces k, k + 32, ...; fixed tree
-            for (int k = B.R.pieceBegin[ii] + lane; k < B.R.pieceBegin[ii + 1]; k += 32)
-                t += __ldcg(B.R.cnPiece + B.R.pieceStep[k]);
-            t = warpSum(t);
-            if (lane == 0) sCV[B.items[ii].cv] = t;
-        }
+    // CN: warp c sums item c's piece partials (lane l: pieces l, l + 32, ..., step
+    // order), fixed xor tree
+    if (warp < B.nC) {
+        double t = 0.0;
+        for (int k = sItem[warp].pieceBegin + lane; k < sItem[warp].pieceEnd; k += 32) t += __ldcg(B.R.cnPiece + k);
+        t = warpSum(t);
+        if (lane == 0) sCV[sItem[warp].cv] = t;
     }
     double hv[3] = {0.0, 0.0, 0.0};
     if (part == 0 && B.hill.present) {
@@ -283,9 +289,9 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     if (tid == 0) {
         double E = 0.0;
         for (int k = 0; k < B.nH; k++) {
-            const BHarm& hm = B.harm[w * B.nH + k];
+            const BHarm& hm = sHarm[k];
             bool coordCv = false;
-            for (int c = 0; c < B.nC; c++) coordCv = coordCv || B.items[w * B.nC + c].cv == hm.cv;
+            for (int c = 0; c < B.nC; c++) coordCv = coordCv || sItem[c].cv == hm.cv;
             if (part == 0 || coordCv) sdU[hm.cv] += harmonicDU(hm, sCV[hm.cv], E);
         }
         if (part == 0) {
@@ -300,12 +306,12 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
         }
     }
     __syncthreads();
-    unsigned long long* F = wk.force;
-    const int P = wk.padded;
+    unsigned long long* F = sW.force;
+    const int P = sW.padded;
 #pragma unroll
     for (int q = 0; q < ROWS_PER_THREAD; q++) {
         if (rItem[q] < 0) continue;
-        const CoordItem& it = B.items[w * B.nC + rItem[q]];
+        const CoordItem& it = sItem[rItem[q]];
         const double g = sdU[it.cv];
         if (g == 0.0) continue;
         const double sc = coordAccScale(it) * crun::IFXD;
@@ -313,7 +319,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
                    (float)((double)vz[q] * sc));
     }
     if (part == 0 && tid < B.nS * 4) {
-        const BSimple& si = B.simple[w * B.nS + tid / 4];
+        const BSimple& si = sSimple[tid / 4];
         const int k = tid % 4;
         const int na = si.type == 1 ? 2 : si.type == 2 ? 3 : 4;
         const double g = sdU[si.cv];
@@ -366,7 +372,7 @@ struct Batch::Impl {
     std::vector<CoordItem> items;
     std::vector<int> coordAtoms;
     std::vector<CoordStep> steps;
-    DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, acc, cnPiece, pieceStepD, pieceBeginD;
+    DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, sysPosqD, acc, cnPiece;
     DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
     DBuf hMirror, hCenters, hHeights, hCount;
     BHill hill{};
@@ -395,47 +401,49 @@ struct Batch::Impl {
     int hcHill() const { return tune.hillChunk > 0 ? tune.hillChunk : 512; }
 
     // Per-CTA step ranges: CTA b also evaluates hill items b, b + grid, ...,
-    // charged hillWeightPct percent of a step each; piece table to match.
+    // charged hillWeightPct percent of a step each; run pieces to match. The
+    // device copies are rewritten in place (a captured graph keeps their
+    // addresses) unless they must grow.
     void balance() {
         const int nItems = hill.present ? ((hillCountHost + hcHill() - 1) / hcHill()) * ((W + WBLK - 1) / WBLK) : 0;
         std::vector<double> pre(grid, 0.0);
         for (int h = 0; h < nItems; h++) pre[h % grid] += tune.hillWeightPct / 100.0;
         std::vector<int> begin = balanceRanges((int)steps.size(), grid, pre);
-        std::vector<int> pieceStep, pieceBegin;
-        buildCoordPieces(steps, begin, (int)items.size(), pieceStep, pieceBegin);
-        if (pieceStep.empty()) pieceStep.push_back(0);
-        // same buffers across rebalances: a captured graph keeps their addresses
-        auto put = [&](DBuf& d, const std::vector<int>& v) {
-            if (d.bytes < sizeof(int) * v.size()) {
-                d.alloc(sizeof(int) * std::max(v.size(), (size_t)grid + 1 + pieceStep.size()));
-                destroyGraph();
-            }
-            cudaCheck(cudaMemcpy(d.p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice), "ranges");
+        const int pieces = buildCoordPieces(steps, begin, items);
+        auto put = [&](DBuf& d, const void* src, size_t bytes) {
+            if (d.bytes < bytes) { d.alloc(bytes); destroyGraph(); }
+            if (bytes) cudaCheck(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice), "ranges");
         };
-        put(beginD, begin);
-        put(pieceStepD, pieceStep);
-        put(pieceBeginD, pieceBegin);
+        put(beginD, begin.data(), sizeof(int) * begin.size());
+        put(stepsD, steps.data(), sizeof(CoordStep) * steps.size());
+        put(itemsD, items.data(), sizeof(CoordItem) * items.size());
+        if (cnPiece.bytes < sizeof(double) * std::max(1, pieces)) {
+            cnPiece.alloc(sizeof(double) * std::max(1, pieces));
+            destroyGraph();
+        }
         balancedItems = nItems;
         dev.R.begin = beginD.as<int>();
-        dev.R.pieceStep = pieceStepD.as<int>();
-        dev.R.pieceBegin = pieceBeginD.as<int>();
+        dev.R.steps = stepsD.as<CoordStep>();
+        dev.R.items = itemsD.as<CoordItem>();
+        dev.items = itemsD.as<CoordItem>();
+        dev.R.cnPiece = cnPiece.as<double>();
     }
 
     int minParts() const { return std::max(1, (rows + FT * ROWS_PER_THREAD - 1) / (FT * ROWS_PER_THREAD)); }
 
     void plan() {
         // coordination steps over all walkers' items (walker-major)
-        std::vector<const float4*> posqOf(items.size());
-        for (size_t i = 0; i < items.size(); i++) posqOf[i] = walkersH[i / std::max(nC, 1)].posq;
-        buildCoordSteps(items, 8, posqOf, steps);
+        buildCoordSteps(items, 8, steps);
         rows = 0;
         for (int c = 0; c < nC; c++) rows += items[c].nA + items[c].nB;
-        itemsD.upload(items);
-        stepsD.upload(steps);
+        std::vector<const float4*> posqOf(W);
+        for (int w = 0; w < W; w++) posqOf[w] = walkersH[w].posq;
+        sysPosqD.upload(posqOf);
+        itemsD.alloc(sizeof(CoordItem) * std::max((size_t)1, items.size()));
+        stepsD.alloc(sizeof(CoordStep) * std::max((size_t)1, steps.size()));
         const size_t accRows = (size_t)std::max(1, rows) * W;
         if (acc.bytes < sizeof(unsigned long long) * 3 * accRows) acc.alloc(sizeof(unsigned long long) * 3 * accRows);
         cudaCheck(cudaMemset(acc.p, 0, acc.bytes), "reset");
-        cnPiece.alloc(sizeof(double) * std::max((size_t)1, steps.size()));
         std::vector<BoxDev> boxes(W);
         for (int w = 0; w < W; w++) boxes[w] = walkersH[w].box;
         boxesD.upload(boxes);
@@ -467,6 +475,7 @@ struct Batch::Impl {
         dev.R.items = itemsD.as<CoordItem>();
         dev.R.steps = stepsD.as<CoordStep>();
         dev.R.slots = atomsD.as<int>();
+        dev.R.sysPosq = sysPosqD.as<const float4*>();
         dev.R.sysBox = boxesD.as<BoxDev>();
         dev.R.itemsPerSys = std::max(nC, 1);
         dev.R.acc = acc.as<unsigned long long>();
@@ -517,6 +526,7 @@ Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_de
         else I.nC++;
     }
     if (I.nS > MAXSIMPLE) throw Error(GLUED_E_INVALID, "batch: at most 16 distance/angle/dihedral CVs per walker");
+    if (I.nC > MAXCOORD) throw Error(GLUED_E_INVALID, "batch: at most 8 coordination CVs per walker");
     int hillBias = -1;
     for (int b = 0; b < f0.numBiases(); b++) {
         const BiasSpec& bs = f0.bias(b);

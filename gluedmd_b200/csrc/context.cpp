@@ -353,38 +353,35 @@ void Context::buildPlan(const GluedForce& f) {
             if (it.kind != coordKind_) coordKind_ = (coordKind_ == 0 || it.kind == 0) ? 0 : -1;
         if (coordKind_ != 3)
             for (auto& it : coord) it.kind = coordKind_;
-        coordRows_ = buildCoordSteps(coord, 8, {}, coordStepsH_);
-        coordItemsH_ = coord;
+        coordRows_ = buildCoordSteps(coord, 8, coordStepsH_);
         coordItemsN_ = (int)coord.size();
         coordAtomsN_ = (int)coordAtoms.size();
-        coordItems_.upload(coord);
-        coordAtoms_.upload(coordAtoms);
-        coordSlots_.alloc(sizeof(int) * std::max(1, coordAtomsN_));
-        coordSteps_.alloc(sizeof(CoordStep) * coordStepsH_.size());
         int dev = 0, sms = 0;
         cudaCheck(cudaGetDevice(&dev), "device");
         cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
         coordGrid_ = sms * coordRunOccupancy(coordKind_, periodic_ ? 1 : 0, true);
         coordGrid_ = std::max(1, std::min(coordGrid_, (int)coordStepsH_.size()));
         std::vector<int> begin = balanceRanges((int)coordStepsH_.size(), coordGrid_, {});
-        std::vector<int> pieceStep, pieceBegin;
-        buildCoordPieces(coordStepsH_, begin, coordItemsN_, pieceStep, pieceBegin);
+        const int pieces = buildCoordPieces(coordStepsH_, begin, coord);
+        coordItemsH_ = coord;
+        coordItems_.upload(coord);
+        coordAtoms_.upload(coordAtoms);
+        coordSlots_.alloc(sizeof(int) * std::max(1, coordAtomsN_));
+        coordSteps_.upload(coordStepsH_);
         coordBegin_.upload(begin);
-        coordPieceStep_.upload(pieceStep);
-        coordPieceBegin_.upload(pieceBegin);
+        coordSysPosq_.alloc(sizeof(const float4*));
         coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
-        coordCnPiece_.alloc(sizeof(double) * coordStepsH_.size());
+        coordCnPiece_.alloc(sizeof(double) * std::max(1, pieces));
         cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
         R_.items = coordItems_.as<CoordItem>();
         R_.steps = coordSteps_.as<CoordStep>();
         R_.begin = coordBegin_.as<int>();
         R_.slots = coordSlots_.as<int>();
+        R_.sysPosq = coordSysPosq_.as<const float4*>();
         R_.sysBox = box_.as<BoxDev>();
         R_.itemsPerSys = 1 << 30;
         R_.acc = coordAcc_.as<unsigned long long>();
         R_.cnPiece = coordCnPiece_.as<double>();
-        R_.pieceStep = coordPieceStep_.as<int>();
-        R_.pieceBegin = coordPieceBegin_.as<int>();
     }
 }
 
@@ -550,11 +547,8 @@ void Context::bind(cudaStream_t s, const void* posq, const int* atomIndex, long 
     padded_ = padded;
     bound_ = true;
     invalidateGraphs();
-    if (!coordStepsH_.empty()) {
-        for (auto& st : coordStepsH_) st.posq = posq_;
-        cudaCheck(cudaMemcpy(coordSteps_.p, coordStepsH_.data(), sizeof(CoordStep) * coordStepsH_.size(),
-                             cudaMemcpyHostToDevice), "coordination steps");
-    }
+    if (coordItemsN_ > 0)
+        cudaCheck(cudaMemcpy(coordSysPosq_.p, &posq_, sizeof(posq_), cudaMemcpyHostToDevice), "coordination posq");
     atomsReordered();
 }
 

@@ -115,7 +115,7 @@ private:
     DBuf jAtom_, jx_, jy_, jz_, jCv_;
     DBuf simple_, groupItems_, gAtoms_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
     DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnPiece_;
-    DBuf coordPieceStep_, coordPieceBegin_;
+    DBuf coordSysPosq_;
     DBuf biasDev_, mergeFlag_, uprobPartial_;
     JacDev J_{};
     int numSimple_ = 0;

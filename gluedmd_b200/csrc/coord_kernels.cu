@@ -57,12 +57,12 @@ __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* 
         out[it.jac0 + (row - base)] = (float)((double)v * crun::IFXD * coordAccScale(it));
     }
     if (blockIdx.x == 0) {
-        // one warp per item: lane l sums pieces l, l + 32, ... in step order, then
-        // a fixed xor tree
+        // one warp per item: lane l sums the item's pieces l, l + 32, ... (step
+        // order), then a fixed xor tree
         const int lane = threadIdx.x & 31;
         for (int i = threadIdx.x >> 5; i < numItems; i += blockDim.x >> 5) {
             double t = 0.0;
-            for (int k = R.pieceBegin[i] + lane; k < R.pieceBegin[i + 1]; k += 32) t += R.cnPiece[R.pieceStep[k]];
+            for (int k = R.items[i].pieceBegin + lane; k < R.items[i].pieceEnd; k += 32) t += R.cnPiece[k];
             t = warpSum(t);
             if (lane == 0) cvv[R.items[i].cv] = t;
         }

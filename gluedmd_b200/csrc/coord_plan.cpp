@@ -8,8 +8,7 @@
 
 namespace glued {
 
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<const float4*>& posqOfItem,
-                    std::vector<CoordStep>& steps) {
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps) {
     const int TA = COORD_NW * ra;
     steps.clear();
     int rows = 0;
@@ -22,7 +21,6 @@ int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<con
             const int nAv = std::min(TA, it.nA - ta * TA);
             for (int c = 0; c < nCh; c++) {
                 CoordStep s{};
-                s.posq = posqOfItem.empty() ? nullptr : posqOfItem[i];
                 s.item = (int)i;
                 s.aStart = it.a0 + ta * TA;
                 s.bStart = it.b0 + c * COORD_CH;
@@ -31,6 +29,7 @@ int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<con
                 const int nBv = std::min(COORD_CH, it.nB - c * COORD_CH);
                 int fl = (c == 0 ? COORD_F_FIRST : 0) | (c == nCh - 1 ? COORD_F_LAST : 0);
                 s.packed = nAv | (nBv << 8) | (fl << 16);
+                s.pieceSlot = -1;
                 steps.push_back(s);
             }
         }
@@ -64,22 +63,22 @@ std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>
     return begin;
 }
 
-void buildCoordPieces(const std::vector<CoordStep>& steps, const std::vector<int>& begin, int numItems,
-                      std::vector<int>& pieceStep, std::vector<int>& pieceBegin) {
-    std::vector<std::vector<int>> per(numItems);
+int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begin, std::vector<CoordItem>& items) {
+    std::vector<std::vector<int>> per(items.size());
     for (size_t b = 0; b + 1 < begin.size(); b++)
         for (int s = begin[b]; s < begin[b + 1]; s++) {
             const int fl = steps[s].packed >> 16;
+            steps[s].pieceSlot = -1;
             if (s == begin[b + 1] - 1 || (fl & COORD_F_LAST)) per[steps[s].item].push_back(s);
         }
-    pieceStep.clear();
-    pieceBegin.assign(numItems + 1, 0);
-    for (int i = 0; i < numItems; i++) {
+    int slot = 0;
+    for (size_t i = 0; i < items.size(); i++) {
         std::sort(per[i].begin(), per[i].end());
-        pieceBegin[i] = (int)pieceStep.size();
-        pieceStep.insert(pieceStep.end(), per[i].begin(), per[i].end());
+        items[i].pieceBegin = slot;
+        for (int s : per[i]) steps[s].pieceSlot = slot++;
+        items[i].pieceEnd = slot;
     }
-    pieceBegin[numItems] = (int)pieceStep.size();
+    return slot;
 }
 
 bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic) {

@@ -31,8 +31,9 @@
 // multiplies by the item's scale (-n/r0 for the n = 6, m = 12 switch, 1/r0
 // otherwise), converts to FP64 and clears the rows. The CN partial of each run
 // piece (a maximal sub-run of one tile on one CTA; FP64 block sum) goes to the
-// slot of the piece's last step, cnPiece[step]; the reader sums an item's pieces
-// in step order from a host-built table, so nothing needs clearing.
+// slot the host assigned to the piece (CoordStep::pieceSlot of its last step);
+// an item's slots are contiguous and in step order, the reader sums them in that
+// order, and nothing needs clearing.
 #pragma once
 
 #include "devfn.cuh"
@@ -197,27 +198,29 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
         }
         __syncthreads();
         // gather indices of a step: B (threads < CH) and A (threads < TA, first steps only)
-        auto loadIdx = [&](int ls, int& ib, int& ia) {
+        auto loadIdx = [&](int ls, int& ib, int& ia, const float4*& pq) {
             const CoordStep& d = sm.st[ls];
             const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
             const bool first = (w0 + ls == s0) || (fl & F_FIRST);
             ib = (tid < CH && tid < nBv) ? __ldg(R.slots + d.bStart + tid) : -1;
             ia = (first && tid < TA && tid < nAv) ? __ldg(R.slots + d.aStart + tid) : -1;
+            pq = R.sysPosq[d.item / R.itemsPerSys];
         };
-        auto issue = [&](int ls, int ib, int ia) {
+        auto issue = [&](int ls, int ib, int ia, const float4* pq) {
             const CoordStep& d = sm.st[ls];
             const int b = (w0 + ls - s0) & 1;
             const int fl = d.packed >> 16;
             const bool first = (w0 + ls == s0) || (fl & F_FIRST);
-            if (tid < CH) cpAsync16(&sm.pos[b][tid], d.posq + (ib >= 0 ? ib : 0), ib >= 0);
-            if (first && tid < TA) cpAsync16(&sm.apos[b][tid], d.posq + (ia >= 0 ? ia : 0), ia >= 0);
+            if (tid < CH) cpAsync16(&sm.pos[b][tid], pq + (ib >= 0 ? ib : 0), ib >= 0);
+            if (first && tid < TA) cpAsync16(&sm.apos[b][tid], pq + (ia >= 0 ? ia : 0), ia >= 0);
             cpAsyncCommit();
         };
         int ib0, ia0, ib1 = -1, ia1 = -1;
-        loadIdx(0, ib0, ia0);
-        if (nw > 1) loadIdx(1, ib1, ia1);
-        issue(0, ib0, ia0);
-        if (nw > 1) issue(1, ib1, ia1);
+        const float4 *pq0, *pq1 = nullptr;
+        loadIdx(0, ib0, ia0, pq0);
+        if (nw > 1) loadIdx(1, ib1, ia1, pq1);
+        issue(0, ib0, ia0, pq0);
+        if (nw > 1) issue(1, ib1, ia1, pq1);
         cpAsyncWaitAll();
         __syncthreads();
         for (int ls = 0; ls < nw; ls++) {
@@ -228,7 +231,8 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             const bool first = (s == s0) || (fl & F_FIRST);
             const bool last = (s == s1 - 1) || (fl & F_LAST);
             int ib2 = -1, ia2 = -1;
-            if (ls + 2 < nw) loadIdx(ls + 2, ib2, ia2);
+            const float4* pq2 = nullptr;
+            if (ls + 2 < nw) loadIdx(ls + 2, ib2, ia2, pq2);
             if (first) {
                 const CoordItem it = R.items[d.item];
                 K = runConst(it, R.sysBox[d.item / R.itemsPerSys]);
@@ -312,7 +316,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             }
             cpAsyncWaitAll();
             __syncthreads();
-            if (ls + 2 < nw) issue(ls + 2, ib2, ia2);
+            if (ls + 2 < nw) issue(ls + 2, ib2, ia2, pq2);
             // B sums over warps in fixed order
             for (int v = tid; v < CH * 3; v += blockDim.x) {
                 if (v / 3 < nBv) {
@@ -327,7 +331,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                     double t = 0.0;
 #pragma unroll
                     for (int y = 0; y < NW; y++) t += sm.red[b][y];
-                    R.cnPiece[s] = t;
+                    R.cnPiece[d.pieceSlot] = t;
                 }
                 hook(d.item, pieceSteps);
             }

@@ -80,6 +80,7 @@ struct CoordItem {
     int partB;      // offset of B partials: [tilesA][nB]
     int cn0;        // offset of this item's per-CTA CN partials
     int row0;       // first fixed-point accumulator row (A rows, then B rows)
+    int pieceBegin, pieceEnd;   // this item's run-piece CN partials in cnPiece
 };
 
 struct CoordDev {
@@ -100,13 +101,14 @@ constexpr int COORD_F_FIRST = 1, COORD_F_LAST = 2;
 
 // One (tile, chunk) step. 32 bytes.
 struct __align__(16) CoordStep {
-    const float4* posq;  // positions of the item's system (slot order)
     int item;
     int aStart;          // index into slots of the tile's first A atom
     int bStart;          // index into slots of the chunk's first B atom
     int rowA;            // acc row of the tile's first A atom
     int rowB;            // acc row of the chunk's first B atom
     int packed;          // nAv | nBv << 8 | flags << 16 (COORD_F_*)
+    int pieceSlot;       // cnPiece slot of the run piece this step ends (static ranges), else -1
+    int pad;
 };
 
 struct CoordRunDev {
@@ -114,12 +116,11 @@ struct CoordRunDev {
     const CoordStep* steps;
     const int* begin;          // [grid + 1]: CTA b runs steps [begin[b], begin[b+1])
     const int* slots;          // per coordination atom: its row in posq
+    const float4* const* sysPosq;  // positions of system item / itemsPerSys
     const BoxDev* sysBox;      // box of system item / itemsPerSys
     int itemsPerSys;
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
-    double* cnPiece;           // [steps]: CN partial of the piece ending at the step
-    const int* pieceStep;      // last steps of the pieces, grouped by item, step order
-    const int* pieceBegin;     // [items + 1] into pieceStep
+    double* cnPiece;           // CN partial of every run piece, item-contiguous (CoordItem::pieceBegin/End)
 };
 
 // Bias records, evaluated in the reference's bias-type order.

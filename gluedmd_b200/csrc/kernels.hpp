@@ -27,13 +27,12 @@ int coordRunOccupancy(int kind, int boxKind, bool hi);
 // Host planning: steps tile-major (fills row0 / tilesA of the items, returns the
 // accumulator row count); per-CTA ranges of numSteps over grid CTAs with preCost[b]
 // steps' worth of other work on CTA b; whether the upper pair bound can bind.
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, const std::vector<const float4*>& posqOfItem,
-                    std::vector<CoordStep>& steps);
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps);
 std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost);
-// Last step of every run piece (maximal sub-run of one tile on one CTA), grouped
-// by item in step order: the slots of cnPiece the reader sums.
-void buildCoordPieces(const std::vector<CoordStep>& steps, const std::vector<int>& begin, int numItems,
-                      std::vector<int>& pieceStep, std::vector<int>& pieceBegin);
+// Run pieces of the static ranges (maximal sub-runs of one tile on one CTA): the
+// piece slots of their last steps, item-contiguous in step order, and every
+// item's slot range. Returns the number of pieces.
+int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begin, std::vector<CoordItem>& items);
 bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic);
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies);
