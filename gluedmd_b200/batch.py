@@ -146,12 +146,12 @@ class Batch:
     def phase_times(self):
         """One step with each launch bracketed by CUDA events and every CTA
         time-stamped (microseconds); see glued_batch_phase_times."""
-        out = (c_double * 16)()
+        out = (c_double * 21)()
         call("glued_batch_phase_times", self._h, out)
         keys = ["runs_us", "finalize_us", "hill_cvs_med_us", "hill_cvs_max_us", "coord_end_min_us",
                 "coord_end_med_us", "coord_end_max_us", "runs_end_med_us", "runs_end_max_us",
                 "fin_cta_med_us", "fin_cta_max_us", "fin_end_max_us", "coord_steps", "grid", "parts",
-                "finalize_grid"]
+                "finalize_grid", "fin_record_us", "fin_rows_cn_us", "fin_hills_us", "fin_du_us", "fin_scatter_us"]
         return dict(zip(keys, out[:]))
 
     @property

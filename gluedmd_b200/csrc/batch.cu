@@ -79,7 +79,7 @@ struct BatchDev {
     double* energy;         // [W]
     double* hillEnergy;     // [W]
     unsigned long long* stamps;   // profiling (nullptr = off): runs kernel [grid][4]
-    unsigned long long* fstamps;  // profiling (nullptr = off): finalize kernel [W * parts][2]
+    unsigned long long* fstamps;  // profiling (nullptr = off): finalize kernel [W * parts][6]
 };
 
 __device__ __forceinline__ unsigned long long globalTimer() {
@@ -99,9 +99,9 @@ __device__ __forceinline__ double harmonicDU(const BHarm& hm, double v, double& 
 __device__ __forceinline__ void scatterRow(unsigned long long* F, int P, int atom, double g, float gx, float gy,
                                            float gz) {
     const double S = 4294967296.0;
-    atomicAdd(F + atom, (unsigned long long)(long long)(-(g * (double)gx) * S));
-    atomicAdd(F + atom + P, (unsigned long long)(long long)(-(g * (double)gy) * S));
-    atomicAdd(F + atom + 2 * P, (unsigned long long)(long long)(-(g * (double)gz) * S));
+    redAddGlobal(F + atom, (unsigned long long)(long long)(-(g * (double)gx) * S));
+    redAddGlobal(F + atom + P, (unsigned long long)(long long)(-(g * (double)gy) * S));
+    redAddGlobal(F + atom + 2 * P, (unsigned long long)(long long)(-(g * (double)gz) * S));
 }
 
 // ------------------------------------------------------------- hill items
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     __shared__ CoordItem sItem[MAXCOORD];
     const int w = blockIdx.x / B.parts, part = blockIdx.x % B.parts;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned long long* st = B.fstamps ? B.fstamps + 2 * (size_t)blockIdx.x : nullptr;
+    unsigned long long* st = B.fstamps ? B.fstamps + 6 * (size_t)blockIdx.x : nullptr;
     if (st && tid == 0) st[0] = globalTimer();
     copyWords(&sW, B.walkers + w, sizeof(BWalker));
     copyWords(sSimple, B.simple + (size_t)w * B.nS, sizeof(BSimple) * B.nS);
@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     copyWords(sItem, B.items + (size_t)w * B.nC, sizeof(CoordItem) * B.nC);
     if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
     __syncthreads();
+    if (st && tid == 0) st[1] = globalTimer();
     // part 0: distance/angle/dihedral values and Jacobians (positions: one round)
     if (part == 0 && tid < B.nS) {
         F3 jac[4];
@@ -244,12 +245,14 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     // the rows of this part: fixed-point sums (cleared as read) and their atoms
     const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
     const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
+    // (all loads first, so that they are in flight together; the rows are
+    // cleared at the end of the kernel)
     long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
-    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD];
+    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD], rRow[ROWS_PER_THREAD];
 #pragma unroll
     for (int q = 0; q < ROWS_PER_THREAD; q++) {
         const int r = r0 + tid + FT * q;
-        rItem[q] = -1; rAtom[q] = 0;
+        rItem[q] = -1; rAtom[q] = 0; rRow[q] = 0;
         vx[q] = vy[q] = vz[q] = 0;
         if (r < r1) {
             // the walker's rows: item 0's A and B rows, then item 1's, ...
@@ -260,11 +263,11 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
             }
             const CoordItem& it = sItem[c];
             const int i = r - base;
-            unsigned long long* a = B.R.acc + 3 * (size_t)(it.row0 + i);
+            rRow[q] = it.row0 + i;
+            const unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
             vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
-            a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
             rItem[q] = c;
-            rAtom[q] = B.R.slots[i < it.nA ? it.a0 + i : it.b0 + (i - it.nA)];
+            rAtom[q] = __ldg(B.R.slots + (i < it.nA ? it.a0 + i : it.b0 + (i - it.nA)));
         }
     }
     // CN: warp c sums item c's piece partials (lane l: pieces l, l + 32, ..., step
@@ -275,6 +278,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
         t = warpSum(t);
         if (lane == 0) sCV[sItem[warp].cv] = t;
     }
+    if (st) { __syncthreads(); if (tid == 0) st[2] = globalTimer(); }
     double hv[3] = {0.0, 0.0, 0.0};
     if (part == 0 && B.hill.present) {
         const int items = (*B.hill.count + B.hc - 1) / B.hc;
@@ -285,6 +289,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     }
     if (part == 0) blockSum<3>(hv, red);   // part-uniform: every thread of part 0 takes part
     else __syncthreads();
+    if (st && tid == 0) st[3] = globalTimer();
     // dU/dCV: part 0 everything, the other parts the coordination CVs only
     if (tid == 0) {
         double E = 0.0;
@@ -306,6 +311,7 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
         }
     }
     __syncthreads();
+    if (st && tid == 0) st[4] = globalTimer();
     unsigned long long* F = sW.force;
     const int P = sW.padded;
 #pragma unroll
@@ -328,7 +334,14 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
             scatterRow(F, P, si.atoms[k], g, j.x, j.y, j.z);
         }
     }
-    if (st) { __syncthreads(); if (tid == 0) st[1] = globalTimer(); }
+    // clear the rows for the next step's runs
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        if (rItem[q] < 0) continue;
+        unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
+        a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
+    }
+    if (st) { __syncthreads(); if (tid == 0) st[5] = globalTimer(); }
 }
 
 typedef void (*RunsFn)(BatchDev);
@@ -787,7 +800,7 @@ void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
     const int fg = I.W * I.parts;
     DBuf st;
-    st.alloc(sizeof(unsigned long long) * (4 * (size_t)I.grid + 2 * (size_t)fg));
+    st.alloc(sizeof(unsigned long long) * (4 * (size_t)I.grid + 6 * (size_t)fg));
     cudaCheck(cudaMemsetAsync(st.p, 0, st.bytes, I.stream), "stamps");
     I.dev.stamps = st.as<unsigned long long>();
     I.dev.fstamps = st.as<unsigned long long>() + 4 * (size_t)I.grid;
@@ -811,8 +824,8 @@ void Batch::phaseTimes(double* out) {
     cudaCheck(cudaMemcpy(h.data(), st.p, st.bytes, cudaMemcpyDeviceToHost), "stamps");
     unsigned long long t0 = ~0ull, f0 = ~0ull;
     for (int g = 0; g < I.grid; g++) t0 = std::min(t0, h[4 * (size_t)g]);
-    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[4 * (size_t)I.grid + 2 * (size_t)g]);
-    std::vector<double> cvs, coord, end, fdur, fend;
+    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[4 * (size_t)I.grid + 6 * (size_t)g]);
+    std::vector<double> cvs, coord, end, fdur, fend, fph[5];
     for (int g = 0; g < I.grid; g++) {
         const unsigned long long* r = h.data() + 4 * (size_t)g;
         cvs.push_back((r[1] - r[0]) * 1e-3);
@@ -820,15 +833,17 @@ void Batch::phaseTimes(double* out) {
         end.push_back((r[3] - t0) * 1e-3);
     }
     for (int g = 0; g < fg; g++) {
-        const unsigned long long* r = h.data() + 4 * (size_t)I.grid + 2 * (size_t)g;
-        fdur.push_back((r[1] - r[0]) * 1e-3);
-        fend.push_back((r[1] - f0) * 1e-3);
+        const unsigned long long* r = h.data() + 4 * (size_t)I.grid + 6 * (size_t)g;
+        fdur.push_back((r[5] - r[0]) * 1e-3);
+        fend.push_back((r[5] - f0) * 1e-3);
+        for (int k = 0; k < 5; k++) fph[k].push_back((r[k + 1] - r[k]) * 1e-3);
     }
     out[0] = a * 1e3; out[1] = b * 1e3;
     out[2] = pct(cvs, 50); out[3] = pct(cvs, 100);
     out[4] = pct(coord, 0); out[5] = pct(coord, 50); out[6] = pct(coord, 100);
     out[7] = pct(end, 50); out[8] = pct(end, 100);
     out[9] = pct(fdur, 50); out[10] = pct(fdur, 100); out[11] = pct(fend, 100);
+    for (int k = 0; k < 5; k++) out[16 + k] = pct(fph[k], 50);
     out[12] = (double)I.steps.size(); out[13] = (double)I.grid; out[14] = (double)I.parts; out[15] = (double)fg;
 }
 

@@ -184,9 +184,9 @@ __global__ void k_scatter(JacDev J, const int* __restrict__ u2g, const double* _
         long long fx = (long long)(-(g * (double)J.gx[r]) * S);
         long long fy = (long long)(-(g * (double)J.gy[r]) * S);
         long long fz = (long long)(-(g * (double)J.gz[r]) * S);
-        atomicAdd(force + a, (unsigned long long)fx);
-        atomicAdd(force + a + padded, (unsigned long long)fy);
-        atomicAdd(force + a + 2 * padded, (unsigned long long)fz);
+        redAddGlobal(force + a, (unsigned long long)fx);
+        redAddGlobal(force + a + padded, (unsigned long long)fy);
+        redAddGlobal(force + a + 2 * padded, (unsigned long long)fz);
     }
 }
 

@@ -72,7 +72,7 @@ __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ void redAddI64(unsigned long long* p, long long v) {
-    atomicAdd(p, (unsigned long long)v);
+    redAddGlobal(p, (unsigned long long)v);
 }
 
 // Pair constants of one item in scaled units (coordinates divided by r0).

@@ -41,6 +41,14 @@ __device__ __forceinline__ F3 minImage(F3 d, const BoxDev& b) {
     return d;
 }
 
+// Fire-and-forget 64-bit integer add into global memory (fixed-point forces and
+// gradient sums). Written as red.global so that a pointer the compiler cannot
+// prove global (loaded from a struct or shared memory) does not turn into a
+// returning atomic that the thread then waits for.
+__device__ __forceinline__ void redAddGlobal(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 __device__ __forceinline__ double warpSum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -286,7 +286,9 @@ int glued_batch_launch_count(glued_batch* b, long long* count);
  * CTA started (min, median, max); end of a runs CTA incl. its hill items (median,
  * max); finalize CTA duration (median, max); last finalize CTA end after the
  * first one started; coordination steps, runs grid, finalize CTAs per walker,
- * finalize grid}. No reference counterpart.                                   */
+ * finalize grid; median durations of the finalize phases: walker record, rows
+ * and CN, hill partials and reduction, dU/dCV, scatter}. No reference
+ * counterpart.                                                                */
 int glued_batch_phase_times(glued_batch* b, double* out);
 
 #ifdef __cplusplus
