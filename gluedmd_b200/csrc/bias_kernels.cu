@@ -62,10 +62,65 @@ __device__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* sG, d
     for (int d = 0; d < D; d++) sG[b.cvIdx[d]] += dV[d] * b.invSp[d];
 }
 
+// Kernel sums of the OPES and hill-sum MetaD biases (CommonGluedKernels.cpp:2642-2700
+// for OPES), spread over KSUM_CTAS CTAs per bias: each CTA sums a contiguous
+// range of kernels (per thread, then a fixed block tree) into 9 FP64 partials
+// {dV/ds_0..7 terms, value}; k_biases sums the partials in CTA order.
+__global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__ biases,
+                                                      const double* __restrict__ cvv, double* __restrict__ part) {
+    __shared__ double red[32 * 9];
+    const BiasDev& b = biases[blockIdx.y];
+    if (b.type != BIAS_OPES && b.type != BIAS_METAD_HILLS) return;  // uniform over the CTA
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int D = b.D;
+    const int K = b.type == BIAS_OPES ? *b.numKernels : *b.hCount;
+    const int k0 = (int)((long long)K * blockIdx.x / gridDim.x);
+    const int k1 = (int)((long long)K * (blockIdx.x + 1) / gridDim.x);
+    double s[8];
+    for (int d = 0; d < D; d++) s[d] = cvv[b.cvIdx[d]];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (b.type == BIAS_OPES) {
+        const double kfloor = exp(-0.5 * b.cutoff2);
+        for (int k = k0 + tid; k < k1; k += nt) {
+            double n2 = 0, dc[8], is2[8];
+            for (int d = 0; d < D; d++) {
+                dc[d] = s[d] - b.centers[k * D + d];
+                double sg = b.sigmas[k * D + d];
+                is2[d] = 1.0 / (sg * sg);
+                n2 += dc[d] * dc[d] * is2[d];
+            }
+            if (!(n2 < b.cutoff2)) continue;
+            double G = exp(-0.5 * n2), kern = G - kfloor;
+            if (kern <= 0.0) continue;
+            double h = exp(b.logW[k]);
+            if (!(h > 0.0 && h < 1e308)) continue;
+            acc[8] += h * kern;
+            for (int d = 0; d < D; d++) acc[d] += h * G * (-dc[d] * is2[d]);
+        }
+    } else {
+        // direct hill sum, exponent > 8 truncated like the grid deposit
+        for (int k = k0 + tid; k < k1; k += nt) {
+            double ex = 0, dc[8];
+            for (int d = 0; d < D; d++) {
+                double x = s[d] - b.hCenters[k * D + d];
+                if (b.period[d] > 0) x -= round(x / b.period[d]) * b.period[d];
+                dc[d] = x;
+                ex += x * x / (2.0 * b.sigma[d] * b.sigma[d]);
+            }
+            if (ex > 8.0) continue;
+            double g = b.hHeights[k] * exp(-ex);
+            acc[8] += g;
+            for (int d = 0; d < D; d++) acc[d] += -g * dc[d] / (b.sigma[d] * b.sigma[d]);
+        }
+    }
+    blockSum<9>(acc, red);
+    if (tid < 9) part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 9 + tid] = acc[tid];
+}
+
 __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ biases, int nb,
                                                  const double* __restrict__ cvv, int numCVs,
                                                  const double* __restrict__ testGrad, double* __restrict__ dUdCV,
-                                                 double* __restrict__ energies) {
+                                                 double* __restrict__ energies, const double* __restrict__ sumPart) {
     extern __shared__ double sG[];
     __shared__ double red[32 * 9];
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -105,26 +160,10 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
                 if (K == 0) {
                     if (tid == 0) energies[b.slot] = -b.barrier;
                 } else {
-                    double s[8];
-                    for (int d = 0; d < D; d++) s[d] = cvv[b.cvIdx[d]];
-                    const double kfloor = exp(-0.5 * b.cutoff2);
+                    // kernel sum: partials of k_kernel_sums, summed in CTA order
                     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-                    for (int k = tid; k < K; k += nt) {
-                        double n2 = 0, dc[8], is2[8];
-                        for (int d = 0; d < D; d++) {
-                            dc[d] = s[d] - b.centers[k * D + d];
-                            double sg = b.sigmas[k * D + d];
-                            is2[d] = 1.0 / (sg * sg);
-                            n2 += dc[d] * dc[d] * is2[d];
-                        }
-                        if (!(n2 < b.cutoff2)) continue;
-                        double G = exp(-0.5 * n2), kern = G - kfloor;
-                        if (kern <= 0.0) continue;
-                        double h = exp(b.logW[k]);
-                        if (!(h > 0.0 && h < 1e308)) continue;
-                        acc[8] += h * kern;
-                        for (int d = 0; d < D; d++) acc[d] += h * G * (-dc[d] * is2[d]);
-                    }
+                    if (tid < KSUM_CTAS)
+                        for (int i = 0; i < 9; i++) acc[i] = sumPart[((size_t)bi * KSUM_CTAS + tid) * 9 + i];
                     blockSum<9>(acc, red);
                     if (tid == 0) {
                         double prob = acc[8];
@@ -146,23 +185,10 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
             const BiasDev& b = biases[bi];
             if (b.type != BIAS_METAD_HILLS) continue;
             // Direct hill sum, exponent > 8 truncated like the grid deposit.
-            const int D = b.D, K = *b.hCount;
-            double s[8];
-            for (int d = 0; d < D; d++) s[d] = cvv[b.cvIdx[d]];
+            const int D = b.D;
             double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            for (int k = tid; k < K; k += nt) {
-                double ex = 0, dc[8];
-                for (int d = 0; d < D; d++) {
-                    double x = s[d] - b.hCenters[k * D + d];
-                    if (b.period[d] > 0) x -= round(x / b.period[d]) * b.period[d];
-                    dc[d] = x;
-                    ex += x * x / (2.0 * b.sigma[d] * b.sigma[d]);
-                }
-                if (ex > 8.0) continue;
-                double g = b.hHeights[k] * exp(-ex);
-                acc[8] += g;
-                for (int d = 0; d < D; d++) acc[d] += -g * dc[d] / (b.sigma[d] * b.sigma[d]);
-            }
+            if (tid < KSUM_CTAS)
+                for (int i = 0; i < 9; i++) acc[i] = sumPart[((size_t)bi * KSUM_CTAS + tid) * 9 + i];
             blockSum<9>(acc, red);
             if (tid == 0) {
                 energies[b.slot] = acc[8];
@@ -255,9 +281,10 @@ __global__ void k_hills_deposit(const BiasDev* __restrict__ bp, const double* __
 }
 
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
-                  const double* testGrad, double* dUdCV, double* energies) {
+                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums) {
+    if (kernelSums && !testGrad && nb > 0) k_kernel_sums<<<dim3(KSUM_CTAS, nb), 256, 0, s>>>(biases, cvv, sumPart);
     size_t smem = sizeof(double) * (size_t)(numCVs > 0 ? numCVs : 1);
-    k_biases<<<1, 512, smem, s>>>(biases, nb, cvv, numCVs, testGrad, dUdCV, energies);
+    k_biases<<<1, 512, smem, s>>>(biases, nb, cvv, numCVs, testGrad, dUdCV, energies, sumPart);
 }
 
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,

@@ -342,7 +342,16 @@ void Context::buildPlan(const GluedForce& f) {
     gAtoms_.upload(gAtoms); gMass_.upload(gMass); gRef_.upload(gRef); gEv_.upload(gEv);
     cmPairs_.upload(cmPairs); cmParams_.upload(cmParams);
     G_.items = groupItems_.as<GroupItem>(); G_.numItems = (int)groups.size();
-    G_.atoms = gAtoms_.as<int>(); G_.mass = gMass_.as<float>(); G_.ref = gRef_.as<float>();
+    gSlots_.alloc(sizeof(int) * std::max((size_t)1, gAtoms.size()));
+    gAtomsN_ = (int)gAtoms.size();
+    groupCached_ = 1;
+    for (const GroupItem& gi : groups) {
+        if (gi.type == CV_CONTACTMAP) continue;
+        const int n = (gi.type == CV_COM_DISTANCE ? gi.s2 : gi.s1) - gi.s0;
+        groupCached_ = std::max(groupCached_, n);
+    }
+    G_.atoms = gAtoms_.as<int>(); G_.slots = gSlots_.as<int>();
+    G_.mass = gMass_.as<float>(); G_.ref = gRef_.as<float>();
     G_.ev = gEv_.as<float>(); G_.cmPairs = cmPairs_.as<int2>(); G_.cmParams = cmParams_.as<float4>();
     // coordination: tile-major step list over a persistent grid (coord_run.cuh)
     if (!coord.empty()) {
@@ -530,6 +539,10 @@ void Context::setupBiases(const GluedForce& f) {
     biasDev_.upload(arr);
     mergeFlag_.alloc(sizeof(int) * 4);
     uprobPartial_.alloc(sizeof(double) * nUprobPartial_);
+    kernelSums_ = false;
+    for (auto& hb : biases_)
+        if (hb.spec.type == BIAS_OPES || hb.spec.type == BIAS_METAD_HILLS) kernelSums_ = true;
+    sumPart_.alloc(sizeof(double) * (size_t)std::max(nb, 1) * KSUM_CTAS * 9);
 }
 
 void Context::syncUploadBias(HostBias& hb) {
@@ -556,6 +569,7 @@ void Context::atomsReordered() {
     requireBound();
     launchInvertIndex(stream_, atomIndex_, u2g_.as<int>(), numParticles_);
     launchComposeSlots(stream_, coordAtoms_.as<int>(), u2g_.as<int>(), coordSlots_.as<int>(), coordAtomsN_);
+    launchComposeSlots(stream_, gAtoms_.as<int>(), u2g_.as<int>(), gSlots_.as<int>(), gAtomsN_);
     cudaCheck(cudaGetLastError(), "invert index");
 }
 
@@ -600,18 +614,20 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
     const int* u2g = u2g_.as<int>();
     auto want = [&](int p) { return onlyPhase < 0 || onlyPhase == p; };
     if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
-    if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_);
+    if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_);
     if (want(2) || want(3))
         launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv,
                     onlyPhase < 0 ? 3 : (onlyPhase == 2 ? 1 : 2));
     if (want(4))
         launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
-                     testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>());
+                     testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>(),
+                     sumPart_.as<double>(), kernelSums_);
     if (includeForces && want(5)) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
 }
 
 int Context::kernelsPerExecute(bool includeForces) const {
     int k = 1;  // biases
+    if (kernelSums_ && !testGrad_.p && !biases_.empty()) k++;
     if (numSimple_ > 0) k++;
     if (G_.numItems > 0) k++;
     if (coordItemsN_ > 0) k += 2;

@@ -113,10 +113,12 @@ private:
     // device state
     DBuf u2g_, box_, cvv_, dudcv_, energies_, testGrad_;
     DBuf jAtom_, jx_, jy_, jz_, jCv_;
-    DBuf simple_, groupItems_, gAtoms_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
+    DBuf simple_, groupItems_, gAtoms_, gSlots_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
+    int gAtomsN_ = 0, groupCached_ = 1;
     DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnPiece_;
     DBuf coordSysPosq_;
-    DBuf biasDev_, mergeFlag_, uprobPartial_;
+    DBuf biasDev_, mergeFlag_, uprobPartial_, sumPart_;
+    bool kernelSums_ = false;
     JacDev J_{};
     int numSimple_ = 0;
     GroupDev G_{};

@@ -9,6 +9,9 @@
 //   k_invert_index: user -> GPU slot map from OpenMM's atomIndexArray
 // Values go to cvValues (double); Jacobian gradients to the float SoA table whose
 // atom / CV columns are written once when the plan is built.
+#include <algorithm>
+
+#include "context.hpp"
 #include "devfn.cuh"
 #include "kernels.hpp"
 #include "force.hpp"
@@ -102,20 +105,52 @@ __device__ void jacobi4(double A[4][4], double V[4][4], double w[4]) {
     for (int i = 0; i < 4; i++) w[i] = A[i][i];
 }
 
-__global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ posq, const int* __restrict__ u2g,
-                                                   GroupDev G, const BoxDev* __restrict__ boxp,
-                                                   double* __restrict__ cvv, JacDev J) {
+// Positions of the group atoms [a0, a1) are gathered once into shared memory
+// (through the precomposed posq rows, GATHER_U loads in flight per thread) when
+// the group fits GROUP_CACHE atoms; every pass of the CV then reads them there.
+constexpr int GROUP_CACHE = 8192;
+constexpr int GROUP_THREADS = 512;
+constexpr int GATHER_U = 16;
+
+__global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __restrict__ posq,
+                                                             const int* __restrict__ u2g, GroupDev G,
+                                                             const BoxDev* __restrict__ boxp,
+                                                             double* __restrict__ cvv, JacDev J) {
+    extern __shared__ float4 sPos[];
     __shared__ double red[32 * 16];
     __shared__ float wbuf[128];
     __shared__ double bc[16];
     const GroupItem it = G.items[blockIdx.x];
     const BoxDev box = *boxp;
     const int tid = threadIdx.x, nt = blockDim.x;
+    // atoms read through pos(j): cached when the group fits
+    int a0 = it.s0, a1 = it.s1;
+    if (it.type == CV_COM_DISTANCE) a1 = it.s2;
+    const bool cached = it.type != CV_CONTACTMAP && a1 - a0 <= GROUP_CACHE;
+    if (cached) {
+        const int n = a1 - a0;
+        for (int base = tid; base < n; base += nt * GATHER_U) {
+            int slot[GATHER_U];
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++) {
+                const int j = base + nt * u;
+                slot[u] = j < n ? __ldg(G.slots + a0 + j) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++)
+                if (slot[u] >= 0) sPos[base + nt * u] = __ldg(posq + slot[u]);
+        }
+        __syncthreads();
+    }
+    auto pos = [&](int j) -> F3 {
+        if (cached) { const float4 p = sPos[j - a0]; return f3(p.x, p.y, p.z); }
+        return loadPos(posq, nullptr, G.slots[j]);
+    };
 
     if (it.type == CV_COM_DISTANCE) {
         double v[6] = {0, 0, 0, 0, 0, 0};
         for (int j = it.s0 + tid; j < it.s2; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             double m = G.mass[j];
             int o = j < it.s1 ? 0 : 3;
             v[o] += m * p.x; v[o + 1] += m * p.y; v[o + 2] += m * p.z;
@@ -138,7 +173,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
     } else if (it.type == CV_GYRATION) {
         double v[3] = {0, 0, 0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             double m = G.mass[j];
             v[0] += m * p.x; v[1] += m * p.y; v[2] += m * p.z;
         }
@@ -147,7 +182,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         F3 com = f3((float)v[0] * iM, (float)v[1] * iM, (float)v[2] * iM);
         double q[1] = {0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 d = minImage(sub3(loadPos(posq, u2g, G.atoms[j]), com), box);
+            F3 d = minImage(sub3(pos(j), com), box);
             q[0] += (double)G.mass[j] * (double)dot3(d, d);
         }
         blockSum<1>(q, red);
@@ -155,7 +190,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         float irg = rg > 1e-10f ? 1.0f / rg : 0.0f;
         if (tid == 0) cvv[it.cv] = (double)rg;
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 d = minImage(sub3(loadPos(posq, u2g, G.atoms[j]), com), box);
+            F3 d = minImage(sub3(pos(j), com), box);
             float w = G.mass[j] / it.f0;
             int r = it.jac0 + j;
             J.gx[r] = w * d.x * irg; J.gy[r] = w * d.y * irg; J.gz[r] = w * d.z * irg;
@@ -163,7 +198,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
     } else if (it.type == CV_RMSD) {
         double q[1] = {0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             F3 d = f3(p.x - G.ref[3 * j], p.y - G.ref[3 * j + 1], p.z - G.ref[3 * j + 2]);
             q[0] += (double)dot3(d, d);
         }
@@ -173,7 +208,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         float sc = (rmsd > 1e-10f ? 1.0f / rmsd : 0.0f) / (float)na;
         if (tid == 0) cvv[it.cv] = (double)rmsd;
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             int r = it.jac0 + j;
             J.gx[r] = (p.x - G.ref[3 * j]) * sc; J.gy[r] = (p.y - G.ref[3 * j + 1]) * sc;
             J.gz[r] = (p.z - G.ref[3 * j + 2]) * sc;
@@ -181,7 +216,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
     } else if (it.type == CV_PCA) {
         double q[1] = {0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             float dx = p.x - G.ref[3 * j], dy = p.y - G.ref[3 * j + 1], dz = p.z - G.ref[3 * j + 2];
             q[0] += (double)(dx * G.ev[3 * j] + dy * G.ev[3 * j + 1] + dz * G.ev[3 * j + 2]);
         }
@@ -201,7 +236,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
             float acc = 0.0f;
             const float* rf = G.ref + 3 * (it.r0 + f * M);
             for (int j = lane; j < M; j += 32) {
-                F3 p = loadPos(posq, u2g, G.atoms[it.s0 + j]);
+                F3 p = pos(it.s0 + j);
                 float dx = p.x - rf[3 * j], dy = p.y - rf[3 * j + 1], dz = p.z - rf[3 * j + 2];
                 acc += dx * dx + dy * dy + dz * dz;
             }
@@ -221,7 +256,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         float s = (float)bc[0], S = (float)bc[1];
         float scS = -2.0f * lam / ((float)M * S), scZ = 2.0f / ((float)M * S);
         for (int j = tid; j < M; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[it.s0 + j]);
+            F3 p = pos(it.s0 + j);
             float sx = 0, sy = 0, sz = 0, zx = 0, zy = 0, zz = 0;
             for (int f = 0; f < N; f++) {
                 const float* rf = G.ref + 3 * (it.r0 + f * M + j);
@@ -278,7 +313,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         const int na = it.s1 - it.s0;
         double v[6] = {0, 0, 0, 0, 0, 0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             v[0] += p.x; v[1] += p.y; v[2] += p.z;
             v[3] += G.ref[3 * j]; v[4] += G.ref[3 * j + 1]; v[5] += G.ref[3 * j + 2];
         }
@@ -286,7 +321,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         double xc[3] = {v[0] / na, v[1] / na, v[2] / na}, yc[3] = {v[3] / na, v[4] / na, v[5] / na};
         double c[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             double x[3] = {p.x - xc[0], p.y - xc[1], p.z - xc[2]};
             double y[3] = {G.ref[3 * j] - yc[0], G.ref[3 * j + 1] - yc[1], G.ref[3 * j + 2] - yc[2]};
             for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) c[3 * a + b] += x[a] * y[b];
@@ -315,7 +350,7 @@ __global__ void __launch_bounds__(256) k_group_cvs(const float4* __restrict__ po
         }
         __syncthreads();
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
-            F3 p = loadPos(posq, u2g, G.atoms[j]);
+            F3 p = pos(j);
             double x[3] = {p.x - xc[0], p.y - xc[1], p.z - xc[2]};
             double y[3] = {G.ref[3 * j] - yc[0], G.ref[3 * j + 1] - yc[1], G.ref[3 * j + 2] - yc[2]};
             double g[3];
@@ -359,8 +394,16 @@ void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const S
 }
 
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
-                    double* cvv, const JacDev& J) {
-    if (G.numItems > 0) k_group_cvs<<<G.numItems, 256, 0, s>>>(posq, u2g, G, box, cvv, J);
+                    double* cvv, const JacDev& J, int maxCached) {
+    if (G.numItems <= 0) return;
+    const size_t smem = sizeof(float4) * (size_t)std::min(std::max(maxCached, 1), GROUP_CACHE);
+    static bool attr = false;
+    if (!attr) {
+        cudaCheck(cudaFuncSetAttribute((const void*)k_group_cvs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(float4) * GROUP_CACHE)), "group CV shared memory");
+        attr = true;
+    }
+    k_group_cvs<<<G.numItems, GROUP_THREADS, smem, s>>>(posq, u2g, G, box, cvv, J);
 }
 
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,

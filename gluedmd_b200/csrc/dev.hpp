@@ -57,6 +57,7 @@ struct GroupDev {
     const GroupItem* items;
     int numItems;
     const int* atoms;
+    const int* slots;      // posq row of every group atom (u2g of atoms), rebuilt on reorder
     const float* mass;
     const float* ref;      // xyz per atom (RMSD/PCA/Kabsch) or per frame-atom (path)
     const float* ev;       // PCA eigenvectors, xyz per atom

@@ -11,8 +11,9 @@ namespace glued {
 void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n);
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
                      const BoxDev* box, double* cvv, const JacDev& J);
+// maxCached: the largest atom range of a cached group CV (shared memory size).
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
-                    double* cvv, const JacDev& J);
+                    double* cvv, const JacDev& J, int maxCached);
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
                      int numAtoms, int mode, double scale, const BoxDev* box);
 // Coordination runs (coord_run.cuh). parts: bit 0 = pair runs, bit 1 = finalize
@@ -34,8 +35,11 @@ std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>
 // item's slot range. Returns the number of pieces.
 int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begin, std::vector<CoordItem>& items);
 bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool periodic);
+// Kernel-sum biases (OPES, hill-sum MetaD) are summed by KSUM_CTAS CTAs per bias
+// into sumPart[nb][KSUM_CTAS][9] first (kernelSums), then k_biases combines them.
+constexpr int KSUM_CTAS = 64;
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
-                  const double* testGrad, double* dUdCV, double* energies);
+                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums);
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
                    int padded);
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
