@@ -30,6 +30,10 @@ sys.path.insert(0, ROOT)
 
 FLOP_PAIR = 45.0      # coordination pair, FMA = 2 flops (per-pair count of the workload spec)
 FLOP_HILL = 14.0      # one hill Gaussian + gradient (plus one exp)
+# DRAM bytes (read + write) of one launch, from the ncu captures summarised under
+# profiles/ (cold caches, one launch of the full workload)
+TRAFFIC_C4_RUNS = 8.085e6
+TRAFFIC_C2_COORD = 0.724e6
 
 
 def peaks():
@@ -298,11 +302,21 @@ def run_c4(args, torch, ws, hill):
     d2h = host_f.numel() * 8 + 8 * W_
     pairs = sum(256 * 1024 for _ in ws)
     flops = pairs * FLOP_PAIR + W_ * b.num_hills() * FLOP_HILL
+    # per-kernel durations (CUDA events around each launch of one step, L2 flushed
+    # before every step): the dominant kernel is the coordination-runs kernel
+    runs, fins = [], []
+    for i in range(20):
+        flush.add_(1.0)
+        pt = b.phase_times()
+        runs.append(pt["runs_us"])
+        fins.append(pt["finalize_us"])
+    runs_us = sum(runs) / len(runs)
+    fin_us = sum(fins) / len(fins)
     return dict(walkers=W_, step_ms=step_ms, value=W_ * 1e3 / step_ms, plain_ms=plain_ms,
                 plain_value=W_ * 1e3 / plain_ms, plain_launches=plain_launches, e2e_value=W_ * 1e3 / e2e_ms,
                 h2d=int(h2d), d2h=int(d2h), launches_per_step=launches / float(args.steps + args.warmup),
                 flops=flops, clocks=clk.summary(), tune=tune, status=status, hills=b.num_hills(),
-                graphed=True)
+                graphed=True, runs_us=runs_us, finalize_us=fin_us)
 
 
 def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
@@ -436,11 +450,17 @@ def main():
         if rank == 0:
             fp32 = ctypes.c_double()
             _native.call("glued_measure_fp32_peak", ctypes.byref(fp32))
-            ach = info["flops"] / (info["step_ms"] * 1e-3) / 1e12
-            roof = {"bound": "fp32", "kernel": "k_batch_step (whole step, one launch)", "achieved": ach,
-                    "peak": fp32.value, "unit": "TFLOP/s", "frac": ach / fp32.value, "traffic": None,
+            ach = info["flops"] / (info["runs_us"] * 1e-6) / 1e12
+            roof = {"bound": "fp32", "kernel": "k_batch_runs (coordination pairs + hill table)", "achieved": ach,
+                    "peak": fp32.value, "unit": "TFLOP/s", "frac": ach / fp32.value,
+                    "traffic": TRAFFIC_C4_RUNS, "traffic_unit": "bytes per launch",
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture "
+                                      "(profiles/k_batch_runs_c4.md)",
+                    "launch_us": info["runs_us"],
                     "peak_source": "FP32 FMA microkernel measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
-                    "algorithmic": f"64 x 262144 pairs x {FLOP_PAIR:.0f} flop + 64 x {info['hills']} hills x {FLOP_HILL:.0f} flop"}
+                    "algorithmic": f"64 x 262144 pairs x {FLOP_PAIR:.0f} flop + 64 x {info['hills']} hills x {FLOP_HILL:.0f} flop",
+                    "whole_step_frac": info["flops"] / (info["step_ms"] * 1e-3) / 1e12 / fp32.value,
+                    "finalize_us": info["finalize_us"]}
             cb = None
             if not args.no_cpu_baseline and world == 1:
                 cb = cpu_reference_c4(ws, hill, steps_budget_s=15.0)
@@ -483,8 +503,11 @@ def main():
         pairs = sum((len(a) - 1 - a[0]) * a[0] for t, a, p in w.cvs if t == 6)
         flops = pairs * FLOP_PAIR
         ach = flops / (info["dom_ms"] * 1e-3) / 1e12
-        roof = {"bound": "fp32", "kernel": "k_coord_pairs", "achieved": ach, "peak": fp32.value,
-                "unit": "TFLOP/s", "frac": ach / fp32.value, "traffic": None,
+        roof = {"bound": "fp32", "kernel": "k_coord_run", "achieved": ach, "peak": fp32.value,
+                "unit": "TFLOP/s", "frac": ach / fp32.value, "traffic": TRAFFIC_C2_COORD,
+                "traffic_unit": "bytes per launch",
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture "
+                                  "(profiles/k_coord_run_c2.md)",
                 "peak_source": "FP32 FMA microkernel measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
                 "algorithmic": f"{pairs} pairs x {FLOP_PAIR:.0f} flop"}
     cb = None
