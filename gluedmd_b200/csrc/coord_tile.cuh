@@ -1,5 +1,11 @@
-// Coordination pair tile shared by the per-context kernel and the batched
-// multi-walker kernel (see coord_kernels.cu for the scheme).
+// Partial-sum coordination tile used by the allocation-free entry point
+// (noalloc.cu): one CTA takes TA = 8*RA A atoms against a split of group B;
+// warp w holds A atoms {w, w+8, ...} in registers (all lanes share them), lane l
+// walks B atoms {l, l+32, l+64, l+96} of each 128-atom chunk; A gradients are
+// reduced over lanes by a fixed shuffle tree, B gradients of a chunk over the 8
+// warps in fixed order, and both are written as float partials per (tile,
+// split); the CN partial of each CTA is a double. The context and batched paths
+// use the step runs of coord_run.cuh instead.
 #pragma once
 
 #include "devfn.cuh"

@@ -10,9 +10,10 @@
 // device code is loaded on a GPU and stays resident on every GPU that loads it
 // until the process exits. The caller passes only inputs and outputs.
 //
-// The kernels are the regular coordination tile (coord_tile.cuh) and a
-// fixed-order reduction of its partials, so the results equal the context
-// path's for the same tiling.
+// The kernels are the partial-sum coordination tile (coord_tile.cuh: one CTA
+// per 64-atom A tile and B split, float partials) and a fixed-order reduction of
+// its partials; the results agree with the context path (fixed-point step runs,
+// coord_run.cuh) to FP32 rounding.
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
