@@ -103,6 +103,7 @@ _SIGS = {
     "glued_batch_status": [c_void_p, P(c_int)],
     "glued_batch_launch_count": [c_void_p, P(c_ll)],
     "glued_batch_phase_times": [c_void_p, P(c_double)],
+    "glued_batch_phase_stamps": [c_void_p, P(ctypes.c_ulonglong), c_ll, P(c_ll)],
 }
 
 

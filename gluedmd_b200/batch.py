@@ -1,7 +1,8 @@
 """Batched multi-walker evaluation (glued_batch_* of include/glued_b200.h).
 
 All walkers of one GPU are evaluated by one graph per step: a persistent
-kernel for the coordination pairs and the hill table, then a finalize kernel. Each walker owns a float4 posq buffer and an int64 fixed-point force
+kernel for the coordination pairs, then a finalize kernel that also sums the
+shared hill table per walker. Each walker owns a float4 posq buffer and an int64 fixed-point force
 buffer in device memory (torch tensors here); walkers may have different atom
 counts and boxes but the same CV / bias structure.
 """
@@ -146,28 +147,42 @@ class Batch:
     def phase_times(self):
         """One step with each launch bracketed by CUDA events and every CTA
         time-stamped (microseconds); see glued_batch_phase_times."""
-        out = (c_double * 21)()
+        out = (c_double * 24)()
         call("glued_batch_phase_times", self._h, out)
-        keys = ["runs_us", "finalize_us", "hill_cvs_med_us", "hill_cvs_max_us", "coord_end_min_us",
+        keys = ["runs_us", "finalize_us", "stage_med_us", "stage_max_us", "coord_end_min_us",
                 "coord_end_med_us", "coord_end_max_us", "runs_end_med_us", "runs_end_max_us",
                 "fin_cta_med_us", "fin_cta_max_us", "fin_end_max_us", "coord_steps", "grid", "parts",
-                "finalize_grid", "fin_record_us", "fin_rows_cn_us", "fin_hills_us", "fin_du_us", "fin_scatter_us"]
-        return dict(zip(keys, out[:]))
+                "finalize_grid", "fin_record_us", "fin_cn_us", "fin_energy_us", "fin_coord_scatter_us",
+                "fin_simple_rows_us", "hill_wait_us", "hill_eval_us", "hill_reduce_us"]
+        self.phase_times_last = dict(zip(keys, out[:]))
+        return dict(self.phase_times_last)
+
+    def phase_stamps(self):
+        """Raw records of the last phase_times call: (runs [grid, 8] = SM id,
+        coordination steps, six %globaltimer stamps in ns; finalize [CTAs, 6])."""
+        n = c_ll()
+        call("glued_batch_phase_stamps", self._h, None, 0, ctypes.byref(n))
+        buf = (ctypes.c_ulonglong * max(1, n.value))()
+        call("glued_batch_phase_stamps", self._h, buf, n.value, ctypes.byref(n))
+        v = np.array(buf[:n.value], dtype=np.uint64)
+        grid = int(self.phase_times_last["grid"]) if hasattr(self, "phase_times_last") else 0
+        runs = v[:8 * grid].reshape(grid, 8)
+        return runs, v[8 * grid:].reshape(-1, 6)
 
     @property
     def tuning(self):
         t = (c_int * 4)()
         call("glued_batch_get_tuning", self._h, t)
-        return dict(ra=t[0], parts=t[1], hill_weight_pct=t[2], hill_chunk=t[3])
+        return dict(ra=t[0], parts=t[1], fused=t[2])
 
-    def set_tuning(self, ra=8, parts=0, hill_weight_pct=150, hill_chunk=0):
-        t = (c_int * 4)(ra, parts, hill_weight_pct, hill_chunk)
+    def set_tuning(self, ra=8, parts=0, fused=0):
+        t = (c_int * 4)(ra, parts, fused, 0)
         call("glued_batch_set_tuning", self._h, t)
 
     def autotune(self):
         t = (c_int * 4)()
         call("glued_batch_autotune", self._h, t)
-        return dict(ra=t[0], parts=t[1], hill_weight_pct=t[2], hill_chunk=t[3])
+        return dict(ra=t[0], parts=t[1], fused=t[2])
 
 
 def force_for(cvs, biases, pbc=True):

@@ -6,16 +6,17 @@
 // platforms/common/src/CommonGluedKernels.cpp:5234-5262). Here all walkers of a
 // GPU are evaluated together:
 //
-//   1. Coordination runs (coord_run.cuh, launched through launchCoord): the
-//      (A tile, B chunk) steps of every walker's coordination CVs, walker-major,
-//      in equal static ranges over a persistent grid (SMs x resident CTAs);
-//      gradients accumulate in 64-bit fixed point, CN partials per run piece.
+//   1. k_batch_runs, a persistent grid (SMs x resident CTAs): every CTA runs an
+//      equal static range of the (A tile, B chunk) coordination steps of all
+//      walkers (coord_run.cuh; gradients in 64-bit fixed point, CN partials per
+//      run piece), then evaluates an equal slice of the shared hill table for
+//      every walker (slice and hill-CV atoms staged in shared memory when the
+//      CTA starts), one FP64 partial per (CTA, walker).
 //   2. k_batch_finalize, walkers x parts CTAs: each part clears and scatters its
 //      share of the walker's coordination rows (dU/dCN needs only CN and the
-//      harmonic terms: the hill bias acts on distance/angle/dihedral CVs) and
-//      evaluates its share of the shared hill table for that walker; the last
-//      part to finish sums the hill partials in part order and completes the
-//      walker (harmonic terms, energy, the distance/angle/dihedral rows).
+//      harmonic terms: the hill bias acts on distance/angle/dihedral CVs); part
+//      0 also sums the hill partials in CTA order and completes the walker
+//      (harmonic terms, energy, the distance/angle/dihedral rows).
 //
 // Every reduction has a fixed order or is an integer sum, so a step is bitwise
 // reproducible. Deposition (updateState at pace): one hill per walker, in walker
@@ -39,8 +40,8 @@ constexpr int MAXSIMPLE = 16;  // distance/angle/dihedral CVs per walker
 constexpr int MAXHARM = 32;    // harmonic terms per walker
 constexpr int FT = 256;        // threads of a finalize CTA
 constexpr int ROWS_PER_THREAD = 2;   // coordination rows one finalize thread scatters
-constexpr int WBLK = 64;       // walkers per hill item (8 per warp)
-constexpr int HC_MAX = 1024;   // hills per hill item, at most (shared-memory staging)
+constexpr int WBLK = 64;       // walkers per hill pass (8 per warp)
+constexpr int HS = 256;        // hills staged in shared memory at a time
 }  // namespace
 
 struct BWalker {
@@ -58,7 +59,10 @@ struct BHill {
     double* heights;
     int* count;
     int maxH, D, cv[2], pace, present;
-    float a[2], isig2[2], period[2], iperiod[2];
+    // scaled units: s' = u s with u = sqrt(log2(e) / (2 sigma^2)) (0 for an
+    // unused dimension); periods pS = u L (0: not periodic), ipS = 1 / pS;
+    // a hill counts while dx'^2 + dy'^2 <= cut = 8 log2(e); dV/ds = gsc * sum g dx'
+    float u[2], pS[2], ipS[2], gsc[2], cut;
     double h0, hif;
 };
 
@@ -72,13 +76,18 @@ struct BatchDev {
     int rowsPerWalker;      // coordination rows of one walker (all its items)
     int parts;              // finalize CTAs per walker
     BHill hill;
-    int nWB;                // walker blocks of <= WBLK walkers
-    int hc;                 // hills per hill item (multiple of 32, <= HC_MAX)
-    double* hillPart;       // [ceil(maxHills / hc)][W][3]
+    const float4* const* hillCvPos;  // [W][2][4] posq addresses of the hill CVs' atoms (nullptr: unused)
+    const int* hillCvType;  // [W][2] CV type of hill dimension d (0: none)
+    const int* rowAtom;     // [W * rowsPerWalker] atom of every coordination row
+    double* hillPart;       // [hillParts][W][3]: hill sums of every runs CTA
+    int hillParts;          // CTAs of the runs grid
     double* cvv;            // [W][nCV]
     double* energy;         // [W]
     double* hillEnergy;     // [W]
-    unsigned long long* stamps;   // profiling (nullptr = off): runs kernel [grid][4]
+    unsigned* bar;                // fused step: grid barrier {count, generation}
+    int* status;                  // bit 0: a grid-barrier wait gave up
+    unsigned long long spinLimit; // polls of a grid-barrier wait before it gives up
+    unsigned long long* stamps;   // profiling (nullptr = off): runs kernel [grid][7] (6 times, SM id)
     unsigned long long* fstamps;  // profiling (nullptr = off): finalize kernel [W * parts][6]
 };
 
@@ -104,108 +113,230 @@ __device__ __forceinline__ void scatterRow(unsigned long long* F, int P, int ato
     redAddGlobal(F + atom + 2 * P, (unsigned long long)(long long)(-(g * (double)gz) * S));
 }
 
-// ------------------------------------------------------------- hill items
-// One item: hc consecutive hills of the shared table against the <= 64 walkers
-// of one walker block. The walkers' hill-CV values are computed once per CTA
-// (sS, one thread per walker and CV); the chunk is staged in shared memory by
-// plain coalesced loads; warp w takes walkers w, w + 8, ...; lane l takes hills
-// l, l + 32, ...; FP32 sums per lane, a fixed xor tree per walker, one partial
-// per (item, walker), summed by the finalize in item order.
-__device__ void hillCVs(const BatchDev& B, int wb, float* sS) {
+// ------------------------------------------------------------- hill slices
+// Every CTA of the runs grid owns an equal contiguous slice of the shared hill
+// table and evaluates it for all walkers after its coordination steps. Data
+// movement stays off the critical path: the CTA's prologue copies (cp.async)
+// the tables it needs first (hill count, posq addresses of the hill CVs' atoms,
+// boxes of <= 64 walkers); when those have landed, before its first
+// coordination step computes, it issues the gathers that depend on them (its
+// slice of the table, HS hills at a time, and the atoms' positions), which land
+// while that step computes. Arithmetic: CVs and hill centres are stored scaled
+// by u = sqrt(log2(e) / (2 sigma^2)) per dimension (the mirror table holds
+// scaled centres), so a hill is exp2(-(dx^2 + dy^2)) of scaled differences;
+// warp w takes walkers w, w + 8, ... (8 at a time in registers), lane l takes
+// hills l, l + 32, ...; FP32 sums per lane, a fixed butterfly over the lanes,
+// one FP64 partial per (CTA, walker), summed by the finalize in CTA order.
+struct HillStage {
+    float4 hills[HS];
+    float4 pos[WBLK * 8];
+    BoxDev box[WBLK];
+    const float4* ptr[WBLK * 8];
+    int count[4];
+    float sS[WBLK * 2];
+};
+
+__device__ __forceinline__ void hillSliceRange(const BatchDev& B, const HillStage& hs, int& h0, int& h1) {
+    const int count = hs.count[0];
+    h0 = (int)((long long)count * blockIdx.x / gridDim.x);
+    h1 = (int)((long long)count * (blockIdx.x + 1) / gridDim.x);
+}
+
+// Tables of walker block wb: count, atom addresses, boxes (no dependent loads).
+__device__ void hillStageTables(const BatchDev& B, int wb, HillStage& hs) {
     const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
-    const BHill& hb = B.hill;
-    const int t = threadIdx.x;
-    if (t < 2 * nw) {
-        const int w = w0 + t / 2, d = t % 2;
-        float v = 0.0f;
-        if (d < hb.D) {
-            const BWalker& wk = B.walkers[w];
-            for (int s = 0; s < B.nS; s++) {
-                const BSimple& si = B.simple[w * B.nS + s];
-                if (si.cv == hb.cv[d]) v = simpleCV(si.type, si.atoms, wk.posq, nullptr, wk.box, nullptr);
-            }
-        }
-        sS[t] = v;
+    static_assert(sizeof(BoxDev) % 16 == 0, "box record");
+    constexpr int BW = sizeof(BoxDev) / 16;
+    const float4* ptrSrc = reinterpret_cast<const float4*>(B.hillCvPos + (size_t)w0 * 8);
+    for (int t = threadIdx.x; t < nw * 4; t += blockDim.x)
+        cpAsync16(reinterpret_cast<float4*>(hs.ptr) + t, ptrSrc + t, true);
+    for (int t = threadIdx.x; t < nw * BW; t += blockDim.x)
+        cpAsync16(reinterpret_cast<float4*>(&hs.box[t / BW]) + t % BW,
+                  reinterpret_cast<const float4*>(B.R.sysBox + w0 + t / BW) + t % BW, true);
+    if (threadIdx.x == 0) cpAsync16(hs.count, B.hill.count, true);
+}
+
+// hills [k0, k0 + HS) of the slice (zero past h1)
+__device__ __forceinline__ void hillStageHills(const BatchDev& B, int k0, int h1, HillStage& hs) {
+    for (int t = threadIdx.x; t < HS; t += blockDim.x) {
+        const int k = k0 + t;
+        cpAsync16(&hs.hills[t], B.hill.mirror + (k < h1 ? k : 0), k < h1);
     }
 }
 
-__device__ void hillItem(const BatchDev& B, int item, int itemsPerBlock, const float* sS, float4* sH) {
-    const BHill& hb = B.hill;
-    const int c = item % itemsPerBlock, wb = item / itemsPerBlock;
+// Gathers that depend on the tables (after they have landed): the first HS
+// hills of the slice and the atoms' positions of walker block wb.
+__device__ void hillStageData(const BatchDev& B, int wb, HillStage& hs) {
     const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
-    const int count = *hb.count;
-    const int hc = B.hc;
-    const int k0 = c * hc, n = max(0, min(hc, count - k0));
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __syncthreads();  // sH free (previous item read), sS written
-    for (int k = tid; k < hc; k += blockDim.x)
-        sH[k] = k < n ? __ldg(hb.mirror + k0 + k) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    __syncthreads();
-    for (int wl = warp; wl < nw; wl += 8) {
-        const float s0 = sS[wl * 2], s1 = sS[wl * 2 + 1];
-        float V = 0.0f, g0 = 0.0f, g1 = 0.0f;
-#pragma unroll 4
-        for (int q = 0; q < hc / 32; q++) {
-            const float4 hk = sH[lane + 32 * q];   // height 0 past the end of the table
-            float dx = s0 - hk.x, dy = s1 - hk.y;
-            if (hb.period[0] > 0.0f) dx -= hb.period[0] * rintf(dx * hb.iperiod[0]);
-            if (hb.period[1] > 0.0f) dy -= hb.period[1] * rintf(dy * hb.iperiod[1]);
-            const float ex = dx * dx * hb.a[0] + dy * dy * hb.a[1];
-            const float g = ex <= 8.0f ? hk.z * __expf(-ex) : 0.0f;
-            V += g; g0 += g * dx; g1 += g * dy;
+    int h0, h1;
+    hillSliceRange(B, hs, h0, h1);
+    hillStageHills(B, h0, h1, hs);
+    for (int t = threadIdx.x; t < nw * 8; t += blockDim.x) {
+        const float4* a = hs.ptr[t];
+        cpAsync16(&hs.pos[t], a ? a : B.hill.mirror, a != nullptr);
+    }
+}
+
+// Scaled hill-CV values of walker block wb from the staged positions.
+__device__ void hillCVs(const BatchDev& B, int wb, HillStage& hs) {
+    const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
+    const int t = threadIdx.x;
+    if (t < 2 * nw) {
+        const int type = B.hillCvType[(w0 + t / 2) * 2 + t % 2];
+        float v = 0.0f;
+        if (type) {
+            F3 p[4];
+            for (int k = 0; k < 4; k++) { const float4 q = hs.pos[t * 4 + k]; p[k] = f3(q.x, q.y, q.z); }
+            v = simpleCVFromPos(type, p, hs.box[t / 2], nullptr);
         }
-        V = warpSumF(V); g0 = warpSumF(g0); g1 = warpSumF(g1);
-        if (lane == 0) {
-            double* out = B.hillPart + 3 * ((size_t)c * B.W + w0 + wl);
-            out[0] = V;
-            out[1] = -(double)g0 * hb.isig2[0];
-            out[2] = -(double)g1 * hb.isig2[1];
+        hs.sS[t] = v * (t % 2 ? B.hill.u[1] : B.hill.u[0]);
+    }
+}
+
+// Hills lane + 32 q (q < nq) of the staged chunk against the 8 walkers of this
+// warp; acc[3 j + c]: sum of g, g dx, g dy for walker slot j.
+template <bool P0, bool P1>
+__device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int nq, const float (&s0)[8],
+                                         const float (&s1)[8], float (&acc)[32]) {
+    constexpr float R = 12582912.0f;   // 1.5 * 2^23: adding and removing it rounds to an integer
+    const int lane = threadIdx.x & 31;
+    for (int q = 0; q < nq; q++) {
+        const float4 hk = hs.hills[lane + 32 * q];   // height 0 past the slice
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            float dx = s0[j] - hk.x, dy = s1[j] - hk.y;
+            if (P0) dx = fmaf(-(fmaf(dx, hb.ipS[0], R) - R), hb.pS[0], dx);
+            if (P1) dy = fmaf(-(fmaf(dy, hb.ipS[1], R) - R), hb.pS[1], dy);
+            const float ex = fmaf(dx, dx, dy * dy);
+            float e;
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-ex));
+            const float g = ex <= hb.cut ? hk.z * e : 0.0f;
+            acc[3 * j] += g;
+            acc[3 * j + 1] = fmaf(g, dx, acc[3 * j + 1]);
+            acc[3 * j + 2] = fmaf(g, dy, acc[3 * j + 2]);
         }
+    }
+}
+
+// This CTA's hill slice for every walker. `gathered`: the data of walker block
+// 0 was issued during the coordination steps.
+__device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, unsigned long long* st) {
+    const BHill& hb = B.hill;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nWB = (B.W + WBLK - 1) / WBLK;
+    for (int wb = 0; wb < nWB; wb++) {
+        const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
+        if (wb > 0) {
+            __syncthreads();   // the previous block's data fully read
+            hillStageTables(B, wb, hs);
+            cpAsyncCommit();
+        }
+        if (wb > 0 || !gathered) {
+            cpAsyncWaitAll();
+            __syncthreads();
+            hillStageData(B, wb, hs);
+            cpAsyncCommit();
+        }
+        cpAsyncWaitAll();
+        __syncthreads();
+        if (st && wb == 0 && threadIdx.x == 0) st[3] = globalTimer();
+        hillCVs(B, wb, hs);
+        __syncthreads();
+        int h0, h1;
+        hillSliceRange(B, hs, h0, h1);
+        float s0[8], s1[8], acc[32];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int wl = min(warp + 8 * j, nw - 1);
+            s0[j] = hs.sS[wl * 2]; s1[j] = hs.sS[wl * 2 + 1];
+        }
+#pragma unroll
+        for (int k = 0; k < 32; k++) acc[k] = 0.0f;
+        for (int k0 = h0; k0 < h1; k0 += HS) {
+            if (k0 != h0) {
+                __syncthreads();
+                hillStageHills(B, k0, h1, hs);
+                cpAsyncCommit();
+                cpAsyncWaitAll();
+                __syncthreads();
+            }
+            const int nq = (min(HS, h1 - k0) + 31) / 32;
+            const bool p0 = hb.pS[0] > 0.0f, p1 = hb.pS[1] > 0.0f;
+            if (p0 && p1) hillEval<true, true>(hs, hb, nq, s0, s1, acc);
+            else if (p0) hillEval<true, false>(hs, hb, nq, s0, s1, acc);
+            else if (p1) hillEval<false, true>(hs, hb, nq, s0, s1, acc);
+            else hillEval<false, false>(hs, hb, nq, s0, s1, acc);
+        }
+        if (st && wb == 0 && threadIdx.x == 0) st[4] = globalTimer();
+        const float v = warpTransposeSum32(acc);   // lane 3 j + c: component c of walker slot j
+        const int j = lane / 3, c = lane - 3 * j;
+        const int wl = warp + 8 * j;
+        if (lane < 24 && wl < nw)
+            B.hillPart[3 * ((size_t)blockIdx.x * B.W + w0 + wl) + c] =
+                c == 0 ? (double)v : (double)v * (c == 1 ? hb.gsc[0] : hb.gsc[1]);
     }
 }
 
 // ------------------------------------------------------------- the runs
-// Persistent CTAs (grid = SMs x resident CTAs): CTA b runs its static range of
-// coordination steps, then its hill items b, b + grid, ... (ranges balanced so
-// that CTAs with more hill items get fewer steps).
+// Persistent CTAs (grid = SMs x resident CTAs): CTA b copies its hill tables,
+// runs its static range of coordination steps (equal step counts; the hill
+// gathers are issued when the first step starts), then evaluates its slice.
+template <int RA, int BOX, int NH, bool HI>
+__device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm, HillStage& hs) {
+    unsigned long long* st = B.stamps ? B.stamps + 7 * (size_t)blockIdx.x : nullptr;
+    if (st && threadIdx.x == 0) {
+        unsigned sm;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+        st[6] = sm;
+        st[0] = globalTimer();
+    }
+    const bool hills = B.hill.present != 0;
+    if (hills) {
+        hillStageTables(B, 0, hs);
+        cpAsyncCommit();
+    }
+    if (st && threadIdx.x == 0) st[1] = globalTimer();
+    const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
+    if (s0 < s1) {
+        if (hills)
+            coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook(), [&]() {
+                hillStageData(B, 0, hs);
+                cpAsyncCommit();
+            });
+        else
+            coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
+    }
+    if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
+    if (hills) hillSlice(B, hs, s0 < s1, st);
+    if (st) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (!hills) st[3] = st[4] = st[2];
+            st[5] = globalTimer();
+        }
+    }
+}
+
 template <int RA, int BOX, int NH, bool HI>
 __global__ void __launch_bounds__(256, 2) k_batch_runs(BatchDev B) {
+    extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ CoordRunSmem<RA> sm;
-    __shared__ float sS[WBLK * 2];
-    const int numHill = B.hill.present ? ((*B.hill.count + B.hc - 1) / B.hc) * B.nWB : 0;
-    int wbHave = -1;
-    unsigned long long* st = B.stamps ? B.stamps + 4 * (size_t)blockIdx.x : nullptr;
-    if (st && threadIdx.x == 0) st[0] = globalTimer();
-    const int perBlock = numHill / max(B.nWB, 1);
-    if ((int)blockIdx.x < numHill) {
-        wbHave = blockIdx.x / perBlock;
-        hillCVs(B, wbHave, sS);
-    }
-    if (st) { __syncthreads(); if (threadIdx.x == 0) st[1] = globalTimer(); }
-    const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
-    if (s0 < s1) coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
-    if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
-    float4* sH = reinterpret_cast<float4*>(&sm.g[0][0][0]);
-    for (int item = blockIdx.x; item < numHill; item += gridDim.x) {
-        const int wb = item / perBlock;
-        if (wb != wbHave) {
-            __syncthreads();
-            hillCVs(B, wb, sS);
-            wbHave = wb;
-        }
-        hillItem(B, item, perBlock, sS, sH);
-    }
-    if (st) { __syncthreads(); if (threadIdx.x == 0) st[3] = globalTimer(); }
+    runsBody<RA, BOX, NH, HI>(B, sm, *reinterpret_cast<HillStage*>(dsm));
 }
 
 // ------------------------------------------------------------- finalize
-// CTA (walker w, part p) after the runs. Every part clears and scatters its share
-// of the walker's coordination rows (at most ROWS_PER_THREAD per thread) with
-// dU/dCN, which needs only CN (the walker's run-piece partials in step order)
-// and the harmonic terms: the hill bias acts only on distance/angle/dihedral
-// CVs. Part 0 also computes those CVs and their Jacobians, sums the hill
-// partials in item order (fixed tree), evaluates the harmonic terms and the hill
-// bias, writes CVs and energies and scatters the distance/angle/dihedral rows.
+// CTA (walker w, part p) after the runs:
+//   - loads whose addresses are known at plan time go first: the part's share of
+//     the walker's coordination rows (fixed-point sums, cleared after use) and
+//     their atoms, then the walker record;
+//   - CN = the walker's run-piece partials in step order; dU/dCN from the
+//     harmonic terms (the hill bias acts only on distance/angle/dihedral CVs);
+//     the part's coordination rows are scattered (gradient rounded to float as
+//     in the per-context Jacobian table);
+//   - part 0 also completes the walker: distance/angle/dihedral CVs, the hill
+//     partials of the runs CTAs summed in CTA order (lane-strided, fixed xor
+//     tree), harmonic terms and hill bias, CVs and energies, and the
+//     distance/angle/dihedral rows.
 // Copies n bytes (multiple of 4) from global to shared memory, all threads.
 __device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
     const int* s = static_cast<const int*>(src);
@@ -215,82 +346,96 @@ __device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
 
 constexpr int MAXCOORD = 8;   // coordination CVs per walker
 
-__global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
-    __shared__ double sCV[MAXCV], sdU[MAXCV];
-    __shared__ F3 sJac[MAXSIMPLE * 4];
-    __shared__ double red[32 * 3];
+struct FinSmem {
+    double sCV[MAXCV], sdU[MAXCV];
+    F3 sJac[MAXSIMPLE * 4];
+    double sHill[3];
     // the walker's record: one round of independent loads
-    __shared__ BWalker sW;
-    __shared__ BSimple sSimple[MAXSIMPLE];
-    __shared__ BHarm sHarm[MAXHARM];
-    __shared__ CoordItem sItem[MAXCOORD];
-    const int w = blockIdx.x / B.parts, part = blockIdx.x % B.parts;
+    BWalker sW;
+    BSimple sSimple[MAXSIMPLE];
+    BHarm sHarm[MAXHARM];
+    CoordItem sItem[MAXCOORD];
+};
+
+__device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
+    double* sCV = fs.sCV;
+    double* sdU = fs.sdU;
+    F3* sJac = fs.sJac;
+    BWalker& sW = fs.sW;
+    BSimple* sSimple = fs.sSimple;
+    BHarm* sHarm = fs.sHarm;
+    CoordItem* sItem = fs.sItem;
+    const int w = fi / B.parts, part = fi % B.parts;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned long long* st = B.fstamps ? B.fstamps + 6 * (size_t)blockIdx.x : nullptr;
+    const BHill& hb = B.hill;
+    unsigned long long* st = B.fstamps ? B.fstamps + 6 * (size_t)fi : nullptr;
     if (st && tid == 0) st[0] = globalTimer();
+    const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
+    const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
+    long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
+    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD];
+    const size_t rowBase = (size_t)w * B.rowsPerWalker;
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        const int r = r0 + tid + FT * q;
+        rItem[q] = -1; rAtom[q] = 0;
+        vx[q] = vy[q] = vz[q] = 0;
+        if (r < r1) {
+            const unsigned long long* a = B.R.acc + 3 * (rowBase + r);
+            vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
+            rAtom[q] = __ldg(B.rowAtom + rowBase + r);
+            rItem[q] = 0;
+        }
+    }
+    // part 0: the hill partials of the runs CTAs (warp 2, CTA order per lane)
+    double hv0 = 0.0, hv1 = 0.0, hv2 = 0.0;
+    if (part == 0 && hb.present && warp == 2)
+        for (int c = lane; c < B.hillParts; c += 32) {
+            const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
+            hv0 += __ldcg(q); hv1 += __ldcg(q + 1); hv2 += __ldcg(q + 2);
+        }
     copyWords(&sW, B.walkers + w, sizeof(BWalker));
     copyWords(sSimple, B.simple + (size_t)w * B.nS, sizeof(BSimple) * B.nS);
     copyWords(sHarm, B.harm + (size_t)w * B.nH, sizeof(BHarm) * B.nH);
     copyWords(sItem, B.items + (size_t)w * B.nC, sizeof(CoordItem) * B.nC);
     if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
+    if (part == 0 && warp == 2) {
+        hv0 = warpSum(hv0); hv1 = warpSum(hv1); hv2 = warpSum(hv2);
+        if (lane == 0) { fs.sHill[0] = hv0; fs.sHill[1] = hv1; fs.sHill[2] = hv2; }
+    }
     __syncthreads();
     if (st && tid == 0) st[1] = globalTimer();
-    // part 0: distance/angle/dihedral values and Jacobians (positions: one round)
-    if (part == 0 && tid < B.nS) {
+    // part 0: distance/angle/dihedral CVs (warp 1)
+    if (part == 0 && warp == 1 && lane < B.nS) {
         F3 jac[4];
-        const float v = simpleCV(sSimple[tid].type, sSimple[tid].atoms, sW.posq, nullptr, sW.box, jac);
-        for (int k = 0; k < 4; k++) sJac[tid * 4 + k] = jac[k];
-        sCV[sSimple[tid].cv] = (double)v;
+        const float v = simpleCV(sSimple[lane].type, sSimple[lane].atoms, sW.posq, nullptr, sW.box, jac);
+        for (int k = 0; k < 4; k++) sJac[lane * 4 + k] = jac[k];
+        sCV[sSimple[lane].cv] = (double)v;
     }
-    // the rows of this part: fixed-point sums (cleared as read) and their atoms
-    const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
-    const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
-    // (all loads first, so that they are in flight together; the rows are
-    // cleared at the end of the kernel)
-    long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
-    int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD], rRow[ROWS_PER_THREAD];
+    // the item of every row (item 0's A and B rows, then item 1's, ...)
 #pragma unroll
     for (int q = 0; q < ROWS_PER_THREAD; q++) {
+        if (rItem[q] < 0) continue;
         const int r = r0 + tid + FT * q;
-        rItem[q] = -1; rAtom[q] = 0; rRow[q] = 0;
-        vx[q] = vy[q] = vz[q] = 0;
-        if (r < r1) {
-            // the walker's rows: item 0's A and B rows, then item 1's, ...
-            int c = 0, base = 0;
-            while (c < B.nC - 1 && r >= base + sItem[c].nA + sItem[c].nB) {
-                base += sItem[c].nA + sItem[c].nB;
-                c++;
-            }
-            const CoordItem& it = sItem[c];
-            const int i = r - base;
-            rRow[q] = it.row0 + i;
-            const unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
-            vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
-            rItem[q] = c;
-            rAtom[q] = __ldg(B.R.slots + (i < it.nA ? it.a0 + i : it.b0 + (i - it.nA)));
+        int c = 0, base = 0;
+        while (c < B.nC - 1 && r >= base + sItem[c].nA + sItem[c].nB) {
+            base += sItem[c].nA + sItem[c].nB;
+            c++;
         }
+        rItem[q] = c;
     }
-    // CN: warp c sums item c's piece partials (lane l: pieces l, l + 32, ..., step
-    // order), fixed xor tree
-    if (warp < B.nC) {
+    // CN: warps 2..7 take items warp - 2, warp + 4, ...; lane l sums pieces l,
+    // l + 32, ... (step order), fixed xor tree
+    for (int c = warp - 2; c >= 0 && c < B.nC; c += FT / 32 - 2) {
+        const CoordItem& it = sItem[c];
         double t = 0.0;
-        for (int k = sItem[warp].pieceBegin + lane; k < sItem[warp].pieceEnd; k += 32) t += __ldcg(B.R.cnPiece + k);
+        for (int k = it.pieceBegin + lane; k < it.pieceEnd; k += 32) t += __ldcg(B.R.cnPiece + k);
         t = warpSum(t);
-        if (lane == 0) sCV[sItem[warp].cv] = t;
+        if (lane == 0) sCV[it.cv] = t;
     }
-    if (st) { __syncthreads(); if (tid == 0) st[2] = globalTimer(); }
-    double hv[3] = {0.0, 0.0, 0.0};
-    if (part == 0 && B.hill.present) {
-        const int items = (*B.hill.count + B.hc - 1) / B.hc;
-        for (int c = tid; c < items; c += FT) {
-            const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
-            hv[0] += __ldcg(q); hv[1] += __ldcg(q + 1); hv[2] += __ldcg(q + 2);
-        }
-    }
-    if (part == 0) blockSum<3>(hv, red);   // part-uniform: every thread of part 0 takes part
-    else __syncthreads();
-    if (st && tid == 0) st[3] = globalTimer();
-    // dU/dCV: part 0 everything, the other parts the coordination CVs only
+    __syncthreads();
+    if (st && tid == 0) st[2] = globalTimer();
+    // dU/dCN (coordination CVs); part 0: all CVs, energies
     if (tid == 0) {
         double E = 0.0;
         for (int k = 0; k < B.nH; k++) {
@@ -300,18 +445,18 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
             if (part == 0 || coordCv) sdU[hm.cv] += harmonicDU(hm, sCV[hm.cv], E);
         }
         if (part == 0) {
-            if (B.hill.present) {
-                E += hv[0];
-                sdU[B.hill.cv[0]] += hv[1];
-                if (B.hill.D > 1) sdU[B.hill.cv[1]] += hv[2];
+            if (hb.present) {
+                E += fs.sHill[0];
+                sdU[hb.cv[0]] += fs.sHill[1];
+                if (hb.D > 1) sdU[hb.cv[1]] += fs.sHill[2];
             }
             for (int k = 0; k < B.nCV; k++) B.cvv[(size_t)w * B.nCV + k] = sCV[k];
             B.energy[w] = E;
-            B.hillEnergy[w] = B.hill.present ? hv[0] : 0.0;
+            B.hillEnergy[w] = hb.present ? fs.sHill[0] : 0.0;
         }
     }
     __syncthreads();
-    if (st && tid == 0) st[4] = globalTimer();
+    if (st && tid == 0) st[3] = globalTimer();
     unsigned long long* F = sW.force;
     const int P = sW.padded;
 #pragma unroll
@@ -319,11 +464,14 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
         if (rItem[q] < 0) continue;
         const CoordItem& it = sItem[rItem[q]];
         const double g = sdU[it.cv];
+        unsigned long long* a = B.R.acc + 3 * (rowBase + r0 + tid + FT * q);
+        a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
         if (g == 0.0) continue;
         const double sc = coordAccScale(it) * crun::IFXD;
         scatterRow(F, P, rAtom[q], g, (float)((double)vx[q] * sc), (float)((double)vy[q] * sc),
                    (float)((double)vz[q] * sc));
     }
+    if (st && tid == 0) st[4] = globalTimer();
     if (part == 0 && tid < B.nS * 4) {
         const BSimple& si = sSimple[tid / 4];
         const int k = tid % 4;
@@ -334,14 +482,59 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
             scatterRow(F, P, si.atoms[k], g, j.x, j.y, j.z);
         }
     }
-    // clear the rows for the next step's runs
-#pragma unroll
-    for (int q = 0; q < ROWS_PER_THREAD; q++) {
-        if (rItem[q] < 0) continue;
-        unsigned long long* a = B.R.acc + 3 * (size_t)rRow[q];
-        a[0] = 0ull; a[1] = 0ull; a[2] = 0ull;
-    }
     if (st) { __syncthreads(); if (tid == 0) st[5] = globalTimer(); }
+}
+
+__global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
+    __shared__ FinSmem fs;
+    finalizeItem(B, blockIdx.x, fs);
+}
+
+// ------------------------------------------------------------- fused step
+// One cooperative launch (all CTAs co-resident): the runs, a grid-wide barrier,
+// then the finalize items b, b + grid, ... The barrier's wait is bounded: after
+// `limit` polls the CTA sets bit 0 of the status word and leaves without its
+// finalize items (the host reports the status as an error).
+__device__ bool gridBarrier(unsigned* bar, int* status, unsigned long long limit) {
+    __shared__ int sOk;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long it = 0;
+            while (*vgen == gen) {
+                __nanosleep(64);
+                if (++it > limit) { atomicOr(status, 1); ok = 0; break; }
+            }
+        }
+        __threadfence();
+        sOk = ok;
+    }
+    __syncthreads();
+    return sOk != 0;
+}
+
+template <int RA, int BOX, int NH, bool HI>
+__global__ void __launch_bounds__(256, 2) k_batch_fused(BatchDev B) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ CoordRunSmem<RA> sm;
+    __shared__ FinSmem fs;
+    runsBody<RA, BOX, NH, HI>(B, sm, *reinterpret_cast<HillStage*>(dsm));
+    if (!gridBarrier(B.bar, B.status, B.spinLimit)) return;
+    const int nFin = B.W * B.parts;
+    for (int fi = blockIdx.x; fi < nFin; fi += gridDim.x) {
+        finalizeItem(B, fi, fs);
+        __syncthreads();
+    }
 }
 
 typedef void (*RunsFn)(BatchDev);
@@ -355,6 +548,17 @@ RunsFn runsKernelB(int box, bool hi) {
 
 RunsFn runsKernel(int box, int kind, bool hi) {
     return kind == 3 ? runsKernelB<3>(box, hi) : kind == -1 ? runsKernelB<-1>(box, true) : runsKernelB<0>(box, true);
+}
+
+template <int NH>
+RunsFn fusedKernelB(int box, bool hi) {
+    if (box == 0) return k_batch_fused<8, 0, NH, true>;
+    if (box == 1) return hi ? k_batch_fused<8, 1, NH, true> : k_batch_fused<8, 1, NH, false>;
+    return hi ? k_batch_fused<8, 2, NH, true> : k_batch_fused<8, 2, NH, false>;
+}
+
+RunsFn fusedKernel(int box, int kind, bool hi) {
+    return kind == 3 ? fusedKernelB<3>(box, hi) : kind == -1 ? fusedKernelB<-1>(box, true) : fusedKernelB<0>(box, true);
 }
 
 __global__ void k_batch_deposit(BatchDev B) {
@@ -372,7 +576,7 @@ __global__ void k_batch_deposit(BatchDev B) {
         for (int d = 0; d < hb.D; d++) c[d] = B.cvv[(size_t)w * B.nCV + hb.cv[d]];
         for (int d = 0; d < hb.D; d++) hb.centers[(size_t)k * hb.D + d] = c[d];
         hb.heights[k] = h;
-        hb.mirror[k] = make_float4((float)c[0], (float)c[1], (float)h, 0.0f);
+        hb.mirror[k] = make_float4((float)(c[0] * hb.u[0]), (float)(c[1] * hb.u[1]), (float)h, 0.0f);
     }
     __syncthreads();
     if (threadIdx.x == 0) *hb.count = min(hb.maxH, n0 + B.W);
@@ -386,7 +590,9 @@ struct Batch::Impl {
     std::vector<int> coordAtoms;
     std::vector<CoordStep> steps;
     DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, sysPosqD, acc, cnPiece;
-    DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
+    DBuf hillCvPosD, hillCvTypeD, rowAtomD;
+    std::vector<BSimple> simpleH;
+    DBuf hillPart, cvv, energy, hillEnergy, status, bar, scratchForce;
     DBuf hMirror, hCenters, hHeights, hCount;
     BHill hill{};
     BatchTuning tune;
@@ -394,15 +600,13 @@ struct Batch::Impl {
     int grid = 0;        // coordination runs: SMs x resident CTAs
     int rows = 0;        // coordination rows of one walker
     int parts = 1;       // finalize CTAs per walker
-    int nWB = 1;         // walker blocks of the hill items
-    int hillCountHost = 0;   // host mirror of the hill count (set_hills + deposits)
-    int balancedItems = -1;  // hill items the current ranges were balanced for
     bool hi = true;
     cudaStream_t stream = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t graph = nullptr;
     long long launches = 0;
     int lastUpdateStep = -1;
+    std::vector<unsigned long long> lastStamps;   // raw records of the last phaseTimes call
     bool ready = false;
     float lastMs = 0;
 
@@ -410,18 +614,13 @@ struct Batch::Impl {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
     }
 
-    RunsFn runs() const { return runsKernel(boxKind, kind, hi); }
-    int hcHill() const { return tune.hillChunk > 0 ? tune.hillChunk : 512; }
+    RunsFn runs() const { return tune.fused ? fusedKernel(boxKind, kind, hi) : runsKernel(boxKind, kind, hi); }
 
-    // Per-CTA step ranges: CTA b also evaluates hill items b, b + grid, ...,
-    // charged hillWeightPct percent of a step each; run pieces to match. The
+    // Per-CTA step ranges (equal step counts) and the run pieces to match. The
     // device copies are rewritten in place (a captured graph keeps their
     // addresses) unless they must grow.
     void balance() {
-        const int nItems = hill.present ? ((hillCountHost + hcHill() - 1) / hcHill()) * ((W + WBLK - 1) / WBLK) : 0;
-        std::vector<double> pre(grid, 0.0);
-        for (int h = 0; h < nItems; h++) pre[h % grid] += tune.hillWeightPct / 100.0;
-        std::vector<int> begin = balanceRanges((int)steps.size(), grid, pre);
+        std::vector<int> begin = balanceRanges((int)steps.size(), grid, {});
         const int pieces = buildCoordPieces(steps, begin, items);
         auto put = [&](DBuf& d, const void* src, size_t bytes) {
             if (d.bytes < bytes) { d.alloc(bytes); destroyGraph(); }
@@ -434,7 +633,6 @@ struct Batch::Impl {
             cnPiece.alloc(sizeof(double) * std::max(1, pieces));
             destroyGraph();
         }
-        balancedItems = nItems;
         dev.R.begin = beginD.as<int>();
         dev.R.steps = stepsD.as<CoordStep>();
         dev.R.items = itemsD.as<CoordItem>();
@@ -472,14 +670,16 @@ struct Batch::Impl {
         cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_), "attr");
         cudaCheck(cudaFuncSetAttribute((const void*)runs(), cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared), "carveout");
+        cudaCheck(cudaFuncSetAttribute((const void*)runs(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)dynSmem()), "smem");
         int perSM = 0;
-        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)runs(), 256, 0), "occupancy");
+        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)runs(), 256, dynSmem()),
+                  "occupancy");
         if (perSM < 1) throw Error(GLUED_E_CUDA, "batched runs kernel cannot be resident");
-        grid = sms * perSM;
+        grid = sms * perSM;   // every CTA resident: required by the fused (cooperative) step
         balance();
         parts = tune.parts > 0 ? std::max(minParts(), tune.parts) : minParts();
-        nWB = (W + WBLK - 1) / WBLK;
-        if (hill.present) hillPart.alloc(sizeof(double) * 3 * (size_t)W * ((hill.maxH + hcHill() - 1) / hcHill()));
+        hillPart.alloc(sizeof(double) * 3 * (size_t)W * grid);
         dev.walkers = walkersD.as<BWalker>();
         dev.W = W; dev.nCV = nCV; dev.nS = nS; dev.nC = nC; dev.nH = nH;
         dev.simple = simpleD.as<BSimple>();
@@ -497,27 +697,67 @@ struct Batch::Impl {
         dev.parts = parts;
         dev.hill = hill;
         dev.hillPart = hillPart.as<double>();
-        dev.nWB = nWB;
-        dev.hc = hcHill();
+        dev.hillParts = grid;
         dev.cvv = cvv.as<double>(); dev.energy = energy.as<double>(); dev.hillEnergy = hillEnergy.as<double>();
+        // plan-time address tables: hill-CV atoms per walker and dimension, atom per row
+        std::vector<const float4*> hcp((size_t)W * 8, nullptr);
+        std::vector<int> hct((size_t)W * 2, 0);
+        for (int w = 0; w < W && hill.present; w++)
+            for (int d = 0; d < hill.D; d++)
+                for (int k = 0; k < nS; k++) {
+                    const BSimple& si = simpleH[(size_t)w * nS + k];
+                    if (si.cv != hill.cv[d]) continue;
+                    const int na = si.type == 1 ? 2 : si.type == 2 ? 3 : 4;
+                    hct[w * 2 + d] = si.type;
+                    for (int a = 0; a < na; a++) hcp[(size_t)w * 8 + d * 4 + a] = walkersH[w].posq + si.atoms[a];
+                }
+        hillCvPosD.upload(hcp);
+        hillCvTypeD.upload(hct);
+        std::vector<int> ra((size_t)std::max(1, W * rows), 0);
+        for (int w = 0; w < W; w++) {
+            int r = 0;
+            for (int c = 0; c < nC; c++) {
+                const CoordItem& it = items[(size_t)w * nC + c];
+                for (int i = 0; i < it.nA; i++) ra[(size_t)w * rows + r++] = coordAtoms[it.a0 + i];
+                for (int i = 0; i < it.nB; i++) ra[(size_t)w * rows + r++] = coordAtoms[it.b0 + i];
+            }
+        }
+        rowAtomD.upload(ra);
+        dev.hillCvPos = hillCvPosD.as<const float4*>();
+        dev.hillCvType = hillCvTypeD.as<int>();
+        dev.rowAtom = rowAtomD.as<int>();
+        if (!bar.p) bar.alloc(sizeof(unsigned) * 4);
+        cudaCheck(cudaMemset(bar.p, 0, bar.bytes), "reset");
+        dev.bar = bar.as<unsigned>();
+        dev.status = status.as<int>();
+        dev.spinLimit = 1ull << 22;
         destroyGraph();
     }
 
+    // dynamic shared memory of the runs kernel: the hill staging area
+    size_t dynSmem() const { return hill.present ? sizeof(HillStage) : 0; }
+
     void launchRuns(cudaStream_t s) {
         void* args[] = {&dev};
-        cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(256), args, 0, s), "runs");
+        const size_t dyn = dynSmem();
+        if (tune.fused)
+            cudaCheck(cudaLaunchCooperativeKernel((const void*)runs(), dim3(grid), dim3(256), args, dyn, s), "fused step");
+        else
+            cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(256), args, dyn, s), "runs");
     }
     void launchFinalize(cudaStream_t s) {
+        if (tune.fused) return;
         void* args[] = {&dev};
         cudaCheck(cudaLaunchKernel((const void*)k_batch_finalize, dim3(W * parts), dim3(FT), args, 0, s), "finalize");
     }
-    // The step's launches on stream s: coordination runs, then the finalize.
+    // The step's launches on stream s: coordination runs, then the finalize
+    // (or the fused cooperative step).
     void launch(cudaStream_t s) {
         launchRuns(s);
         launchFinalize(s);
         cudaCheck(cudaGetLastError(), "step launch");
     }
-    int launchesPerStep() const { return 2; }
+    int launchesPerStep() const { return tune.fused ? 1 : 2; }
 };
 
 Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_desc* walkers) : impl_(new Impl()) {
@@ -654,15 +894,19 @@ Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_de
         h.hif = gamma <= 1.0 ? 0.0 : 1.0 / ((gamma - 1.0) * kT);
         h.pace = bs.iparams[0];
         h.maxH = bs.iparams[1];
+        const double LOG2E = 1.4426950408889634;
+        h.cut = (float)(8.0 * LOG2E);
         for (int d = 0; d < 2; d++) {
             h.cv[d] = d < D ? bs.cvs[d] : 0;
-            double sg = d < D ? bs.params[1 + d] : 1.0;
-            h.a[d] = d < D ? (float)(1.0 / (2.0 * sg * sg)) : 0.0f;
-            h.isig2[d] = d < D ? (float)(1.0 / (sg * sg)) : 0.0f;
-            int per = d < D ? bs.iparams[2 + d] : 0;
-            double L = d < D ? bs.params[3 + 2 * D + d] - bs.params[3 + D + d] : 0.0;
-            h.period[d] = per ? (float)L : 0.0f;
-            h.iperiod[d] = per ? (float)(1.0 / L) : 0.0f;
+            const double sg = d < D ? bs.params[1 + d] : 1.0;
+            if (d < D && !(sg > 0.0)) throw Error(GLUED_E_INVALID, "batch: METAD_HILLS sigma must be > 0");
+            const double u = d < D ? std::sqrt(LOG2E / (2.0 * sg * sg)) : 0.0;
+            h.u[d] = (float)u;
+            h.gsc[d] = d < D ? (float)(-1.0 / (sg * sg * u)) : 0.0f;
+            const int per = d < D ? bs.iparams[2 + d] : 0;
+            const double L = d < D ? bs.params[3 + 2 * D + d] - bs.params[3 + D + d] : 0.0;
+            h.pS[d] = per ? (float)(L * u) : 0.0f;
+            h.ipS[d] = per ? (float)(1.0 / (L * u)) : 0.0f;
         }
         if (h.maxH < 1) throw Error(GLUED_E_INVALID, "batch: METAD_HILLS maxHills must be >= 1");
         I.hMirror.alloc(sizeof(float4) * (size_t)h.maxH);
@@ -674,6 +918,7 @@ Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_de
     }
     I.walkersD.upload(I.walkersH);
     I.simpleD.upload(simple);
+    I.simpleH = simple;
     I.harmD.upload(harm);
     I.atomsD.upload(I.coordAtoms);
     I.cvv.alloc(sizeof(double) * (size_t)I.W * std::max(I.nCV, 1));
@@ -699,10 +944,7 @@ void Batch::setStream(cudaStream_t s) {
 void Batch::setTuning(const BatchTuning& t) {
     if (t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 8");
     if (t.parts < 0 || t.parts > 4096) throw Error(GLUED_E_INVALID, "batch tuning: finalize parts must be 0..4096");
-    if (t.hillWeightPct < 0 || t.hillWeightPct > 10000)
-        throw Error(GLUED_E_INVALID, "batch tuning: hill weight must be 0..10000 percent of a step");
-    if (t.hillChunk != 0 && (t.hillChunk < 128 || t.hillChunk > HC_MAX || t.hillChunk % 128))
-        throw Error(GLUED_E_INVALID, "batch tuning: hill chunk must be 0 or a multiple of 128 up to 1024");
+    if (t.fused != 0 && t.fused != 1) throw Error(GLUED_E_INVALID, "batch tuning: fused must be 0 or 1");
     cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
     impl_->tune = t;
     impl_->plan();
@@ -715,26 +957,35 @@ void Batch::execute() {
     if (!I.graph) {
         cudaGraph_t g = nullptr;
         cudaCheck(cudaStreamBeginCapture(I.cap, cudaStreamCaptureModeThreadLocal), "capture begin");
+        bool launched = true;
         try {
             I.launch(I.cap);
-        } catch (...) {
-            cudaStreamEndCapture(I.cap, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
+        } catch (const Error&) {
+            launched = false;
         }
-        cudaCheck(cudaStreamEndCapture(I.cap, &g), "capture end");
-        cudaError_t ie = cudaGraphInstantiate(&I.graph, g, 0);
-        cudaGraphDestroy(g);
-        cudaCheck(ie, "graph instantiate");
+        cudaError_t ce = cudaStreamEndCapture(I.cap, &g);
+        cudaError_t ie = cudaErrorUnknown;
+        if (launched && ce == cudaSuccess && g) ie = cudaGraphInstantiate(&I.graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (!launched || ce != cudaSuccess || ie != cudaSuccess) {
+            cudaGetLastError();
+            I.graph = nullptr;
+            if (!I.tune.fused) throw Error(GLUED_E_CUDA, "batch: step graph capture failed");
+            // the cooperative launch could not be captured: use the two-launch step
+            I.tune.fused = 0;
+            I.plan();
+            execute();
+            return;
+        }
     }
     cudaCheck(cudaGraphLaunch(I.graph, I.stream), "graph launch");
     I.launches += I.launchesPerStep();
     I.ready = true;
 }
 
-// Autotuner: finalize CTAs per walker and the weight of a hill item in the range
-// balance are timed on the live walkers with CUDA events (forces go to a scratch
-// buffer) and the fastest combination is kept.
+// Autotuner: the step variant (two launches or one cooperative launch) and the
+// finalize CTAs per walker are timed on the live walkers with CUDA events
+// (forces go to a scratch buffer) and the fastest combination is kept.
 BatchTuning Batch::autotune() {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
@@ -751,26 +1002,24 @@ BatchTuning Batch::autotune() {
     float bestMs = 1e30f;
     const BatchTuning saved = I.tune;
     const int base = I.minParts();
-    for (int hc : {256, 512, 1024})
-        for (int pct : {100, 150, 200, 300})
-            for (int mul : {1, 2}) {
-                if (!I.hill.present && (hc != 512 || pct != 150)) continue;
-                BatchTuning t;
-                t.ra = 8; t.parts = base * mul; t.hillWeightPct = pct; t.hillChunk = hc;
-                I.tune = t;
-                I.plan();
-                for (int r = 0; r < 2; r++) I.launch(I.stream);
-                cudaCheck(cudaEventRecord(a, I.stream), "event");
-                const int reps = 8;
-                for (int r = 0; r < reps; r++) I.launch(I.stream);
-                cudaCheck(cudaEventRecord(b, I.stream), "event");
-                cudaCheck(cudaEventSynchronize(b), "event");
-                float ms = 0;
-                cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
-                ms /= reps;
-                I.launches += (long long)(reps + 2) * I.launchesPerStep();
-                if (ms < bestMs) { bestMs = ms; best = t; }
-            }
+    for (int fused : {0, 1})
+        for (int mul : {1, 2, 4}) {
+            BatchTuning t;
+            t.ra = 8; t.parts = base * mul; t.fused = fused;
+            I.tune = t;
+            I.plan();
+            for (int r = 0; r < 2; r++) I.launch(I.stream);
+            cudaCheck(cudaEventRecord(a, I.stream), "event");
+            const int reps = 8;
+            for (int r = 0; r < reps; r++) I.launch(I.stream);
+            cudaCheck(cudaEventRecord(b, I.stream), "event");
+            cudaCheck(cudaEventSynchronize(b), "event");
+            float ms = 0;
+            cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
+            ms /= reps;
+            I.launches += (long long)(reps + 2) * I.launchesPerStep();
+            if (ms < bestMs) { bestMs = ms; best = t; }
+        }
     (void)saved;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -783,11 +1032,6 @@ BatchTuning Batch::autotune() {
     return best;
 }
 
-// One regular step launched without the graph, with every CTA recording
-// %globaltimer at entry, end of phase A, barrier exit and exit, and how many
-// coordination / hill items it processed. out[0..7]: phase-A end (earliest,
-// latest CTA), barrier exit (latest), exit (latest) in microseconds after the
-// earliest entry; coordination items, hill items, most and fewest items per CTA.
 // Percentile p (0..100) of v (sorted in place).
 static double pct(std::vector<double>& v, double p) {
     if (v.empty()) return 0.0;
@@ -796,14 +1040,19 @@ static double pct(std::vector<double>& v, double p) {
     return v[i];
 }
 
+// One regular step launched without the graph, each launch between CUDA events
+// and every CTA recording %globaltimer at its phase boundaries (runs: entry,
+// staging issued, coordination done, hill slice done; finalize: six stamps);
+// the layout of out[21] is given with glued_batch_phase_times.
 void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
+    constexpr int RS = 7, FS = 6;   // stamps per runs / finalize CTA
     const int fg = I.W * I.parts;
     DBuf st;
-    st.alloc(sizeof(unsigned long long) * (4 * (size_t)I.grid + 6 * (size_t)fg));
+    st.alloc(sizeof(unsigned long long) * (RS * (size_t)I.grid + FS * (size_t)fg));
     cudaCheck(cudaMemsetAsync(st.p, 0, st.bytes, I.stream), "stamps");
     I.dev.stamps = st.as<unsigned long long>();
-    I.dev.fstamps = st.as<unsigned long long>() + 4 * (size_t)I.grid;
+    I.dev.fstamps = st.as<unsigned long long>() + RS * (size_t)I.grid;
     cudaEvent_t e[3];
     for (auto& x : e) cudaCheck(cudaEventCreate(&x), "event");
     cudaCheck(cudaEventRecord(e[0], I.stream), "event");
@@ -822,29 +1071,52 @@ void Batch::phaseTimes(double* out) {
     I.ready = true;
     std::vector<unsigned long long> h(st.bytes / sizeof(unsigned long long));
     cudaCheck(cudaMemcpy(h.data(), st.p, st.bytes, cudaMemcpyDeviceToHost), "stamps");
+    // raw records: runs CTA {SM, steps, 6 times}, finalize CTA {6 times}
+    {
+        std::vector<int> begin = balanceRanges((int)I.steps.size(), I.grid, {});
+        I.lastStamps.clear();
+        for (int g = 0; g < I.grid; g++) {
+            const unsigned long long* r = h.data() + RS * (size_t)g;
+            I.lastStamps.push_back(r[6]);
+            I.lastStamps.push_back((unsigned long long)(begin[g + 1] - begin[g]));
+            for (int k = 0; k < 6; k++) I.lastStamps.push_back(r[k]);
+        }
+        for (int g = 0; g < fg; g++)
+            for (int k = 0; k < FS; k++) I.lastStamps.push_back(h[RS * (size_t)I.grid + FS * (size_t)g + k]);
+    }
     unsigned long long t0 = ~0ull, f0 = ~0ull;
-    for (int g = 0; g < I.grid; g++) t0 = std::min(t0, h[4 * (size_t)g]);
-    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[4 * (size_t)I.grid + 6 * (size_t)g]);
-    std::vector<double> cvs, coord, end, fdur, fend, fph[5];
+    for (int g = 0; g < I.grid; g++) t0 = std::min(t0, h[RS * (size_t)g]);
+    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[RS * (size_t)I.grid + FS * (size_t)g]);
+    std::vector<double> stage, coord, end, hw, he, hr, fdur, fend, fph[5];
     for (int g = 0; g < I.grid; g++) {
-        const unsigned long long* r = h.data() + 4 * (size_t)g;
-        cvs.push_back((r[1] - r[0]) * 1e-3);
+        const unsigned long long* r = h.data() + RS * (size_t)g;
+        stage.push_back((r[1] - r[0]) * 1e-3);
         coord.push_back((r[2] - t0) * 1e-3);
-        end.push_back((r[3] - t0) * 1e-3);
+        hw.push_back((r[3] - r[2]) * 1e-3);
+        he.push_back((r[4] - r[3]) * 1e-3);
+        hr.push_back((r[5] - r[4]) * 1e-3);
+        end.push_back((r[5] - t0) * 1e-3);
     }
     for (int g = 0; g < fg; g++) {
-        const unsigned long long* r = h.data() + 4 * (size_t)I.grid + 6 * (size_t)g;
+        const unsigned long long* r = h.data() + RS * (size_t)I.grid + FS * (size_t)g;
         fdur.push_back((r[5] - r[0]) * 1e-3);
         fend.push_back((r[5] - f0) * 1e-3);
         for (int k = 0; k < 5; k++) fph[k].push_back((r[k + 1] - r[k]) * 1e-3);
     }
     out[0] = a * 1e3; out[1] = b * 1e3;
-    out[2] = pct(cvs, 50); out[3] = pct(cvs, 100);
+    out[2] = pct(stage, 50); out[3] = pct(stage, 100);
     out[4] = pct(coord, 0); out[5] = pct(coord, 50); out[6] = pct(coord, 100);
     out[7] = pct(end, 50); out[8] = pct(end, 100);
     out[9] = pct(fdur, 50); out[10] = pct(fdur, 100); out[11] = pct(fend, 100);
-    for (int k = 0; k < 5; k++) out[16 + k] = pct(fph[k], 50);
     out[12] = (double)I.steps.size(); out[13] = (double)I.grid; out[14] = (double)I.parts; out[15] = (double)fg;
+    for (int k = 0; k < 5; k++) out[16 + k] = pct(fph[k], 50);
+    out[21] = pct(hw, 50); out[22] = pct(he, 50); out[23] = pct(hr, 50);
+}
+
+long long Batch::phaseStamps(unsigned long long* out, long long cap) {
+    const std::vector<unsigned long long>& v = impl_->lastStamps;
+    if (out) std::copy(v.begin(), v.begin() + std::min<long long>(cap, (long long)v.size()), out);
+    return (long long)v.size();
 }
 
 void Batch::updateState(int step) {
@@ -856,9 +1128,6 @@ void Batch::updateState(int step) {
     k_batch_deposit<<<1, 256, 0, I.stream>>>(I.dev);
     cudaCheck(cudaGetLastError(), "deposit");
     I.launches++;
-    I.hillCountHost = std::min(I.hill.maxH, I.hillCountHost + I.W);
-    const int nItems = ((I.hillCountHost + I.hcHill() - 1) / I.hcHill()) * ((I.W + WBLK - 1) / WBLK);
-    if (nItems != I.balancedItems) I.balance();
 }
 
 void Batch::energies(double* out) {
@@ -890,15 +1159,14 @@ void Batch::setHills(const double* centers, const double* heights, int n) {
     const int D = I.hill.D;
     std::vector<float4> m(n);
     for (int k = 0; k < n; k++)
-        m[k] = make_float4((float)centers[k * D], D > 1 ? (float)centers[k * D + 1] : 0.0f, (float)heights[k], 0.0f);
+        m[k] = make_float4((float)(centers[k * D] * I.hill.u[0]), D > 1 ? (float)(centers[k * D + 1] * I.hill.u[1]) : 0.0f,
+                           (float)heights[k], 0.0f);
     if (n > 0) {
         cudaCheck(cudaMemcpy(I.hill.centers, centers, sizeof(double) * (size_t)n * D, cudaMemcpyHostToDevice), "hills");
         cudaCheck(cudaMemcpy(I.hill.heights, heights, sizeof(double) * n, cudaMemcpyHostToDevice), "hills");
         cudaCheck(cudaMemcpy(I.hill.mirror, m.data(), sizeof(float4) * n, cudaMemcpyHostToDevice), "hills");
     }
     cudaCheck(cudaMemcpy(I.hill.count, &n, sizeof(int), cudaMemcpyHostToDevice), "hills");
-    I.hillCountHost = n;
-    I.balance();
 }
 
 void Batch::getHills(double* centers, double* heights, int n) {

@@ -11,10 +11,10 @@
 namespace glued {
 
 struct BatchTuning {
-    int ra = 8;               // A atoms per thread in the coordination tile (TA = 8 * ra)
-    int parts = 0;            // finalize CTAs per walker (0: the fewest that cover its rows)
-    int hillWeightPct = 150;  // cost of one hill item in the range balance, percent of a step
-    int hillChunk = 0;        // hills per hill item (multiple of 128, <= 1024; 0: 512)
+    int ra = 8;       // A atoms per thread in the coordination tile (TA = 8 * ra)
+    int parts = 0;    // finalize CTAs per walker, which also split the hill table
+                      // (0: the fewest that cover its coordination rows)
+    int fused = 0;    // 1: one cooperative launch (runs, grid barrier, finalize)
 };
 
 class Batch {
@@ -39,6 +39,7 @@ public:
     bool graphed() const;
     double lastStepMs();
     void phaseTimes(double* out);
+    long long phaseStamps(unsigned long long* out, long long cap);
 
 private:
     struct Impl;

@@ -360,7 +360,7 @@ int glued_batch_set_tuning(glued_batch* b, const int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t;
-        t.ra = tune[0]; t.parts = tune[1]; t.hillWeightPct = tune[2]; t.hillChunk = tune[3];
+        t.ra = tune[0]; t.parts = tune[1]; t.fused = tune[2];
         b->b->setTuning(t);
     });
 }
@@ -368,14 +368,14 @@ int glued_batch_get_tuning(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t = b->b->tuning();
-        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.hillWeightPct; tune[3] = t.hillChunk;
+        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.fused; tune[3] = 0;
     });
 }
 int glued_batch_autotune(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch");
         glued::BatchTuning t = b->b->autotune();
-        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.hillWeightPct; tune[3] = t.hillChunk; }
+        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.fused; tune[3] = 0; }
     });
 }
 int glued_batch_execute(glued_batch* b) {
@@ -418,6 +418,15 @@ int glued_batch_launch_count(glued_batch* b, long long* count) {
 }
 int glued_batch_phase_times(glued_batch* b, double* out) {
     return guard([&] { need(b, "batch"); need(out, "out"); b->b->phaseTimes(out); });
+}
+
+int glued_batch_phase_stamps(glued_batch* b, unsigned long long* out, long long cap, long long* n) {
+    return guard([&] {
+        need(b, "batch");
+        need(n, "n");
+        if (cap < 0) throw glued::Error(GLUED_E_INVALID, "cap must be >= 0");
+        *n = b->b->phaseStamps(cap > 0 ? out : nullptr, cap);
+    });
 }
 
 }  // extern "C"

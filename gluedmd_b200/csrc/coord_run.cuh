@@ -174,12 +174,20 @@ __device__ __host__ __forceinline__ double coordAccScale(const CoordItem& it) {
 struct NoPieceHook {
     __device__ void operator()(int, int) const {}
 };
+struct NoStartHook {
+    __device__ void operator()() const {}
+};
 
 // Runs steps [s0, s1) of R on this CTA. Hook(item, steps) is called by all
 // threads after a piece (maximal sub-run of one tile) has been fully
-// accumulated; a hook that publishes completion must fence first.
-template <int RA, int BOX, int NH, bool HI, class Hook>
-__device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook) {
+// accumulated; a hook that publishes completion must fence first. Start() is
+// called once by all threads when the copies issued before the call and those
+// of the first two steps have landed (after a barrier), before the first step
+// computes: cp.async copies it issues land while that step computes and are
+// complete after its end-of-step wait.
+template <int RA, int BOX, int NH, bool HI, class Hook, class Start = NoStartHook>
+__device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook,
+                         const Start& start = Start()) {
     using namespace crun;
     constexpr int TA = NW * RA;
     const int tid = threadIdx.x, lane = tid & 31, ty = tid >> 5;
@@ -223,6 +231,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
         if (nw > 1) issue(1, ib1, ia1, pq1);
         cpAsyncWaitAll();
         __syncthreads();
+        if (w0 == s0) start();
         for (int ls = 0; ls < nw; ls++) {
             const int s = w0 + ls;
             const int b = (s - s0) & 1;

@@ -11,11 +11,11 @@ namespace glued {
 
 // Periodic box, reduced triclinic form (OpenMM): a = (ax,0,0), b = (bx,by,0),
 // c = (cx,cy,cz). kind 0: no PBC; 1: rectangular; 2: triclinic.
-struct BoxDev {
+struct __align__(16) BoxDev {
     float inv[3];
     float a[3], b[3], c[3];
     int kind;
-    int pad[2];
+    int pad[3];
 };
 
 // Jacobian table rows (the reference's SoA, CommonGluedKernels.h:95-100).

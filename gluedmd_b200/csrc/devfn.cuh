@@ -60,6 +60,25 @@ __device__ __forceinline__ float warpSumF(float v) {
     return v;
 }
 
+// Sums each of 32 slots over the warp's lanes with a fixed butterfly (31
+// shuffles for all slots instead of 5 per slot): in the round with offset o a
+// lane keeps the half of its live slots selected by lane bit o and adds the
+// partner's copy of that half. Returns the sum of slot `lane`; v is clobbered.
+__device__ __forceinline__ float warpTransposeSum32(float (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < o; i++) {
+            const float send = up ? v[i] : v[i + o];
+            const float keep = up ? v[i + o] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0];
+}
+
 // Sum of NV doubles over the block, fixed reduction tree (deterministic).
 // Result valid in every thread. scratch: >= 32 * NV doubles of shared memory.
 template <int NV>
@@ -86,21 +105,21 @@ __device__ __forceinline__ void blockSum(double (&v)[NV], double* scratch) {
     __syncthreads();
 }
 
-// Distance / angle / dihedral value and Jacobian rows (jac[k] for atoms[k]), the
+// Distance / angle / dihedral value and Jacobian rows (jac[k] for atom k) from the
+// positions p[0..3] of its atoms, the
 // reference's formulas (CommonGluedKernels.cpp:177-444). jac may be null.
-__device__ __forceinline__ float simpleCV(int type, const int* atoms, const float4* __restrict__ posq,
-                                         const int* __restrict__ u2g, const BoxDev& box, F3* jac) {
+__device__ __forceinline__ float simpleCVFromPos(int type, const F3* p, const BoxDev& box, F3* jac) {
     if (type == 1) {  // distance
-        F3 d = minImage(sub3(loadPos(posq, u2g, atoms[1]), loadPos(posq, u2g, atoms[0])), box);
+        F3 d = minImage(sub3(p[1], p[0]), box);
         float dist = sqrtf(dot3(d, d));
         float inv = dist > 1e-10f ? 1.0f / dist : 0.0f;
         if (jac) { jac[0] = f3(-d.x * inv, -d.y * inv, -d.z * inv); jac[1] = f3(d.x * inv, d.y * inv, d.z * inv); }
         return dist;
     }
     if (type == 2) {  // angle at atoms[1]
-        F3 pb = loadPos(posq, u2g, atoms[1]);
-        F3 d1 = minImage(sub3(loadPos(posq, u2g, atoms[0]), pb), box);
-        F3 d2 = minImage(sub3(loadPos(posq, u2g, atoms[2]), pb), box);
+        F3 pb = p[1];
+        F3 d1 = minImage(sub3(p[0], pb), box);
+        F3 d2 = minImage(sub3(p[2], pb), box);
         float r1 = sqrtf(dot3(d1, d1)), r2 = sqrtf(dot3(d2, d2));
         float i1 = r1 > 1e-10f ? 1.0f / r1 : 0.0f, i2 = r2 > 1e-10f ? 1.0f / r2 : 0.0f;
         F3 n1 = f3(d1.x * i1, d1.y * i1, d1.z * i1), n2 = f3(d2.x * i2, d2.y * i2, d2.z * i2);
@@ -117,8 +136,8 @@ __device__ __forceinline__ float simpleCV(int type, const int* atoms, const floa
         return th;
     }
     // dihedral, Blondel-Karplus
-    F3 pa = loadPos(posq, u2g, atoms[0]), pb = loadPos(posq, u2g, atoms[1]);
-    F3 pc = loadPos(posq, u2g, atoms[2]), pd = loadPos(posq, u2g, atoms[3]);
+    F3 pa = p[0], pb = p[1];
+    F3 pc = p[2], pd = p[3];
     F3 b1 = minImage(sub3(pb, pa), box), b2 = minImage(sub3(pc, pb), box), b3 = minImage(sub3(pd, pc), box);
     F3 t = cross3(b1, b2), u = cross3(b2, b3);
     float d = sqrtf(dot3(b2, b2));
@@ -138,6 +157,15 @@ __device__ __forceinline__ float simpleCV(int type, const int* atoms, const floa
         jac[3] = jD;
     }
     return phi;
+}
+
+// The same from posq (atoms are user indices, mapped through u2g).
+__device__ __forceinline__ float simpleCV(int type, const int* atoms, const float4* __restrict__ posq,
+                                         const int* __restrict__ u2g, const BoxDev& box, F3* jac) {
+    const int na = type == 1 ? 2 : type == 2 ? 3 : 4;
+    F3 p[4];
+    for (int k = 0; k < 4; k++) p[k] = k < na ? loadPos(posq, u2g, atoms[k]) : f3(0.f, 0.f, 0.f);
+    return simpleCVFromPos(type, p, box, jac);
 }
 
 // Rational switch (1 - x^n)/(1 - x^m) for positive integer n, m evaluated as

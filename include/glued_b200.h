@@ -229,7 +229,8 @@ int glued_coordination_noalloc(void* stream, const void* posq, const int* group_
 
 /* ----------------------------------------------------------------------- batch
  * Many walkers on one GPU evaluated by one graph per step (a persistent
- * kernel for the coordination pairs and the hill table, then a finalize kernel)
+ * kernel for the coordination pairs, then a finalize kernel that also sums the
+ * shared hill table per walker)
  * (no reference counterpart as a kernel: it replaces the reference's
  * one-Context-per-walker stepping, tests/test_multiwalker.py:156-158, and its
  * shared-bias pointer aliasing, CommonGluedKernels.cpp:5234-5262).
@@ -251,13 +252,12 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
                        glued_batch** out);
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
-/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
- * fewest that cover the walker's coordination rows), hill_weight_pct (cost the
- * balance of the coordination ranges charges per hill item, percent of a step,
- * 0..10000), hill_chunk (hills per hill item: 0 = 512, else a multiple of 128 up
- * to 1024)}. autotune times every candidate on the live walkers (forces of the
- * trial launches go to a scratch buffer), keeps the fastest and returns it in
- * tune (synchronizing).                                                        */
+/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker, which
+ * also split the hill table; 0 = the fewest that cover the walker's
+ * coordination rows), fused (1: one cooperative launch with a bounded grid
+ * barrier between the runs and the finalize; 0: two launches), 0}. autotune
+ * times every candidate on the live walkers (forces of the trial launches go to
+ * a scratch buffer), keeps the fastest and returns it in tune (synchronizing). */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);
@@ -275,21 +275,29 @@ int glued_batch_num_cvs(glued_batch* b, int* n);
 int glued_batch_num_hills(glued_batch* b, int* n);
 int glued_batch_set_hills(glued_batch* b, const double* centers, const double* heights, int n);
 int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int n);
-/* Status word of the step's device checks (0 = ok; no bounded wait remains in
- * the current kernels, so it stays 0).                                         */
+/* Status word of the step's device checks (0 = ok; bit 0: a grid-barrier wait
+ * of the fused step gave up after its bound).                                  */
 int glued_batch_status(glued_batch* b, int* status);
 int glued_batch_launch_count(glued_batch* b, long long* count);
 /* Profiling: runs one regular step (forces are accumulated as by execute), each
- * launch bracketed by CUDA events and every CTA time-stamped. out[16], times in
- * microseconds: {runs kernel, finalize kernel (events); hill-CV prologue of a
+ * launch bracketed by CUDA events and every CTA time-stamped. out[24], times in
+ * microseconds: {runs kernel, finalize kernel (events); staging prologue of a
  * runs CTA (median, max); end of a CTA's coordination steps after the first runs
- * CTA started (min, median, max); end of a runs CTA incl. its hill items (median,
- * max); finalize CTA duration (median, max); last finalize CTA end after the
- * first one started; coordination steps, runs grid, finalize CTAs per walker,
- * finalize grid; median durations of the finalize phases: walker record, rows
- * and CN, hill partials and reduction, dU/dCV, scatter}. No reference
- * counterpart.                                                                */
+ * CTA started (min, median, max); end of a runs CTA incl. its hill slice
+ * (median, max); finalize CTA duration (median, max); last finalize CTA end
+ * after the first one started; coordination steps, runs grid, finalize CTAs per
+ * walker, finalize grid; median durations of the finalize phases: loads and
+ * walker record, CN and distance/angle/dihedral CVs, dU/dCV and energies,
+ * coordination scatter, distance/angle/dihedral rows; median durations of the
+ * runs CTAs' hill phases: wait for the staged data, hill-table evaluation,
+ * lane reduction and store}. No reference counterpart.                        */
 int glued_batch_phase_times(glued_batch* b, double* out);
+/* Raw records of the last glued_batch_phase_times call: per runs CTA {SM id,
+ * coordination steps, %globaltimer at entry, staging issued, coordination done,
+ * hill data ready, hill evaluation done, exit}, then per finalize CTA six
+ * %globaltimer stamps. *n = number of values; min(cap, *n) are copied to out
+ * (out may be NULL when cap is 0). No reference counterpart.                   */
+int glued_batch_phase_stamps(glued_batch* b, unsigned long long* out, long long cap, long long* n);
 
 #ifdef __cplusplus
 }

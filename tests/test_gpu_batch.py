@@ -50,10 +50,14 @@ def _oracle(w, biases, hill):
     return s
 
 
+@pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("with_hills", [False, True])
-def test_batch_matches_fp64_oracle(with_hills):
+def test_batch_matches_fp64_oracle(with_hills, fused):
+    """Both step variants: two launches, and one cooperative launch with a grid
+    barrier between the runs and the finalize."""
     ws, hill = _walkers()
     b, walkers, specs = _setup(ws, hill, with_hills)
+    b.set_tuning(8, 0, fused)
     for wk in walkers:
         wk.force.zero_()
     b.execute()
