@@ -40,7 +40,10 @@ constexpr int MAXSIMPLE = 16;  // distance/angle/dihedral CVs per walker
 constexpr int MAXHARM = 32;    // harmonic terms per walker
 constexpr int FT = 256;        // threads of a finalize CTA
 constexpr int ROWS_PER_THREAD = 2;   // coordination rows one finalize thread scatters
-constexpr int WBLK = 64;       // walkers per hill pass (8 per warp)
+constexpr int RUNS_THREADS = COORD_NW * 32;   // threads of a runs CTA (one CTA per SM)
+constexpr int WBLK = 64;       // walkers per hill pass
+constexpr int JW = WBLK / COORD_NW;   // walker slots per warp in a hill pass
+static_assert(JW * COORD_NW == WBLK && 3 * JW <= 32, "hill walker slots");
 constexpr int HS = 256;        // hills staged in shared memory at a time
 }  // namespace
 
@@ -84,9 +87,7 @@ struct BatchDev {
     double* cvv;            // [W][nCV]
     double* energy;         // [W]
     double* hillEnergy;     // [W]
-    unsigned* bar;                // fused step: grid barrier {count, generation}
-    int* status;                  // bit 0: a grid-barrier wait gave up
-    unsigned long long spinLimit; // polls of a grid-barrier wait before it gives up
+    int* status;                  // bit 0: a deposit found the hill table full
     unsigned long long* stamps;   // profiling (nullptr = off): runs kernel [grid][7] (6 times, SM id)
     unsigned long long* fstamps;  // profiling (nullptr = off): finalize kernel [W * parts][6]
 };
@@ -193,17 +194,17 @@ __device__ void hillCVs(const BatchDev& B, int wb, HillStage& hs) {
     }
 }
 
-// Hills lane + 32 q (q < nq) of the staged chunk against the 8 walkers of this
+// Hills lane + 32 q (q < nq) of the staged chunk against the JW walkers of this
 // warp; acc[3 j + c]: sum of g, g dx, g dy for walker slot j.
 template <bool P0, bool P1>
-__device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int nq, const float (&s0)[8],
-                                         const float (&s1)[8], float (&acc)[32]) {
+__device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int nq, const float (&s0)[JW],
+                                         const float (&s1)[JW], float (&acc)[32]) {
     constexpr float R = 12582912.0f;   // 1.5 * 2^23: adding and removing it rounds to an integer
     const int lane = threadIdx.x & 31;
     for (int q = 0; q < nq; q++) {
         const float4 hk = hs.hills[lane + 32 * q];   // height 0 past the slice
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
+        for (int j = 0; j < JW; j++) {
             float dx = s0[j] - hk.x, dy = s1[j] - hk.y;
             if (P0) dx = fmaf(-(fmaf(dx, hb.ipS[0], R) - R), hb.pS[0], dx);
             if (P1) dy = fmaf(-(fmaf(dy, hb.ipS[1], R) - R), hb.pS[1], dy);
@@ -244,10 +245,10 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, unsig
         __syncthreads();
         int h0, h1;
         hillSliceRange(B, hs, h0, h1);
-        float s0[8], s1[8], acc[32];
+        float s0[JW], s1[JW], acc[32];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int wl = min(warp + 8 * j, nw - 1);
+        for (int j = 0; j < JW; j++) {
+            const int wl = min(warp + COORD_NW * j, nw - 1);
             s0[j] = hs.sS[wl * 2]; s1[j] = hs.sS[wl * 2 + 1];
         }
 #pragma unroll
@@ -270,8 +271,8 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, unsig
         if (st && wb == 0 && threadIdx.x == 0) st[4] = globalTimer();
         const float v = warpTransposeSum32(acc);   // lane 3 j + c: component c of walker slot j
         const int j = lane / 3, c = lane - 3 * j;
-        const int wl = warp + 8 * j;
-        if (lane < 24 && wl < nw)
+        const int wl = warp + COORD_NW * j;
+        if (lane < 3 * JW && wl < nw)
             B.hillPart[3 * ((size_t)blockIdx.x * B.W + w0 + wl) + c] =
                 c == 0 ? (double)v : (double)v * (c == 1 ? hb.gsc[0] : hb.gsc[1]);
     }
@@ -317,11 +318,16 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     }
 }
 
+// Dynamic shared memory: the coordination buffers, then (with a hill bias) the
+// hill staging area.
+template <int RA>
+constexpr size_t hillStageOffset() { return (sizeof(CoordRunSmem<RA>) + 255) / 256 * 256; }
+
 template <int RA, int BOX, int NH, bool HI>
-__global__ void __launch_bounds__(256, 2) k_batch_runs(BatchDev B) {
-    extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ CoordRunSmem<RA> sm;
-    runsBody<RA, BOX, NH, HI>(B, sm, *reinterpret_cast<HillStage*>(dsm));
+__global__ void __launch_bounds__(RUNS_THREADS, 1) k_batch_runs(BatchDev B) {
+    extern __shared__ __align__(256) unsigned char dsm[];
+    runsBody<RA, BOX, NH, HI>(B, *reinterpret_cast<CoordRunSmem<RA>*>(dsm),
+                              *reinterpret_cast<HillStage*>(dsm + hillStageOffset<RA>()));
 }
 
 // ------------------------------------------------------------- finalize
@@ -490,53 +496,6 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
     finalizeItem(B, blockIdx.x, fs);
 }
 
-// ------------------------------------------------------------- fused step
-// One cooperative launch (all CTAs co-resident): the runs, a grid-wide barrier,
-// then the finalize items b, b + grid, ... The barrier's wait is bounded: after
-// `limit` polls the CTA sets bit 0 of the status word and leaves without its
-// finalize items (the host reports the status as an error).
-__device__ bool gridBarrier(unsigned* bar, int* status, unsigned long long limit) {
-    __shared__ int sOk;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* vgen = bar + 1;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned long long it = 0;
-            while (*vgen == gen) {
-                __nanosleep(64);
-                if (++it > limit) { atomicOr(status, 1); ok = 0; break; }
-            }
-        }
-        __threadfence();
-        sOk = ok;
-    }
-    __syncthreads();
-    return sOk != 0;
-}
-
-template <int RA, int BOX, int NH, bool HI>
-__global__ void __launch_bounds__(256, 2) k_batch_fused(BatchDev B) {
-    extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ CoordRunSmem<RA> sm;
-    __shared__ FinSmem fs;
-    runsBody<RA, BOX, NH, HI>(B, sm, *reinterpret_cast<HillStage*>(dsm));
-    if (!gridBarrier(B.bar, B.status, B.spinLimit)) return;
-    const int nFin = B.W * B.parts;
-    for (int fi = blockIdx.x; fi < nFin; fi += gridDim.x) {
-        finalizeItem(B, fi, fs);
-        __syncthreads();
-    }
-}
-
 typedef void (*RunsFn)(BatchDev);
 
 template <int NH>
@@ -548,17 +507,6 @@ RunsFn runsKernelB(int box, bool hi) {
 
 RunsFn runsKernel(int box, int kind, bool hi) {
     return kind == 3 ? runsKernelB<3>(box, hi) : kind == -1 ? runsKernelB<-1>(box, true) : runsKernelB<0>(box, true);
-}
-
-template <int NH>
-RunsFn fusedKernelB(int box, bool hi) {
-    if (box == 0) return k_batch_fused<8, 0, NH, true>;
-    if (box == 1) return hi ? k_batch_fused<8, 1, NH, true> : k_batch_fused<8, 1, NH, false>;
-    return hi ? k_batch_fused<8, 2, NH, true> : k_batch_fused<8, 2, NH, false>;
-}
-
-RunsFn fusedKernel(int box, int kind, bool hi) {
-    return kind == 3 ? fusedKernelB<3>(box, hi) : kind == -1 ? fusedKernelB<-1>(box, true) : fusedKernelB<0>(box, true);
 }
 
 __global__ void k_batch_deposit(BatchDev B) {
@@ -579,7 +527,10 @@ __global__ void k_batch_deposit(BatchDev B) {
         hb.mirror[k] = make_float4((float)(c[0] * hb.u[0]), (float)(c[1] * hb.u[1]), (float)h, 0.0f);
     }
     __syncthreads();
-    if (threadIdx.x == 0) *hb.count = min(hb.maxH, n0 + B.W);
+    if (threadIdx.x == 0) {
+        *hb.count = min(hb.maxH, n0 + B.W);
+        if (n0 + B.W > hb.maxH) atomicOr(B.status, 1);
+    }
 }
 
 // ================================================================== host
@@ -592,7 +543,7 @@ struct Batch::Impl {
     DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, sysPosqD, acc, cnPiece;
     DBuf hillCvPosD, hillCvTypeD, rowAtomD;
     std::vector<BSimple> simpleH;
-    DBuf hillPart, cvv, energy, hillEnergy, status, bar, scratchForce;
+    DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
     DBuf hMirror, hCenters, hHeights, hCount;
     BHill hill{};
     BatchTuning tune;
@@ -614,7 +565,7 @@ struct Batch::Impl {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
     }
 
-    RunsFn runs() const { return tune.fused ? fusedKernel(boxKind, kind, hi) : runsKernel(boxKind, kind, hi); }
+    RunsFn runs() const { return runsKernel(boxKind, kind, hi); }
 
     // Per-CTA step ranges (equal step counts) and the run pieces to match. The
     // device copies are rewritten in place (a captured graph keeps their
@@ -668,15 +619,12 @@ struct Batch::Impl {
         int dev_ = 0, sms = 0;
         cudaCheck(cudaGetDevice(&dev_), "device");
         cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_), "attr");
-        cudaCheck(cudaFuncSetAttribute((const void*)runs(), cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared), "carveout");
-        cudaCheck(cudaFuncSetAttribute((const void*)runs(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)dynSmem()), "smem");
+        runKernelSetup((const void*)runs(), dynSmem());
         int perSM = 0;
-        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)runs(), 256, dynSmem()),
+        cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, (const void*)runs(), RUNS_THREADS, dynSmem()),
                   "occupancy");
         if (perSM < 1) throw Error(GLUED_E_CUDA, "batched runs kernel cannot be resident");
-        grid = sms * perSM;   // every CTA resident: required by the fused (cooperative) step
+        grid = sms * perSM;   // persistent: every CTA resident
         balance();
         parts = tune.parts > 0 ? std::max(minParts(), tune.parts) : minParts();
         hillPart.alloc(sizeof(double) * 3 * (size_t)W * grid);
@@ -726,38 +674,29 @@ struct Batch::Impl {
         dev.hillCvPos = hillCvPosD.as<const float4*>();
         dev.hillCvType = hillCvTypeD.as<int>();
         dev.rowAtom = rowAtomD.as<int>();
-        if (!bar.p) bar.alloc(sizeof(unsigned) * 4);
-        cudaCheck(cudaMemset(bar.p, 0, bar.bytes), "reset");
-        dev.bar = bar.as<unsigned>();
         dev.status = status.as<int>();
-        dev.spinLimit = 1ull << 22;
         destroyGraph();
     }
 
-    // dynamic shared memory of the runs kernel: the hill staging area
-    size_t dynSmem() const { return hill.present ? sizeof(HillStage) : 0; }
+    // dynamic shared memory of the runs kernel: coordination buffers, then the
+    // hill staging area
+    size_t dynSmem() const { return hillStageOffset<8>() + (hill.present ? sizeof(HillStage) : 0); }
 
     void launchRuns(cudaStream_t s) {
         void* args[] = {&dev};
-        const size_t dyn = dynSmem();
-        if (tune.fused)
-            cudaCheck(cudaLaunchCooperativeKernel((const void*)runs(), dim3(grid), dim3(256), args, dyn, s), "fused step");
-        else
-            cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(256), args, dyn, s), "runs");
+        cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(RUNS_THREADS), args, dynSmem(), s), "runs");
     }
     void launchFinalize(cudaStream_t s) {
-        if (tune.fused) return;
         void* args[] = {&dev};
         cudaCheck(cudaLaunchKernel((const void*)k_batch_finalize, dim3(W * parts), dim3(FT), args, 0, s), "finalize");
     }
-    // The step's launches on stream s: coordination runs, then the finalize
-    // (or the fused cooperative step).
+    // The step's launches on stream s: coordination runs, then the finalize.
     void launch(cudaStream_t s) {
         launchRuns(s);
         launchFinalize(s);
         cudaCheck(cudaGetLastError(), "step launch");
     }
-    int launchesPerStep() const { return tune.fused ? 1 : 2; }
+    int launchesPerStep() const { return 2; }
 };
 
 Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_desc* walkers) : impl_(new Impl()) {
@@ -944,7 +883,7 @@ void Batch::setStream(cudaStream_t s) {
 void Batch::setTuning(const BatchTuning& t) {
     if (t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 8");
     if (t.parts < 0 || t.parts > 4096) throw Error(GLUED_E_INVALID, "batch tuning: finalize parts must be 0..4096");
-    if (t.fused != 0 && t.fused != 1) throw Error(GLUED_E_INVALID, "batch tuning: fused must be 0 or 1");
+    if (t.reserved != 0) throw Error(GLUED_E_INVALID, "batch tuning: tune[2] is reserved and must be 0");
     cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
     impl_->tune = t;
     impl_->plan();
@@ -970,12 +909,7 @@ void Batch::execute() {
         if (!launched || ce != cudaSuccess || ie != cudaSuccess) {
             cudaGetLastError();
             I.graph = nullptr;
-            if (!I.tune.fused) throw Error(GLUED_E_CUDA, "batch: step graph capture failed");
-            // the cooperative launch could not be captured: use the two-launch step
-            I.tune.fused = 0;
-            I.plan();
-            execute();
-            return;
+            throw Error(GLUED_E_CUDA, "batch: step graph capture failed");
         }
     }
     cudaCheck(cudaGraphLaunch(I.graph, I.stream), "graph launch");
@@ -983,9 +917,8 @@ void Batch::execute() {
     I.ready = true;
 }
 
-// Autotuner: the step variant (two launches or one cooperative launch) and the
-// finalize CTAs per walker are timed on the live walkers with CUDA events
-// (forces go to a scratch buffer) and the fastest combination is kept.
+// Autotuner: the finalize CTAs per walker are timed on the live walkers with
+// CUDA events (forces go to a scratch buffer) and the fastest is kept.
 BatchTuning Batch::autotune() {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
@@ -1000,12 +933,10 @@ BatchTuning Batch::autotune() {
     cudaCheck(cudaEventCreate(&b), "event");
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
-    const BatchTuning saved = I.tune;
     const int base = I.minParts();
-    for (int fused : {0, 1})
-        for (int mul : {1, 2, 4}) {
+    for (int mul : {1, 2, 4}) {
             BatchTuning t;
-            t.ra = 8; t.parts = base * mul; t.fused = fused;
+            t.ra = 8; t.parts = base * mul;
             I.tune = t;
             I.plan();
             for (int r = 0; r < 2; r++) I.launch(I.stream);
@@ -1020,15 +951,12 @@ BatchTuning Batch::autotune() {
             I.launches += (long long)(reps + 2) * I.launchesPerStep();
             if (ms < bestMs) { bestMs = ms; best = t; }
         }
-    (void)saved;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaCheck(cudaMemcpy(I.walkersD.p, I.walkersH.data(), sizeof(BWalker) * I.walkersH.size(), cudaMemcpyHostToDevice), "tune");
     I.tune = best;
     I.plan();
     I.lastMs = bestMs;
-    int st = status();
-    if (st) throw Error(GLUED_E_TIMEOUT, "batch: bounded wait gave up during autotuning (status " + std::to_string(st) + ")");
     return best;
 }
 
@@ -1043,7 +971,7 @@ static double pct(std::vector<double>& v, double p) {
 // One regular step launched without the graph, each launch between CUDA events
 // and every CTA recording %globaltimer at its phase boundaries (runs: entry,
 // staging issued, coordination done, hill slice done; finalize: six stamps);
-// the layout of out[21] is given with glued_batch_phase_times.
+// the layout of out[24] is given with glued_batch_phase_times.
 void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
     constexpr int RS = 7, FS = 6;   // stamps per runs / finalize CTA

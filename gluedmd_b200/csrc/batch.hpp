@@ -11,10 +11,10 @@
 namespace glued {
 
 struct BatchTuning {
-    int ra = 8;       // A atoms per thread in the coordination tile (TA = 8 * ra)
-    int parts = 0;    // finalize CTAs per walker, which also split the hill table
-                      // (0: the fewest that cover its coordination rows)
-    int fused = 0;    // 1: one cooperative launch (runs, grid barrier, finalize)
+    int ra = 8;       // A atoms per thread in the coordination tile (TA = 16 * ra)
+    int parts = 0;    // finalize CTAs per walker (0: the fewest that cover its
+                      // coordination rows)
+    int reserved = 0; // must be 0
 };
 
 class Batch {

@@ -4,10 +4,11 @@
 // The reference evaluates every pair of a CV in one GPU thread. Here the pairs
 // of every coordination CV of the context are one list of (A tile, B chunk)
 // steps spread evenly over a persistent grid (coord_run.cuh):
-//   - warp w holds A atoms {w, w+8, ...} of the tile in registers (all lanes
-//     share them), lane l takes B atoms {l, l+32, l+64, l+96} of each chunk,
+//   - one 16-warp CTA per SM; warp w holds A atoms {w, w+16, ...} of the tile in
+//     registers (all lanes share them), lane l takes B atoms {l, l+32, l+64,
+//     l+96} of each chunk,
 //   - per-pair force factor h = (df/dx)/x in units of r0; A sums over lanes at
-//     the end of a tile's run, B sums over the 8 warps per chunk, both added as
+//     the end of a tile's run, B sums over the 16 warps per chunk, both added as
 //     64-bit fixed point (bitwise reproducible, independent of the grid),
 //   - k_coord_finalize converts the sums to the float Jacobian rows and the CN
 //     values and clears the accumulators for the next evaluation.
@@ -22,6 +23,9 @@
 //           window (CommonGluedKernels.cpp:983-1003);
 //   0     : non-integer exponents: the reference formula (pow, Taylor branch).
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "context.hpp"
 #include "coord_run.cuh"
@@ -29,9 +33,13 @@
 
 namespace glued {
 
+// One CTA of COORD_NW warps per SM: its warps meet at a barrier every step, so
+// none of them runs ahead; buffers in dynamic shared memory (above the 48 KB
+// static limit).
 template <int RA, int BOX, int NH, bool HI>
-__global__ void __launch_bounds__(256, 2) k_coord_run(CoordRunDev R) {
-    __shared__ CoordRunSmem<RA> sm;
+__global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    CoordRunSmem<RA>& sm = *reinterpret_cast<CoordRunSmem<RA>*>(dsm);
     const int s0 = R.begin[blockIdx.x], s1 = R.begin[blockIdx.x + 1];
     if (s0 < s1) coordRun<RA, BOX, NH, HI>(R, s0, s1, sm, NoPieceHook());
 }
@@ -81,22 +89,23 @@ void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* s
     if (n > 0) k_compose_slots<<<(n + 255) / 256, 256, 0, s>>>(atoms, u2g, slots, n);
 }
 
-// Two 33 KB CTAs per SM need the shared-memory carveout at its maximum; the
-// default split may leave room for one, which halves the resident grid.
-template <class K>
-static void maxSharedCarveout(K* fn) {
-    static bool done = false;
-    if (!done) {
-        cudaCheck(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared), "carveout");
-        done = true;
-    }
+void runKernelSetup(const void* fn, size_t dynSmem) {
+    static std::mutex mu;
+    static std::set<std::pair<std::pair<const void*, int>, size_t>> done;
+    int dev = 0;
+    cudaCheck(cudaGetDevice(&dev), "device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done.insert({{fn, dev}, dynSmem}).second) return;
+    cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared), "carveout");
+    cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynSmem), "smem");
 }
 
 template <int RA, int BOX, int NH, bool HI>
 static void launchRun(cudaStream_t s, int grid, const CoordRunDev& R) {
-    maxSharedCarveout(k_coord_run<RA, BOX, NH, HI>);
-    k_coord_run<RA, BOX, NH, HI><<<grid, 256, 0, s>>>(R);
+    const size_t dyn = sizeof(CoordRunSmem<RA>);
+    runKernelSetup((const void*)k_coord_run<RA, BOX, NH, HI>, dyn);
+    k_coord_run<RA, BOX, NH, HI><<<grid, COORD_NW * 32, dyn, s>>>(R);
 }
 
 template <int BOX>
@@ -138,10 +147,10 @@ int coordRunOccupancy(int kind, int boxKind, bool hi) {
         fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 0, true>
              : boxKind == 1 ? (const void*)k_coord_run<8, 1, 0, true> : (const void*)k_coord_run<8, 2, 0, true>;
     }
-    cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   (int)cudaSharedmemCarveoutMaxShared), "carveout");
+    const size_t dyn = sizeof(CoordRunSmem<8>);
+    runKernelSetup(fn, dyn);
     int perSM = 0;
-    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, 256, 0), "occupancy");
+    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, COORD_NW * 32, dyn), "occupancy");
     return std::max(1, perSM);
 }
 

@@ -171,6 +171,123 @@ __device__ __host__ __forceinline__ double coordAccScale(const CoordItem& it) {
     return it.kind > 0 ? -(double)it.n / (double)it.r0 : 1.0 / (double)it.r0;
 }
 
+// Packed FP32 (f32x2, sm_100): one instruction operates on two floats held in
+// a 64-bit register pair. These halve the issue slots of the pair arithmetic;
+// the FP32 pipe throughput per element is unchanged.
+namespace f2 {
+__device__ __forceinline__ unsigned long long pk(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk(unsigned long long v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long add(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long sub(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long mul(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+}  // namespace f2
+
+// The pairs of one full step (TA x CH, switch m = 2n = 4 NH) with packed
+// arithmetic: A atoms (2i, 2i+1) of the warp form one packed operand, each B atom
+// is broadcast (negated) into both halves, and the B atoms of the lane are taken
+// two at a time so that their packed gradient partials fit in registers. Same
+// per-pair operations and bounds as the scalar loop; the A-gradient, B-gradient
+// and CN sums are kept as two partials (even / odd A atoms) and added at the end
+// of the step. Writes the warp's B partials to gw (negated sums) and adds the
+// step's CN to cnc.
+template <int RA, int BOX, int NH, bool HI>
+__device__ __forceinline__ void pairsPacked(const float (&ax)[RA], const float (&ay)[RA], const float (&az)[RA],
+                                            float (&gax)[RA], float (&gay)[RA], float (&gaz)[RA],
+                                            const float4* pos, const RunConst& K, float* gw, float& cnc) {
+    static_assert(RA % 2 == 0 && NH > 0 && BOX != 2, "packed pair block");
+    constexpr float R = 12582912.0f;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long R2 = f2::pk(R, R), ONE2 = f2::pk(1.0f, 1.0f);
+    const unsigned long long ivx = f2::pk(K.box.inv[0], K.box.inv[0]), ivy = f2::pk(K.box.inv[1], K.box.inv[1]),
+                             ivz = f2::pk(K.box.inv[2], K.box.inv[2]);
+    const unsigned long long nLx = f2::pk(-K.box.a[0], -K.box.a[0]), nLy = f2::pk(-K.box.b[1], -K.box.b[1]),
+                             nLz = f2::pk(-K.box.c[2], -K.box.c[2]);
+    const float INF = __int_as_float(0x7f800000);
+    unsigned long long cn2 = 0ull;
+#pragma unroll
+    for (int half = 0; half < crun::RB / 2; half++) {
+        unsigned long long nbx[2], nby[2], nbz[2], gbx[2], gby[2], gbz[2];
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++) {
+            const float4 p = pos[lane + 32 * (2 * half + jj)];
+            const float x = -__fmul_rn(p.x, K.ir0), y = -__fmul_rn(p.y, K.ir0), z = -__fmul_rn(p.z, K.ir0);
+            nbx[jj] = f2::pk(x, x); nby[jj] = f2::pk(y, y); nbz[jj] = f2::pk(z, z);
+            gbx[jj] = gby[jj] = gbz[jj] = 0ull;
+        }
+#pragma unroll
+        for (int i = 0; i < RA / 2; i++) {
+            const unsigned long long px = f2::pk(ax[2 * i], ax[2 * i + 1]), py = f2::pk(ay[2 * i], ay[2 * i + 1]),
+                                     pz = f2::pk(az[2 * i], az[2 * i + 1]);
+            unsigned long long gx = f2::pk(gax[2 * i], gax[2 * i + 1]), gy = f2::pk(gay[2 * i], gay[2 * i + 1]),
+                               gz = f2::pk(gaz[2 * i], gaz[2 * i + 1]);
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++) {
+                unsigned long long dx = f2::add(px, nbx[jj]), dy = f2::add(py, nby[jj]), dz = f2::add(pz, nbz[jj]);
+                if (BOX == 1) {
+                    dx = f2::fma(f2::sub(f2::fma(dx, ivx, R2), R2), nLx, dx);
+                    dy = f2::fma(f2::sub(f2::fma(dy, ivy, R2), R2), nLy, dy);
+                    dz = f2::fma(f2::sub(f2::fma(dz, ivz, R2), R2), nLz, dz);
+                }
+                const unsigned long long x2 = f2::fma(dz, dz, f2::fma(dy, dy, f2::mul(dx, dx)));
+                unsigned long long pw = NH == 1 ? ONE2 : x2;
+#pragma unroll
+                for (int e = 2; e < NH; e++) pw = f2::mul(pw, x2);
+                const unsigned long long yy = f2::fma(pw, x2, ONE2);
+                float xa, xb, ya, yb;
+                f2::upk(x2, xa, xb);
+                f2::upk(yy, ya, yb);
+                ya = (HI ? (xa >= K.lo && xa < K.hi) : (xa >= K.lo)) ? ya : INF;
+                yb = (HI ? (xb >= K.lo && xb < K.hi) : (xb >= K.lo)) ? yb : INF;
+                float fa, fb;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(fa) : "f"(ya));
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(fb) : "f"(yb));
+                const unsigned long long ff = f2::pk(fa, fb);
+                const unsigned long long h = f2::mul(f2::mul(pw, ff), ff);
+                cn2 = f2::add(cn2, ff);
+                gx = f2::fma(h, dx, gx); gy = f2::fma(h, dy, gy); gz = f2::fma(h, dz, gz);
+                gbx[jj] = f2::fma(h, dx, gbx[jj]); gby[jj] = f2::fma(h, dy, gby[jj]); gbz[jj] = f2::fma(h, dz, gbz[jj]);
+            }
+            f2::upk(gx, gax[2 * i], gax[2 * i + 1]);
+            f2::upk(gy, gay[2 * i], gay[2 * i + 1]);
+            f2::upk(gz, gaz[2 * i], gaz[2 * i + 1]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++) {
+            const int o = (lane + 32 * (2 * half + jj)) * 3;
+            float a, c;
+            f2::upk(gbx[jj], a, c); gw[o] = -(a + c);
+            f2::upk(gby[jj], a, c); gw[o + 1] = -(a + c);
+            f2::upk(gbz[jj], a, c); gw[o + 2] = -(a + c);
+        }
+    }
+    float c0, c1;
+    f2::upk(cn2, c0, c1);
+    cnc += c0 + c1;
+}
+
 struct NoPieceHook {
     __device__ void operator()(int, int) const {}
 };
@@ -248,24 +365,34 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
 #pragma unroll
                 for (int k = 0; k < RA; k++) {
                     const float4 p = sm.apos[b][ty + NW * k];
-                    ax[k] = p.x * K.ir0; ay[k] = p.y * K.ir0; az[k] = p.z * K.ir0;
+                    ax[k] = __fmul_rn(p.x, K.ir0); ay[k] = __fmul_rn(p.y, K.ir0); az[k] = __fmul_rn(p.z, K.ir0);
                     gax[k] = gay[k] = gaz[k] = 0.0f;
                 }
                 cn = 0.0;
                 pieceSteps = 0;
             }
             pieceSteps++;
+            float cnc = 0.0f;
+            const bool full = nAv == TA && nBv == CH;
+            float* gw = sm.g[b][ty];
+            bool packed = false;
+            if constexpr (NH > 0 && BOX != 2) {
+                if (full) {
+                    pairsPacked<RA, BOX, NH, HI>(ax, ay, az, gax, gay, gaz, sm.pos[b], K, gw, cnc);
+                    packed = true;
+                }
+            }
+            if (!packed) {
             // B scaled exactly as A, so that an atom present in both groups gives
-            // a difference of exactly zero (excluded by the lower bound)
+            // a difference of exactly zero (excluded by the lower bound); the
+            // products are rounded (never contracted into the subtraction)
             float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
 #pragma unroll
             for (int j = 0; j < RB; j++) {
                 const float4 p = sm.pos[b][lane + 32 * j];
-                bx[j] = p.x * K.ir0; by[j] = p.y * K.ir0; bz[j] = p.z * K.ir0;
+                bx[j] = __fmul_rn(p.x, K.ir0); by[j] = __fmul_rn(p.y, K.ir0); bz[j] = __fmul_rn(p.z, K.ir0);
                 gbx[j] = gby[j] = gbz[j] = 0.0f;
             }
-            float cnc = 0.0f;
-            const bool full = nAv == TA && nBv == CH;
             if (NH > 0 && full) {
 #pragma unroll
                 for (int k = 0; k < RA; k++) {
@@ -299,14 +426,14 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                     }
                 }
             }
-            cn += (double)cnc;
             // B partials of this warp
-            float* gw = sm.g[b][ty];
 #pragma unroll
             for (int j = 0; j < RB; j++) {
                 const int o = (lane + 32 * j) * 3;
                 gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
             }
+            }
+            cn += (double)cnc;
             if (last) {
                 // A sums over lanes; lane 3k + c adds component c of atom k
 #pragma unroll

@@ -96,7 +96,7 @@ struct CoordDev {
 };
 
 // Coordination as static per-CTA runs of (A tile, B chunk) steps (coord_run.cuh).
-constexpr int COORD_NW = 8;     // warps per CTA
+constexpr int COORD_NW = 16;    // warps per CTA
 constexpr int COORD_CH = 128;   // B atoms per chunk
 constexpr int COORD_F_FIRST = 1, COORD_F_LAST = 2;
 

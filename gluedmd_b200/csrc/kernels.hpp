@@ -25,6 +25,9 @@ void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, i
                  bool hi, const JacDev& J, double* cvv, int parts = 3);
 void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* slots, int n);
 int coordRunOccupancy(int kind, int boxKind, bool hi);
+// Once per (kernel, device, size): maximum shared-memory carveout and the
+// dynamic shared-memory limit of a persistent runs kernel.
+void runKernelSetup(const void* fn, size_t dynSmem);
 // Host planning: steps tile-major (fills row0 / tilesA of the items, returns the
 // accumulator row count); per-CTA ranges of numSteps over grid CTAs with preCost[b]
 // steps' worth of other work on CTA b; whether the upper pair bound can bind.

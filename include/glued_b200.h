@@ -252,12 +252,10 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
                        glued_batch** out);
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
-/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker, which
- * also split the hill table; 0 = the fewest that cover the walker's
- * coordination rows), fused (1: one cooperative launch with a bounded grid
- * barrier between the runs and the finalize; 0: two launches), 0}. autotune
- * times every candidate on the live walkers (forces of the trial launches go to
- * a scratch buffer), keeps the fastest and returns it in tune (synchronizing). */
+/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
+ * fewest that cover the walker's coordination rows), 0, 0}. autotune times the
+ * candidates on the live walkers (forces of the trial launches go to a scratch
+ * buffer), keeps the fastest and returns it in tune (synchronizing).          */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);
@@ -275,8 +273,9 @@ int glued_batch_num_cvs(glued_batch* b, int* n);
 int glued_batch_num_hills(glued_batch* b, int* n);
 int glued_batch_set_hills(glued_batch* b, const double* centers, const double* heights, int n);
 int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int n);
-/* Status word of the step's device checks (0 = ok; bit 0: a grid-barrier wait
- * of the fused step gave up after its bound).                                  */
+/* Status word of the batch's device checks (0 = ok; bit 0: a deposit found the
+ * hill table full, maxHills, and dropped hills). Sticky until the batch is
+ * destroyed.                                                                   */
 int glued_batch_status(glued_batch* b, int* status);
 int glued_batch_launch_count(glued_batch* b, long long* count);
 /* Profiling: runs one regular step (forces are accumulated as by execute), each

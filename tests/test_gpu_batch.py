@@ -50,14 +50,14 @@ def _oracle(w, biases, hill):
     return s
 
 
-@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("parts", [0, 5])
 @pytest.mark.parametrize("with_hills", [False, True])
-def test_batch_matches_fp64_oracle(with_hills, fused):
-    """Both step variants: two launches, and one cooperative launch with a grid
-    barrier between the runs and the finalize."""
+def test_batch_matches_fp64_oracle(with_hills, parts):
+    """The batched step against the FP64 oracle, with the fewest finalize parts
+    per walker and with more parts than rows need."""
     ws, hill = _walkers()
     b, walkers, specs = _setup(ws, hill, with_hills)
-    b.set_tuning(8, 0, fused)
+    b.set_tuning(8, parts)
     for wk in walkers:
         wk.force.zero_()
     b.execute()
@@ -119,6 +119,24 @@ def test_batch_deposit_walker_order():
         d = cv[i, 0] - np.float32(ws[i]["d0"] + 0.05)
         Vh = E[i] - 0.5 * 100.0 * d * d
         assert abs(h[n0 + i] - 1.2 * math.exp(-Vh * hif)) < 1e-9
+    assert b.status() == 0
+
+
+def test_batch_full_hill_table_sets_status():
+    """A deposit that finds the table at its capacity keeps the hills that fit,
+    drops the rest and raises bit 0 of the status word."""
+    ws, hill = _walkers(n_walkers=4, n_hills=500)
+    hill["iparams"] = [1, 502, 1, 0]  # pace 1, room for two more hills
+    b, walkers, specs = _setup(ws, hill, True, coord_restraint=False)
+    assert b.num_hills() == 500 and b.status() == 0
+    b.execute()
+    cv = b.cv_values()
+    b.update_state(1)
+    assert b.num_hills() == 502
+    assert b.status() == 1
+    c, h = b.get_hills()
+    for i in range(2):
+        assert c[500 + i, 0] == cv[i, 2] and c[500 + i, 1] == cv[i, 1]
 
 
 def test_batch_rejects_unsupported_structure():
