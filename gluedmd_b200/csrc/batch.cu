@@ -595,7 +595,7 @@ struct Batch::Impl {
 
     void plan() {
         // coordination steps over all walkers' items (walker-major)
-        buildCoordSteps(items, 8, steps);
+        buildCoordSteps(items, 8, steps, std::max(nC, 1));
         rows = 0;
         for (int c = 0; c < nC; c++) rows += items[c].nA + items[c].nB;
         std::vector<const float4*> posqOf(W);
@@ -638,7 +638,6 @@ struct Batch::Impl {
         dev.R.slots = atomsD.as<int>();
         dev.R.sysPosq = sysPosqD.as<const float4*>();
         dev.R.sysBox = boxesD.as<BoxDev>();
-        dev.R.itemsPerSys = std::max(nC, 1);
         dev.R.acc = acc.as<unsigned long long>();
         dev.R.cnPiece = cnPiece.as<double>();
         dev.rowsPerWalker = rows;

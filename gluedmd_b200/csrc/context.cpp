@@ -362,7 +362,7 @@ void Context::buildPlan(const GluedForce& f) {
             if (it.kind != coordKind_) coordKind_ = (coordKind_ == 0 || it.kind == 0) ? 0 : -1;
         if (coordKind_ != 3)
             for (auto& it : coord) it.kind = coordKind_;
-        coordRows_ = buildCoordSteps(coord, 8, coordStepsH_);
+        coordRows_ = buildCoordSteps(coord, 8, coordStepsH_, 1 << 30);
         coordItemsN_ = (int)coord.size();
         coordAtomsN_ = (int)coordAtoms.size();
         int dev = 0, sms = 0;
@@ -388,7 +388,6 @@ void Context::buildPlan(const GluedForce& f) {
         R_.slots = coordSlots_.as<int>();
         R_.sysPosq = coordSysPosq_.as<const float4*>();
         R_.sysBox = box_.as<BoxDev>();
-        R_.itemsPerSys = 1 << 30;
         R_.acc = coordAcc_.as<unsigned long long>();
         R_.cnPiece = coordCnPiece_.as<double>();
     }

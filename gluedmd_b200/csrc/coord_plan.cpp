@@ -8,7 +8,7 @@
 
 namespace glued {
 
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps) {
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps, int itemsPerSys) {
     const int TA = COORD_NW * ra;
     steps.clear();
     int rows = 0;
@@ -30,6 +30,7 @@ int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep
                 int fl = (c == 0 ? COORD_F_FIRST : 0) | (c == nCh - 1 ? COORD_F_LAST : 0);
                 s.packed = nAv | (nBv << 8) | (fl << 16);
                 s.pieceSlot = -1;
+                s.sys = (int)i / std::max(1, itemsPerSys);
                 steps.push_back(s);
             }
         }

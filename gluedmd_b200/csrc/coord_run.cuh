@@ -205,26 +205,38 @@ __device__ __forceinline__ unsigned long long mul(unsigned long long a, unsigned
 }
 }  // namespace f2
 
+// Image constants of a step in packed form (both halves equal).
+struct PackedConst {
+    unsigned long long ivx, ivy, ivz, nLx, nLy, nLz;
+};
+__device__ __forceinline__ PackedConst packedConst(const RunConst& K) {
+    PackedConst c;
+    c.ivx = f2::pk(K.box.inv[0], K.box.inv[0]); c.ivy = f2::pk(K.box.inv[1], K.box.inv[1]);
+    c.ivz = f2::pk(K.box.inv[2], K.box.inv[2]);
+    c.nLx = f2::pk(-K.box.a[0], -K.box.a[0]); c.nLy = f2::pk(-K.box.b[1], -K.box.b[1]);
+    c.nLz = f2::pk(-K.box.c[2], -K.box.c[2]);
+    return c;
+}
+
 // The pairs of one full step (TA x CH, switch m = 2n = 4 NH) with packed
-// arithmetic: A atoms (2i, 2i+1) of the warp form one packed operand, each B atom
-// is broadcast (negated) into both halves, and the B atoms of the lane are taken
-// two at a time so that their packed gradient partials fit in registers. Same
-// per-pair operations and bounds as the scalar loop; the A-gradient, B-gradient
-// and CN sums are kept as two partials (even / odd A atoms) and added at the end
-// of the step. Writes the warp's B partials to gw (negated sums) and adds the
-// step's CN to cnc.
+// arithmetic: A atoms (2i, 2i+1) of the warp are one packed operand (apx[i], ...,
+// kept packed across steps), each B atom is broadcast (negated) into both
+// halves, and the B atoms of the lane are taken two at a time so that their
+// packed gradient partials fit in registers. Same per-pair operations and
+// bounds as the scalar loop; B-gradient and CN sums are kept as two partials
+// (even / odd A atoms) and added at the end of the step. Writes the warp's B
+// partials to gw (negated sums) and adds the step's CN to cnc.
 template <int RA, int BOX, int NH, bool HI>
-__device__ __forceinline__ void pairsPacked(const float (&ax)[RA], const float (&ay)[RA], const float (&az)[RA],
-                                            float (&gax)[RA], float (&gay)[RA], float (&gaz)[RA],
+__device__ __forceinline__ void pairsPacked(const unsigned long long (&apx)[RA / 2],
+                                            const unsigned long long (&apy)[RA / 2],
+                                            const unsigned long long (&apz)[RA / 2], unsigned long long (&gpx)[RA / 2],
+                                            unsigned long long (&gpy)[RA / 2], unsigned long long (&gpz)[RA / 2],
                                             const float4* pos, const RunConst& K, float* gw, float& cnc) {
     static_assert(RA % 2 == 0 && NH > 0 && BOX != 2, "packed pair block");
-    constexpr float R = 12582912.0f;
+    constexpr float R = 12582912.0f;   // 1.5 * 2^23: adding and removing it rounds to an integer
     const int lane = threadIdx.x & 31;
     const unsigned long long R2 = f2::pk(R, R), ONE2 = f2::pk(1.0f, 1.0f);
-    const unsigned long long ivx = f2::pk(K.box.inv[0], K.box.inv[0]), ivy = f2::pk(K.box.inv[1], K.box.inv[1]),
-                             ivz = f2::pk(K.box.inv[2], K.box.inv[2]);
-    const unsigned long long nLx = f2::pk(-K.box.a[0], -K.box.a[0]), nLy = f2::pk(-K.box.b[1], -K.box.b[1]),
-                             nLz = f2::pk(-K.box.c[2], -K.box.c[2]);
+    const PackedConst C = packedConst(K);
     const float INF = __int_as_float(0x7f800000);
     unsigned long long cn2 = 0ull;
 #pragma unroll
@@ -239,17 +251,14 @@ __device__ __forceinline__ void pairsPacked(const float (&ax)[RA], const float (
         }
 #pragma unroll
         for (int i = 0; i < RA / 2; i++) {
-            const unsigned long long px = f2::pk(ax[2 * i], ax[2 * i + 1]), py = f2::pk(ay[2 * i], ay[2 * i + 1]),
-                                     pz = f2::pk(az[2 * i], az[2 * i + 1]);
-            unsigned long long gx = f2::pk(gax[2 * i], gax[2 * i + 1]), gy = f2::pk(gay[2 * i], gay[2 * i + 1]),
-                               gz = f2::pk(gaz[2 * i], gaz[2 * i + 1]);
 #pragma unroll
             for (int jj = 0; jj < 2; jj++) {
-                unsigned long long dx = f2::add(px, nbx[jj]), dy = f2::add(py, nby[jj]), dz = f2::add(pz, nbz[jj]);
+                unsigned long long dx = f2::add(apx[i], nbx[jj]), dy = f2::add(apy[i], nby[jj]),
+                                   dz = f2::add(apz[i], nbz[jj]);
                 if (BOX == 1) {
-                    dx = f2::fma(f2::sub(f2::fma(dx, ivx, R2), R2), nLx, dx);
-                    dy = f2::fma(f2::sub(f2::fma(dy, ivy, R2), R2), nLy, dy);
-                    dz = f2::fma(f2::sub(f2::fma(dz, ivz, R2), R2), nLz, dz);
+                    dx = f2::fma(f2::sub(f2::fma(dx, C.ivx, R2), R2), C.nLx, dx);
+                    dy = f2::fma(f2::sub(f2::fma(dy, C.ivy, R2), R2), C.nLy, dy);
+                    dz = f2::fma(f2::sub(f2::fma(dz, C.ivz, R2), R2), C.nLz, dz);
                 }
                 const unsigned long long x2 = f2::fma(dz, dz, f2::fma(dy, dy, f2::mul(dx, dx)));
                 unsigned long long pw = NH == 1 ? ONE2 : x2;
@@ -267,12 +276,9 @@ __device__ __forceinline__ void pairsPacked(const float (&ax)[RA], const float (
                 const unsigned long long ff = f2::pk(fa, fb);
                 const unsigned long long h = f2::mul(f2::mul(pw, ff), ff);
                 cn2 = f2::add(cn2, ff);
-                gx = f2::fma(h, dx, gx); gy = f2::fma(h, dy, gy); gz = f2::fma(h, dz, gz);
+                gpx[i] = f2::fma(h, dx, gpx[i]); gpy[i] = f2::fma(h, dy, gpy[i]); gpz[i] = f2::fma(h, dz, gpz[i]);
                 gbx[jj] = f2::fma(h, dx, gbx[jj]); gby[jj] = f2::fma(h, dy, gby[jj]); gbz[jj] = f2::fma(h, dz, gbz[jj]);
             }
-            f2::upk(gx, gax[2 * i], gax[2 * i + 1]);
-            f2::upk(gy, gay[2 * i], gay[2 * i + 1]);
-            f2::upk(gz, gaz[2 * i], gaz[2 * i + 1]);
         }
 #pragma unroll
         for (int jj = 0; jj < 2; jj++) {
@@ -306,9 +312,12 @@ template <int RA, int BOX, int NH, bool HI, class Hook, class Start = NoStartHoo
 __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook,
                          const Start& start = Start()) {
     using namespace crun;
+    static_assert(RA % 2 == 0 && 3 * RA <= 32, "A atoms per warp");
     constexpr int TA = NW * RA;
+    constexpr int RH = RA / 2;
     const int tid = threadIdx.x, lane = tid & 31, ty = tid >> 5;
-    float ax[RA], ay[RA], az[RA], gax[RA], gay[RA], gaz[RA];
+    // A atoms 2i, 2i+1 of the warp (scaled) and their gradient sums, packed
+    unsigned long long apx[RH], apy[RH], apz[RH], gpx[RH], gpy[RH], gpz[RH];
     RunConst K;
     double cn = 0.0;
     int pieceSteps = 0;
@@ -329,7 +338,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             const bool first = (w0 + ls == s0) || (fl & F_FIRST);
             ib = (tid < CH && tid < nBv) ? __ldg(R.slots + d.bStart + tid) : -1;
             ia = (first && tid < TA && tid < nAv) ? __ldg(R.slots + d.aStart + tid) : -1;
-            pq = R.sysPosq[d.item / R.itemsPerSys];
+            pq = R.sysPosq[d.sys];
         };
         auto issue = [&](int ls, int ib, int ia, const float4* pq) {
             const CoordStep& d = sm.st[ls];
@@ -361,12 +370,14 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             if (ls + 2 < nw) loadIdx(ls + 2, ib2, ia2, pq2);
             if (first) {
                 const CoordItem it = R.items[d.item];
-                K = runConst(it, R.sysBox[d.item / R.itemsPerSys]);
+                K = runConst(it, R.sysBox[d.sys]);
 #pragma unroll
-                for (int k = 0; k < RA; k++) {
-                    const float4 p = sm.apos[b][ty + NW * k];
-                    ax[k] = __fmul_rn(p.x, K.ir0); ay[k] = __fmul_rn(p.y, K.ir0); az[k] = __fmul_rn(p.z, K.ir0);
-                    gax[k] = gay[k] = gaz[k] = 0.0f;
+                for (int i = 0; i < RH; i++) {
+                    const float4 p = sm.apos[b][ty + NW * (2 * i)], q = sm.apos[b][ty + NW * (2 * i + 1)];
+                    apx[i] = f2::pk(__fmul_rn(p.x, K.ir0), __fmul_rn(q.x, K.ir0));
+                    apy[i] = f2::pk(__fmul_rn(p.y, K.ir0), __fmul_rn(q.y, K.ir0));
+                    apz[i] = f2::pk(__fmul_rn(p.z, K.ir0), __fmul_rn(q.z, K.ir0));
+                    gpx[i] = gpy[i] = gpz[i] = 0ull;
                 }
                 cn = 0.0;
                 pieceSteps = 0;
@@ -378,77 +389,70 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             bool packed = false;
             if constexpr (NH > 0 && BOX != 2) {
                 if (full) {
-                    pairsPacked<RA, BOX, NH, HI>(ax, ay, az, gax, gay, gaz, sm.pos[b], K, gw, cnc);
+                    pairsPacked<RA, BOX, NH, HI>(apx, apy, apz, gpx, gpy, gpz, sm.pos[b], K, gw, cnc);
                     packed = true;
                 }
             }
             if (!packed) {
-            // B scaled exactly as A, so that an atom present in both groups gives
-            // a difference of exactly zero (excluded by the lower bound); the
-            // products are rounded (never contracted into the subtraction)
-            float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
+                // Scalar pairs (ragged steps, triclinic boxes, other switch
+                // kinds). B is scaled exactly as A, so that an atom present in
+                // both groups gives a difference of exactly zero (excluded by the
+                // lower bound); the products are rounded, never contracted.
+                float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
 #pragma unroll
-            for (int j = 0; j < RB; j++) {
-                const float4 p = sm.pos[b][lane + 32 * j];
-                bx[j] = __fmul_rn(p.x, K.ir0); by[j] = __fmul_rn(p.y, K.ir0); bz[j] = __fmul_rn(p.z, K.ir0);
-                gbx[j] = gby[j] = gbz[j] = 0.0f;
-            }
-            if (NH > 0 && full) {
-#pragma unroll
-                for (int k = 0; k < RA; k++) {
-#pragma unroll
-                    for (int j = 0; j < RB; j++) {
-                        float dx = ax[k] - bx[j], dy = ay[k] - by[j], dz = az[k] - bz[j];
-                        imageS<BOX>(dx, dy, dz, K.box);
-                        const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        float f, h;
-                        switchX2<NH>(x2, HI ? (x2 >= K.lo && x2 < K.hi) : (x2 >= K.lo), K, f, h);
-                        cnc += f;
-                        gax[k] = fmaf(h, dx, gax[k]); gay[k] = fmaf(h, dy, gay[k]); gaz[k] = fmaf(h, dz, gaz[k]);
-                        gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
-                    }
+                for (int j = 0; j < RB; j++) {
+                    const float4 p = sm.pos[b][lane + 32 * j];
+                    bx[j] = __fmul_rn(p.x, K.ir0); by[j] = __fmul_rn(p.y, K.ir0); bz[j] = __fmul_rn(p.z, K.ir0);
+                    gbx[j] = gby[j] = gbz[j] = 0.0f;
                 }
-            } else {
 #pragma unroll
-                for (int k = 0; k < RA; k++) {
-                    const bool av = (ty + NW * k) < nAv;
+                for (int i = 0; i < RH; i++) {
+                    float ax[2], ay[2], az[2], gx[2], gy[2], gz[2];
+                    f2::upk(apx[i], ax[0], ax[1]); f2::upk(apy[i], ay[0], ay[1]); f2::upk(apz[i], az[0], az[1]);
+                    f2::upk(gpx[i], gx[0], gx[1]); f2::upk(gpy[i], gy[0], gy[1]); f2::upk(gpz[i], gz[0], gz[1]);
 #pragma unroll
-                    for (int j = 0; j < RB; j++) {
-                        const bool bv = (lane + 32 * j) < nBv;
-                        float dx = ax[k] - bx[j], dy = ay[k] - by[j], dz = az[k] - bz[j];
-                        imageS<BOX>(dx, dy, dz, K.box);
-                        const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        float f, h;
-                        switchX2<NH>(x2, av && bv && x2 >= K.lo && x2 < K.hi, K, f, h);
-                        cnc += f;
-                        gax[k] = fmaf(h, dx, gax[k]); gay[k] = fmaf(h, dy, gay[k]); gaz[k] = fmaf(h, dz, gaz[k]);
-                        gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
+                    for (int e = 0; e < 2; e++) {
+                        const bool av = (ty + NW * (2 * i + e)) < nAv;
+#pragma unroll
+                        for (int j = 0; j < RB; j++) {
+                            const bool bv = (lane + 32 * j) < nBv;
+                            float dx = ax[e] - bx[j], dy = ay[e] - by[j], dz = az[e] - bz[j];
+                            imageS<BOX>(dx, dy, dz, K.box);
+                            const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            float f, h;
+                            switchX2<NH>(x2, av && bv && x2 >= K.lo && x2 < K.hi, K, f, h);
+                            cnc += f;
+                            gx[e] = fmaf(h, dx, gx[e]); gy[e] = fmaf(h, dy, gy[e]); gz[e] = fmaf(h, dz, gz[e]);
+                            gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
+                        }
                     }
+                    gpx[i] = f2::pk(gx[0], gx[1]); gpy[i] = f2::pk(gy[0], gy[1]); gpz[i] = f2::pk(gz[0], gz[1]);
                 }
-            }
-            // B partials of this warp
 #pragma unroll
-            for (int j = 0; j < RB; j++) {
-                const int o = (lane + 32 * j) * 3;
-                gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
-            }
+                for (int j = 0; j < RB; j++) {
+                    const int o = (lane + 32 * j) * 3;
+                    gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
+                }
             }
             cn += (double)cnc;
             if (last) {
-                // A sums over lanes; lane 3k + c adds component c of atom k
+                // A sums over lanes: slot 3k + c = component c of A atom k, one
+                // butterfly for all slots; lane 3k + c adds its slot
+                float v[32];
 #pragma unroll
-                for (int k = 0; k < RA; k++) {
-                    const float x = warpSumF(gax[k]), y = warpSumF(gay[k]), z = warpSumF(gaz[k]);
-                    const int i = ty + NW * k;
-                    if (i < nAv) {
-                        unsigned long long* a = R.acc + 3 * (size_t)(d.rowA + i);
-                        if (lane == 3 * k) redAddI64(a, __float2ll_rn(x * FX));
-                        if (lane == 3 * k + 1) redAddI64(a + 1, __float2ll_rn(y * FX));
-                        if (lane == 3 * k + 2) redAddI64(a + 2, __float2ll_rn(z * FX));
-                    }
+                for (int i = 0; i < RH; i++) {
+                    f2::upk(gpx[i], v[6 * i], v[6 * i + 3]);
+                    f2::upk(gpy[i], v[6 * i + 1], v[6 * i + 4]);
+                    f2::upk(gpz[i], v[6 * i + 2], v[6 * i + 5]);
                 }
-                const double c = warpSum(cn);
-                if (lane == 0) sm.red[b][ty] = c;
+#pragma unroll
+                for (int k = 3 * RA; k < 32; k++) v[k] = 0.0f;
+                const float t = warpTransposeSum32(v);
+                const int k = lane / 3, c = lane - 3 * k;
+                const int i = ty + NW * k;
+                if (lane < 3 * RA && i < nAv) redAddI64(R.acc + 3 * (size_t)(d.rowA + i) + c, __float2ll_rn(t * FX));
+                const double cs = warpSum(cn);
+                if (lane == 0) sm.red[b][ty] = cs;
             }
             cpAsyncWaitAll();
             __syncthreads();

@@ -109,7 +109,7 @@ struct __align__(16) CoordStep {
     int rowB;            // acc row of the chunk's first B atom
     int packed;          // nAv | nBv << 8 | flags << 16 (COORD_F_*)
     int pieceSlot;       // cnPiece slot of the run piece this step ends (static ranges), else -1
-    int pad;
+    int sys;             // system of the item (index into sysPosq / sysBox)
 };
 
 struct CoordRunDev {
@@ -117,9 +117,8 @@ struct CoordRunDev {
     const CoordStep* steps;
     const int* begin;          // [grid + 1]: CTA b runs steps [begin[b], begin[b+1])
     const int* slots;          // per coordination atom: its row in posq
-    const float4* const* sysPosq;  // positions of system item / itemsPerSys
-    const BoxDev* sysBox;      // box of system item / itemsPerSys
-    int itemsPerSys;
+    const float4* const* sysPosq;  // positions of system CoordStep::sys
+    const BoxDev* sysBox;      // box of system CoordStep::sys
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
     double* cnPiece;           // CN partial of every run piece, item-contiguous (CoordItem::pieceBegin/End)
 };

@@ -31,7 +31,8 @@ void runKernelSetup(const void* fn, size_t dynSmem);
 // Host planning: steps tile-major (fills row0 / tilesA of the items, returns the
 // accumulator row count); per-CTA ranges of numSteps over grid CTAs with preCost[b]
 // steps' worth of other work on CTA b; whether the upper pair bound can bind.
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps);
+// itemsPerSys: items of one system (sysPosq / sysBox entry), item-major.
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps, int itemsPerSys);
 std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost);
 // Run pieces of the static ranges (maximal sub-runs of one tile on one CTA): the
 // piece slots of their last steps, item-contiguous in step order, and every
