@@ -1,13 +1,14 @@
 // Coordination pairs as static per-CTA runs of (item, A tile, B chunk) steps.
 //
 // Work decomposition. Every coordination item (one CV of one system) is cut into
-// A tiles of TA = 8*RA atoms and B chunks of CH = 128 atoms; one step is one
-// (tile, chunk) block of TA x CH pairs. The host lists the steps tile-major
-// (CoordStep) and gives every CTA one contiguous range of them, balanced so that
-// each CTA of the persistent grid has the same number of steps (the batched
-// path lowers the share of CTAs that also evaluate hill items). A CTA walks its
-// range once: A atoms stay in registers while consecutive steps belong to the
-// same tile.
+// A tiles of TA = NW*RA atoms (NW = 16 warps, RA = 8: 128 atoms) and B chunks of
+// CH = 128 atoms; one step is one (tile, chunk) block of TA x CH pairs. The host
+// lists the steps tile-major (CoordStep) and gives every CTA of a persistent grid
+// of one 512-thread CTA per SM one contiguous range of them with the same number
+// of steps. One CTA per SM, its warps meeting at a barrier every step, keeps
+// every warp of the SM at the same pace (with two CTAs per SM the scheduler let
+// one run ahead and the other finish alone). A CTA walks its range once: A atoms
+// stay in registers while consecutive steps belong to the same tile.
 //
 // Data movement. Positions are gathered with 16-byte cp.async copies into
 // shared memory two steps ahead (double buffer), so a step computes while the
@@ -16,24 +17,27 @@
 // of a window of up to WIN steps sit in shared memory.
 //
 // Arithmetic. Coordinates are scaled by 1/r0 (A once per tile, B once per step,
-// both rounded the same way), so the pair's squared distance is x^2 directly. For the
+// both rounded the same way, never contracted), so the pair's squared distance is
+// x^2 directly and an atom present in both groups gives exactly zero. For the
 // n = 6, m = 12 switch, f = 1/(1 + x^6) and the gradient factor h = x^4 f^2 need
-// one reciprocal and no square root. The reference's lower bound r^2 >= 1e-20
-// (CommonGluedKernels.cpp:983-987) is compared on every pair; the upper bound
-// x <= 1000 (and the optional cutoff) only where the box admits such distances
-// (template flag HI).
+// one reciprocal and no square root; full steps of that switch use packed FP32
+// (f32x2) instructions, two pairs per instruction. The reference's lower bound
+// r^2 >= 1e-20 (CommonGluedKernels.cpp:983-987) is compared on every pair; the
+// upper bound x <= 1000 (and the optional cutoff) only where the box admits such
+// distances (template flag HI).
 //
 // Accumulation. Per-pair gradients h*d (scaled units) are summed in FP32 over a
-// step: per lane over its A atoms for B, per warp over lanes for A. Those step
-// sums are converted to 64-bit fixed point (value * 2^32) and added with integer
-// atomics into acc[row][3] (integer addition is exact and order-independent, so
-// the sums are bitwise reproducible and do not depend on the grid); the reader
-// multiplies by the item's scale (-n/r0 for the n = 6, m = 12 switch, 1/r0
-// otherwise), converts to FP64 and clears the rows. The CN partial of each run
-// piece (a maximal sub-run of one tile on one CTA; FP64 block sum) goes to the
-// slot the host assigned to the piece (CoordStep::pieceSlot of its last step);
-// an item's slots are contiguous and in step order, the reader sums them in that
-// order, and nothing needs clearing.
+// step: per lane over its A atoms for B, per warp over lanes for A (one butterfly
+// for all A atoms of the warp). Those sums are converted to 64-bit fixed point
+// (value * 2^32) and added with integer atomics into acc[row][3] (integer
+// addition is exact and order-independent, so the sums are bitwise reproducible
+// and do not depend on the grid); the reader multiplies by the item's scale
+// (-n/r0 for the n = 6, m = 12 switch, 1/r0 otherwise), converts to FP64 and
+// clears the rows. The CN partial of each run piece (a maximal sub-run of one
+// tile on one CTA; FP64 block sum) goes to the slot the host assigned to the
+// piece (CoordStep::pieceSlot of its last step); an item's slots are contiguous
+// and in step order, the reader sums them in that order, and nothing needs
+// clearing.
 #pragma once
 
 #include "devfn.cuh"
