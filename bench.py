@@ -379,7 +379,7 @@ def main():
                     help="profiling run: warm-up + timed steps only, fixed tiling, no baselines (for ncu)")
     ap.add_argument("--walkers", type=int, default=64, help="C4 walker count (profiling of small cases)")
     ap.add_argument("--hills", type=int, default=50000, help="C4 hill count (profiling of small cases)")
-    ap.add_argument("--tuning", default="8,0", help="fixed C4 tuning ra,finalize_parts (--profile)")
+    ap.add_argument("--tuning", default="8,0,0", help="fixed C4 tuning ra,finalize_parts,plain_finalize_launch (--profile)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -433,7 +433,7 @@ def main():
         b = Batch([force_for(w["cvs"], c4_biases(w, hill)) for w in ws], pool.walkers)
         b.set_hills(hill["centers"], hill["heights"])
         tv = [int(x) for x in args.tuning.split(",")] + [0, 0]
-        b.set_tuning(tv[0], tv[1])
+        b.set_tuning(tv[0], tv[1], tv[2])
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
         ms = time_steps(torch, lambda i: (b.update_state(i), b.execute()), args.steps, args.warmup, flush)
         print(json.dumps({"profile": "c4", "walkers": args.walkers, "hills": b.num_hills(), "ms_per_step": ms / args.steps,

@@ -173,16 +173,16 @@ class Batch:
     def tuning(self):
         t = (c_int * 4)()
         call("glued_batch_get_tuning", self._h, t)
-        return dict(ra=t[0], parts=t[1])
+        return dict(ra=t[0], parts=t[1], plain=t[2])
 
-    def set_tuning(self, ra=8, parts=0):
-        t = (c_int * 4)(ra, parts, 0, 0)
+    def set_tuning(self, ra=8, parts=0, plain=0):
+        t = (c_int * 4)(ra, parts, plain, 0)
         call("glued_batch_set_tuning", self._h, t)
 
     def autotune(self):
         t = (c_int * 4)()
         call("glued_batch_autotune", self._h, t)
-        return dict(ra=t[0], parts=t[1])
+        return dict(ra=t[0], parts=t[1], plain=t[2])
 
 
 def force_for(cvs, biases, pbc=True):

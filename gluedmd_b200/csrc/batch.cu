@@ -308,6 +308,9 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
             coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
     }
     if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
+    // the finalize (a programmatic dependent launch) may be scheduled once every
+    // CTA is here; it waits for this grid's completion before reading its output
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (hills) hillSlice(B, hs, s0 < s1, st);
     if (st) {
         __syncthreads();
@@ -381,16 +384,26 @@ __device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
     long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
     int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD];
     const size_t rowBase = (size_t)w * B.rowsPerWalker;
+    // loads that do not depend on the runs kernel: atoms of the rows, the record
 #pragma unroll
     for (int q = 0; q < ROWS_PER_THREAD; q++) {
         const int r = r0 + tid + FT * q;
-        rItem[q] = -1; rAtom[q] = 0;
+        rItem[q] = r < r1 ? 0 : -1;
+        rAtom[q] = r < r1 ? __ldg(B.rowAtom + rowBase + r) : 0;
+    }
+    copyWords(&sW, B.walkers + w, sizeof(BWalker));
+    copyWords(sSimple, B.simple + (size_t)w * B.nS, sizeof(BSimple) * B.nS);
+    copyWords(sHarm, B.harm + (size_t)w * B.nH, sizeof(BHarm) * B.nH);
+    copyWords(sItem, B.items + (size_t)w * B.nC, sizeof(CoordItem) * B.nC);
+    // launched as a programmatic dependent of the runs kernel: wait here until
+    // it has completed and its writes are visible (no-op otherwise)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < ROWS_PER_THREAD; q++) {
         vx[q] = vy[q] = vz[q] = 0;
-        if (r < r1) {
-            const unsigned long long* a = B.R.acc + 3 * (rowBase + r);
+        if (rItem[q] == 0) {
+            const unsigned long long* a = B.R.acc + 3 * (rowBase + r0 + tid + FT * q);
             vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
-            rAtom[q] = __ldg(B.rowAtom + rowBase + r);
-            rItem[q] = 0;
         }
     }
     // part 0: the hill partials of the runs CTAs (warp 2, CTA order per lane)
@@ -400,10 +413,6 @@ __device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
             const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
             hv0 += __ldcg(q); hv1 += __ldcg(q + 1); hv2 += __ldcg(q + 2);
         }
-    copyWords(&sW, B.walkers + w, sizeof(BWalker));
-    copyWords(sSimple, B.simple + (size_t)w * B.nS, sizeof(BSimple) * B.nS);
-    copyWords(sHarm, B.harm + (size_t)w * B.nH, sizeof(BHarm) * B.nH);
-    copyWords(sItem, B.items + (size_t)w * B.nC, sizeof(CoordItem) * B.nC);
     if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
     if (part == 0 && warp == 2) {
         hv0 = warpSum(hv0); hv1 = warpSum(hv1); hv2 = warpSum(hv2);
@@ -685,9 +694,21 @@ struct Batch::Impl {
         void* args[] = {&dev};
         cudaCheck(cudaLaunchKernel((const void*)runs(), dim3(grid), dim3(RUNS_THREADS), args, dynSmem(), s), "runs");
     }
+    // Programmatic dependent launch: the finalize CTAs may start as runs CTAs
+    // retire, load what does not depend on the runs, then wait in hardware
+    // (griddepcontrol.wait) for the runs grid to complete.
     void launchFinalize(cudaStream_t s) {
-        void* args[] = {&dev};
-        cudaCheck(cudaLaunchKernel((const void*)k_batch_finalize, dim3(W * parts), dim3(FT), args, 0, s), "finalize");
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(W * parts);
+        cfg.blockDim = dim3(FT);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = tune.plain ? 0 : 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaCheck(cudaLaunchKernelEx(&cfg, k_batch_finalize, dev), "finalize");
     }
     // The step's launches on stream s: coordination runs, then the finalize.
     void launch(cudaStream_t s) {
@@ -882,7 +903,7 @@ void Batch::setStream(cudaStream_t s) {
 void Batch::setTuning(const BatchTuning& t) {
     if (t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 8");
     if (t.parts < 0 || t.parts > 4096) throw Error(GLUED_E_INVALID, "batch tuning: finalize parts must be 0..4096");
-    if (t.reserved != 0) throw Error(GLUED_E_INVALID, "batch tuning: tune[2] is reserved and must be 0");
+    if (t.plain != 0 && t.plain != 1) throw Error(GLUED_E_INVALID, "batch tuning: finalize launch mode must be 0 or 1");
     cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
     impl_->tune = t;
     impl_->plan();
@@ -916,8 +937,9 @@ void Batch::execute() {
     I.ready = true;
 }
 
-// Autotuner: the finalize CTAs per walker are timed on the live walkers with
-// CUDA events (forces go to a scratch buffer) and the fastest is kept.
+// Autotuner: the finalize CTAs per walker and its launch mode are timed on the
+// live walkers with CUDA events (forces go to a scratch buffer) and the fastest
+// combination is kept.
 BatchTuning Batch::autotune() {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
@@ -933,9 +955,10 @@ BatchTuning Batch::autotune() {
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
     const int base = I.minParts();
-    for (int mul : {1, 2, 4}) {
+    for (int plain : {0, 1})
+        for (int mul : {1, 2, 4}) {
             BatchTuning t;
-            t.ra = 8; t.parts = base * mul;
+            t.ra = 8; t.parts = base * mul; t.plain = plain;
             I.tune = t;
             I.plan();
             for (int r = 0; r < 2; r++) I.launch(I.stream);

@@ -14,7 +14,8 @@ struct BatchTuning {
     int ra = 8;       // A atoms per thread in the coordination tile (TA = 16 * ra)
     int parts = 0;    // finalize CTAs per walker (0: the fewest that cover its
                       // coordination rows)
-    int reserved = 0; // must be 0
+    int plain = 0;    // 1: finalize as a plain stream-ordered launch; 0: as a
+                      // programmatic dependent launch of the runs kernel
 };
 
 class Batch {

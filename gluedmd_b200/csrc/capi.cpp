@@ -360,7 +360,7 @@ int glued_batch_set_tuning(glued_batch* b, const int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t;
-        t.ra = tune[0]; t.parts = tune[1]; t.reserved = tune[2];
+        t.ra = tune[0]; t.parts = tune[1]; t.plain = tune[2];
         b->b->setTuning(t);
     });
 }
@@ -368,14 +368,14 @@ int glued_batch_get_tuning(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t = b->b->tuning();
-        tune[0] = t.ra; tune[1] = t.parts; tune[2] = 0; tune[3] = 0;
+        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = 0;
     });
 }
 int glued_batch_autotune(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch");
         glued::BatchTuning t = b->b->autotune();
-        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = 0; tune[3] = 0; }
+        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = 0; }
     });
 }
 int glued_batch_execute(glued_batch* b) {

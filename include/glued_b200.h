@@ -253,9 +253,11 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
 /* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
- * fewest that cover the walker's coordination rows), 0, 0}. autotune times the
- * candidates on the live walkers (forces of the trial launches go to a scratch
- * buffer), keeps the fastest and returns it in tune (synchronizing).          */
+ * fewest that cover the walker's coordination rows), finalize launch (0: a
+ * programmatic dependent launch of the runs kernel, 1: a plain stream-ordered
+ * launch), 0}. autotune times the candidates on the live walkers (forces of the
+ * trial launches go to a scratch buffer), keeps the fastest and returns it in
+ * tune (synchronizing).                                                        */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);

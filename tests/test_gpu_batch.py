@@ -50,14 +50,15 @@ def _oracle(w, biases, hill):
     return s
 
 
-@pytest.mark.parametrize("parts", [0, 5])
+@pytest.mark.parametrize("parts,plain", [(0, 0), (5, 0), (0, 1)])
 @pytest.mark.parametrize("with_hills", [False, True])
-def test_batch_matches_fp64_oracle(with_hills, parts):
-    """The batched step against the FP64 oracle, with the fewest finalize parts
-    per walker and with more parts than rows need."""
+def test_batch_matches_fp64_oracle(with_hills, parts, plain):
+    """The batched step against the FP64 oracle: the fewest finalize parts per
+    walker and more parts than rows need, finalize as a programmatic dependent
+    launch and as a plain launch."""
     ws, hill = _walkers()
     b, walkers, specs = _setup(ws, hill, with_hills)
-    b.set_tuning(8, parts)
+    b.set_tuning(8, parts, plain)
     for wk in walkers:
         wk.force.zero_()
     b.execute()
