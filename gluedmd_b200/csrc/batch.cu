@@ -354,9 +354,11 @@ __device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
 }
 
 constexpr int MAXCOORD = 8;   // coordination CVs per walker
+constexpr int HPU = 8;        // hill partials per lane loaded at a time
 
 struct FinSmem {
     double sCV[MAXCV], sdU[MAXCV];
+    double tE[MAXHARM], tdU[MAXHARM];   // harmonic terms: energy, dU/dCV
     F3 sJac[MAXSIMPLE * 4];
     double sHill[3];
     // the walker's record: one round of independent loads
@@ -406,12 +408,22 @@ __device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
             vx[q] = (long long)__ldcg(a); vy[q] = (long long)__ldcg(a + 1); vz[q] = (long long)__ldcg(a + 2);
         }
     }
-    // part 0: the hill partials of the runs CTAs (warp 2, CTA order per lane)
+    // part 0: the hill partials of the runs CTAs (warp 2; lane l sums CTAs l,
+    // l + 32, ... in that order, HPU of them loaded at a time)
     double hv0 = 0.0, hv1 = 0.0, hv2 = 0.0;
     if (part == 0 && hb.present && warp == 2)
-        for (int c = lane; c < B.hillParts; c += 32) {
-            const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
-            hv0 += __ldcg(q); hv1 += __ldcg(q + 1); hv2 += __ldcg(q + 2);
+        for (int c0 = lane; c0 < B.hillParts; c0 += 32 * HPU) {
+            double a0[HPU], a1[HPU], a2[HPU];
+#pragma unroll
+            for (int u = 0; u < HPU; u++) {
+                const int c = c0 + 32 * u;
+                const double* q = B.hillPart + 3 * ((size_t)c * B.W + w);
+                a0[u] = c < B.hillParts ? __ldcg(q) : 0.0;
+                a1[u] = c < B.hillParts ? __ldcg(q + 1) : 0.0;
+                a2[u] = c < B.hillParts ? __ldcg(q + 2) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < HPU; u++) { hv0 += a0[u]; hv1 += a1[u]; hv2 += a2[u]; }
         }
     if (tid < MAXCV) { sCV[tid] = 0.0; sdU[tid] = 0.0; }
     if (part == 0 && warp == 2) {
@@ -450,14 +462,25 @@ __device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
     }
     __syncthreads();
     if (st && tid == 0) st[2] = globalTimer();
-    // dU/dCN (coordination CVs); part 0: all CVs, energies
+    // dU/dCN (coordination CVs); part 0: all CVs, energies. Lane k of warp 0
+    // evaluates harmonic term k; lane 0 adds them in term order.
+    if (warp == 0) {
+        if (lane < B.nH) {
+            const BHarm& hm = sHarm[lane];
+            bool coordCv = false;
+            for (int c = 0; c < B.nC; c++) coordCv = coordCv || sItem[c].cv == hm.cv;
+            double e = 0.0, du = 0.0;
+            if (part == 0 || coordCv) du = harmonicDU(hm, sCV[hm.cv], e);
+            fs.tE[lane] = e;
+            fs.tdU[lane] = du;
+        }
+        __syncwarp();
+    }
     if (tid == 0) {
         double E = 0.0;
         for (int k = 0; k < B.nH; k++) {
-            const BHarm& hm = sHarm[k];
-            bool coordCv = false;
-            for (int c = 0; c < B.nC; c++) coordCv = coordCv || sItem[c].cv == hm.cv;
-            if (part == 0 || coordCv) sdU[hm.cv] += harmonicDU(hm, sCV[hm.cv], E);
+            E += fs.tE[k];
+            sdU[sHarm[k].cv] += fs.tdU[k];
         }
         if (part == 0) {
             if (hb.present) {

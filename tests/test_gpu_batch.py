@@ -27,9 +27,11 @@ def _setup(ws, hill, with_hills=True, coord_restraint=True):
     for w in ws:
         cn0 = W.coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"]) if coord_restraint else None
         # restraint centres away from the current values, so that dU/dCV is not a
-        # difference of nearly equal numbers (forces would be pure rounding noise)
+        # difference of nearly equal numbers (forces would be pure rounding noise);
+        # the coordination centre 1% + 2 away, so that the CN error of FP32 pair
+        # sums (~1e-8 relative for a CN of ~1e4) is not amplified by k / (CN - CN0)
         wr = dict(w, d0=w["d0"] + 0.05)
-        biases = c4_biases(wr, hill["params"], hill["iparams"], cn0=None if cn0 is None else cn0 + 2.0)
+        biases = c4_biases(wr, hill["params"], hill["iparams"], cn0=None if cn0 is None else cn0 * 1.01 + 2.0)
         if not with_hills:
             biases = [b for b in biases if b[0] != 103]
         forces.append(force_for(w["cvs"], biases))
@@ -50,13 +52,14 @@ def _oracle(w, biases, hill):
     return s
 
 
-@pytest.mark.parametrize("parts,plain", [(0, 0), (5, 0), (0, 1)])
+@pytest.mark.parametrize("coord,parts,plain", [((64, 256), 0, 0), ((64, 256), 5, 1), ((900, 1500), 0, 0)])
 @pytest.mark.parametrize("with_hills", [False, True])
-def test_batch_matches_fp64_oracle(with_hills, parts, plain):
-    """The batched step against the FP64 oracle: the fewest finalize parts per
-    walker and more parts than rows need, finalize as a programmatic dependent
-    launch and as a plain launch."""
-    ws, hill = _walkers()
+def test_batch_matches_fp64_oracle(with_hills, coord, parts, plain):
+    """The batched step against the FP64 oracle: full coordination tiles with
+    the fewest finalize parts per walker (programmatic dependent launch) and
+    with more parts than rows need (plain launch), and ragged tiles (partial A
+    tiles and B chunks, 2,400 rows per walker over five finalize parts)."""
+    ws, hill = _walkers(coord=coord)
     b, walkers, specs = _setup(ws, hill, with_hills)
     b.set_tuning(8, parts, plain)
     for wk in walkers:
