@@ -16,6 +16,7 @@
 //            thread, so the deposit is deterministic.
 #include "devfn.cuh"
 #include "kernels.hpp"
+#include "pdl.cuh"
 #include "force.hpp"
 
 namespace glued {
@@ -68,6 +69,7 @@ __device__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* sG, d
 // {dV/ds_0..7 terms, value}; k_biases sums the partials in CTA order.
 __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__ biases,
                                                       const double* __restrict__ cvv, double* __restrict__ part) {
+    pdlEnter();
     __shared__ double red[32 * 9];
     const BiasDev& b = biases[blockIdx.y];
     if (b.type != BIAS_OPES && b.type != BIAS_METAD_HILLS) return;  // uniform over the CTA
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
                                                  const double* __restrict__ cvv, int numCVs,
                                                  const double* __restrict__ testGrad, double* __restrict__ dUdCV,
                                                  double* __restrict__ energies, const double* __restrict__ sumPart) {
+    pdlEnter();
     extern __shared__ double sG[];
     __shared__ double red[32 * 9];
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -202,6 +205,7 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
 
 __global__ void k_scatter(JacDev J, const int* __restrict__ u2g, const double* __restrict__ dUdCV,
                           unsigned long long* __restrict__ force, int padded) {
+    pdlEnter();
     const double S = 4294967296.0;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.rows; r += gridDim.x * blockDim.x) {
         double g = dUdCV[J.cv[r]];
@@ -282,9 +286,9 @@ __global__ void k_hills_deposit(const BiasDev* __restrict__ bp, const double* __
 
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums) {
-    if (kernelSums && !testGrad && nb > 0) k_kernel_sums<<<dim3(KSUM_CTAS, nb), 256, 0, s>>>(biases, cvv, sumPart);
+    if (kernelSums && !testGrad && nb > 0) launchPdl(k_kernel_sums, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
     size_t smem = sizeof(double) * (size_t)(numCVs > 0 ? numCVs : 1);
-    k_biases<<<1, 512, smem, s>>>(biases, nb, cvv, numCVs, testGrad, dUdCV, energies, sumPart);
+    launchPdl(k_biases, dim3(1), dim3(512), smem, s, biases, nb, cvv, numCVs, testGrad, dUdCV, energies, sumPart);
 }
 
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
@@ -292,7 +296,7 @@ void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double
     if (J.rows <= 0) return;
     int blocks = (J.rows + 255) / 256;
     if (blocks > 1184) blocks = 1184;
-    k_scatter<<<blocks, 256, 0, s>>>(J, u2g, dUdCV, reinterpret_cast<unsigned long long*>(force), padded);
+    launchPdl(k_scatter, dim3(blocks), dim3(256), 0, s, J, u2g, dUdCV, reinterpret_cast<unsigned long long*>(force), padded);
 }
 
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies) {

@@ -30,6 +30,7 @@
 #include "context.hpp"
 #include "coord_run.cuh"
 #include "kernels.hpp"
+#include "pdl.cuh"
 
 namespace glued {
 
@@ -38,6 +39,7 @@ namespace glued {
 // static limit).
 template <int RA, int BOX, int NH, bool HI>
 __global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
+    pdlEnter();
     extern __shared__ __align__(16) unsigned char dsm[];
     CoordRunSmem<RA>& sm = *reinterpret_cast<CoordRunSmem<RA>*>(dsm);
     const int s0 = R.begin[blockIdx.x], s1 = R.begin[blockIdx.x + 1];
@@ -48,6 +50,7 @@ __global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
 // every accumulator read is cleared; CN values = sums of the run pieces' partials
 // in step order.
 __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* __restrict__ cvv, int totalRows) {
+    pdlEnter();
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid < 3 * totalRows) {
         const int comp = gid % 3;
@@ -105,6 +108,7 @@ template <int RA, int BOX, int NH, bool HI>
 static void launchRun(cudaStream_t s, int grid, const CoordRunDev& R) {
     const size_t dyn = sizeof(CoordRunSmem<RA>);
     runKernelSetup((const void*)k_coord_run<RA, BOX, NH, HI>, dyn);
+    // plain launch: the persistent grid fills every SM, nothing to overlap
     k_coord_run<RA, BOX, NH, HI><<<grid, COORD_NW * 32, dyn, s>>>(R);
 }
 
@@ -130,7 +134,7 @@ void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, i
     }
     if (parts & 2) {
         const int n = std::max(3 * totalRows, numItems);
-        k_coord_finalize<<<(n + 255) / 256, 256, 0, s>>>(R, numItems, J, cvv, totalRows);
+        launchPdl(k_coord_finalize, dim3((n + 255) / 256), dim3(256), 0, s, R, numItems, J, cvv, totalRows);
     }
 }
 

@@ -14,6 +14,7 @@
 #include "context.hpp"
 #include "devfn.cuh"
 #include "kernels.hpp"
+#include "pdl.cuh"
 #include "force.hpp"
 
 namespace glued {
@@ -29,6 +30,7 @@ __global__ void k_invert_index(const int* __restrict__ atomIndex, int* __restric
 __global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restrict__ u2g,
                              const SimpleItem* __restrict__ items, int n, const BoxDev* __restrict__ boxp,
                              double* __restrict__ cvv, JacDev J) {
+    pdlEnter();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const BoxDev box = *boxp;
@@ -116,6 +118,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
                                                              const int* __restrict__ u2g, GroupDev G,
                                                              const BoxDev* __restrict__ boxp,
                                                              double* __restrict__ cvv, JacDev J) {
+    pdlEnter();
     extern __shared__ float4 sPos[];
     __shared__ double red[32 * 16];
     __shared__ float wbuf[128];
@@ -390,7 +393,7 @@ void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n) {
 
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
                      const BoxDev* box, double* cvv, const JacDev& J) {
-    if (n > 0) k_simple_cvs<<<(n + 127) / 128, 128, 0, s>>>(posq, u2g, items, n, box, cvv, J);
+    if (n > 0) launchPdl(k_simple_cvs, dim3((n + 127) / 128), dim3(128), 0, s, posq, u2g, items, n, box, cvv, J);
 }
 
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
@@ -403,7 +406,7 @@ void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const Gr
                                        (int)(sizeof(float4) * GROUP_CACHE)), "group CV shared memory");
         attr = true;
     }
-    k_group_cvs<<<G.numItems, GROUP_THREADS, smem, s>>>(posq, u2g, G, box, cvv, J);
+    launchPdl(k_group_cvs, dim3(G.numItems), dim3(GROUP_THREADS), smem, s, posq, u2g, G, box, cvv, J);
 }
 
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
