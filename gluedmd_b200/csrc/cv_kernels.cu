@@ -132,16 +132,24 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
     const bool cached = it.type != CV_CONTACTMAP && a1 - a0 <= GROUP_CACHE;
     if (cached) {
         const int n = a1 - a0;
+        // masses (COM distance, gyration) ride in the .w lane of the cache
+        const bool withMass = it.type == CV_COM_DISTANCE || it.type == CV_GYRATION;
         for (int base = tid; base < n; base += nt * GATHER_U) {
             int slot[GATHER_U];
+            float m[GATHER_U];
 #pragma unroll
             for (int u = 0; u < GATHER_U; u++) {
                 const int j = base + nt * u;
                 slot[u] = j < n ? __ldg(G.slots + a0 + j) : -1;
+                m[u] = (withMass && j < n) ? __ldg(G.mass + a0 + j) : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < GATHER_U; u++)
-                if (slot[u] >= 0) sPos[base + nt * u] = __ldg(posq + slot[u]);
+                if (slot[u] >= 0) {
+                    float4 p = __ldg(posq + slot[u]);
+                    p.w = m[u];
+                    sPos[base + nt * u] = p;
+                }
         }
         __syncthreads();
     }
@@ -149,12 +157,13 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         if (cached) { const float4 p = sPos[j - a0]; return f3(p.x, p.y, p.z); }
         return loadPos(posq, nullptr, G.slots[j]);
     };
+    auto massAt = [&](int j) -> float { return cached ? sPos[j - a0].w : G.mass[j]; };
 
     if (it.type == CV_COM_DISTANCE) {
         double v[6] = {0, 0, 0, 0, 0, 0};
         for (int j = it.s0 + tid; j < it.s2; j += nt) {
             F3 p = pos(j);
-            double m = G.mass[j];
+            double m = massAt(j);
             int o = j < it.s1 ? 0 : 3;
             v[o] += m * p.x; v[o + 1] += m * p.y; v[o + 2] += m * p.z;
         }
@@ -168,7 +177,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         if (tid == 0) cvv[it.cv] = (double)dist;
         for (int j = it.s0 + tid; j < it.s2; j += nt) {
             bool g1 = j < it.s1;
-            float w = G.mass[j] / (g1 ? it.f0 : it.f1);
+            float w = massAt(j) / (g1 ? it.f0 : it.f1);
             float s = g1 ? -inv * w : inv * w;
             int r = it.jac0 + j;
             J.gx[r] = d.x * s; J.gy[r] = d.y * s; J.gz[r] = d.z * s;
@@ -177,7 +186,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         double v[3] = {0, 0, 0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 p = pos(j);
-            double m = G.mass[j];
+            double m = massAt(j);
             v[0] += m * p.x; v[1] += m * p.y; v[2] += m * p.z;
         }
         blockSum<3>(v, red);
@@ -186,7 +195,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         double q[1] = {0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 d = minImage(sub3(pos(j), com), box);
-            q[0] += (double)G.mass[j] * (double)dot3(d, d);
+            q[0] += (double)massAt(j) * (double)dot3(d, d);
         }
         blockSum<1>(q, red);
         float rg = (float)sqrt(q[0] / (double)it.f0);
@@ -194,12 +203,13 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         if (tid == 0) cvv[it.cv] = (double)rg;
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 d = minImage(sub3(pos(j), com), box);
-            float w = G.mass[j] / it.f0;
+            float w = massAt(j) / it.f0;
             int r = it.jac0 + j;
             J.gx[r] = w * d.x * irg; J.gy[r] = w * d.y * irg; J.gz[r] = w * d.z * irg;
         }
     } else if (it.type == CV_RMSD) {
         double q[1] = {0};
+#pragma unroll 4
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 p = pos(j);
             F3 d = f3(p.x - G.ref[3 * j], p.y - G.ref[3 * j + 1], p.z - G.ref[3 * j + 2]);
@@ -210,6 +220,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         float rmsd = (float)sqrt(q[0] / na);
         float sc = (rmsd > 1e-10f ? 1.0f / rmsd : 0.0f) / (float)na;
         if (tid == 0) cvv[it.cv] = (double)rmsd;
+#pragma unroll 4
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 p = pos(j);
             int r = it.jac0 + j;
@@ -218,6 +229,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         }
     } else if (it.type == CV_PCA) {
         double q[1] = {0};
+#pragma unroll 4
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
             F3 p = pos(j);
             float dx = p.x - G.ref[3 * j], dy = p.y - G.ref[3 * j + 1], dz = p.z - G.ref[3 * j + 2];
