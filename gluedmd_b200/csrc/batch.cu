@@ -44,7 +44,8 @@ constexpr int RUNS_THREADS = COORD_NW * 32;   // threads of a runs CTA (one CTA 
 constexpr int WBLK = 64;       // walkers per hill pass
 constexpr int JW = WBLK / COORD_NW;   // walker slots per warp in a hill pass
 static_assert(JW * COORD_NW == WBLK && 3 * JW <= 32, "hill walker slots");
-constexpr int HS = 256;        // hills staged in shared memory at a time
+constexpr int HS = 512;        // hills staged in shared memory at a time (a slice of the
+                               // 50,000-hill table over 148 CTAs is 338)
 }  // namespace
 
 struct BWalker {
