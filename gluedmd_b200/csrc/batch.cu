@@ -58,7 +58,8 @@ struct BWalker {
 struct BSimple { int type; int cv; int atoms[4]; };
 struct BHarm { int cv; float k, at; int periodic; };
 struct BHill {
-    float4* mirror;
+    float* mirror;      // [3][cap]: scaled x, scaled y, height of every hill
+    int cap;            // maxH rounded up to a multiple of 4
     double* centers;
     double* heights;
     int* count;
@@ -125,12 +126,15 @@ __device__ __forceinline__ void scatterRow(unsigned long long* F, int P, int ato
 // slice of the table, HS hills at a time, and the atoms' positions), which land
 // while that step computes. Arithmetic: CVs and hill centres are stored scaled
 // by u = sqrt(log2(e) / (2 sigma^2)) per dimension (the mirror table holds
-// scaled centres), so a hill is exp2(-(dx^2 + dy^2)) of scaled differences;
-// warp w takes walkers w, w + 8, ... (8 at a time in registers), lane l takes
-// hills l, l + 32, ...; FP32 sums per lane, a fixed butterfly over the lanes,
-// one FP64 partial per (CTA, walker), summed by the finalize in CTA order.
+// scaled centres, as three arrays x, y, height), so a hill is
+// exp2(-(dx^2 + dy^2)) of scaled differences; slices start on multiples of 4
+// hills so that they move in 16-byte copies. Warp w takes walkers w, w + 16,
+// ... (JW at a time in registers), lane l takes the hill pairs (2p, 2p+1),
+// p = l, l + 32, ..., in packed FP32 (f32x2: two hills per instruction); FP32
+// sums per lane, a fixed butterfly over the lanes, one FP64 partial per (CTA,
+// walker), summed by the finalize in CTA order.
 struct HillStage {
-    float4 hills[HS];
+    float hx[HS], hy[HS], hh[HS];   // the staged chunk: scaled centres, heights
     float4 pos[WBLK * 8];
     BoxDev box[WBLK];
     const float4* ptr[WBLK * 8];
@@ -138,10 +142,11 @@ struct HillStage {
     float sS[WBLK * 2];
 };
 
-__device__ __forceinline__ void hillSliceRange(const BatchDev& B, const HillStage& hs, int& h0, int& h1) {
-    const int count = hs.count[0];
-    h0 = (int)((long long)count * blockIdx.x / gridDim.x);
-    h1 = (int)((long long)count * (blockIdx.x + 1) / gridDim.x);
+// This CTA's hill groups (4 hills each) [g0, g1) of the table.
+__device__ __forceinline__ void hillSliceRange(const BatchDev& B, const HillStage& hs, int& g0, int& g1) {
+    const int groups = (hs.count[0] + 3) / 4;
+    g0 = (int)((long long)groups * blockIdx.x / gridDim.x);
+    g1 = (int)((long long)groups * (blockIdx.x + 1) / gridDim.x);
 }
 
 // Tables of walker block wb: count, atom addresses, boxes (no dependent loads).
@@ -158,11 +163,17 @@ __device__ void hillStageTables(const BatchDev& B, int wb, HillStage& hs) {
     if (threadIdx.x == 0) cpAsync16(hs.count, B.hill.count, true);
 }
 
-// hills [k0, k0 + HS) of the slice (zero past h1)
-__device__ __forceinline__ void hillStageHills(const BatchDev& B, int k0, int h1, HillStage& hs) {
-    for (int t = threadIdx.x; t < HS; t += blockDim.x) {
-        const int k = k0 + t;
-        cpAsync16(&hs.hills[t], B.hill.mirror + (k < h1 ? k : 0), k < h1);
+// Hill groups [c0, min(g1, c0 + HS / 4)) into the chunk arrays; the bytes past
+// the table's count and the rest of the chunk are zero (height 0).
+__device__ __forceinline__ void hillStageHills(const BatchDev& B, const HillStage& hs, int c0, int g1) {
+    const int count = hs.count[0];
+    const int ng = min(g1 - c0, HS / 4);
+    for (int t = threadIdx.x; t < 3 * (HS / 4); t += blockDim.x) {
+        const int c = t / (HS / 4), g = t % (HS / 4);
+        const int k = 4 * (c0 + g);
+        const int bytes = g < ng ? 4 * max(0, min(4, count - k)) : 0;
+        const float* d = c == 0 ? hs.hx : c == 1 ? hs.hy : hs.hh;
+        cpAsyncBytes(const_cast<float*>(d) + 4 * g, B.hill.mirror + (size_t)c * B.hill.cap + (bytes ? k : 0), bytes);
     }
 }
 
@@ -170,12 +181,12 @@ __device__ __forceinline__ void hillStageHills(const BatchDev& B, int k0, int h1
 // hills of the slice and the atoms' positions of walker block wb.
 __device__ void hillStageData(const BatchDev& B, int wb, HillStage& hs) {
     const int w0 = wb * WBLK, nw = min(WBLK, B.W - w0);
-    int h0, h1;
-    hillSliceRange(B, hs, h0, h1);
-    hillStageHills(B, h0, h1, hs);
+    int g0, g1;
+    hillSliceRange(B, hs, g0, g1);
+    hillStageHills(B, hs, g0, g1);
     for (int t = threadIdx.x; t < nw * 8; t += blockDim.x) {
         const float4* a = hs.ptr[t];
-        cpAsync16(&hs.pos[t], a ? a : B.hill.mirror, a != nullptr);
+        cpAsync16(&hs.pos[t], a ? a : reinterpret_cast<const float4*>(B.hill.mirror), a != nullptr);
     }
 }
 
@@ -195,34 +206,48 @@ __device__ void hillCVs(const BatchDev& B, int wb, HillStage& hs) {
     }
 }
 
-// Hills lane + 32 q (q < nq) of the staged chunk against the JW walkers of this
-// warp; acc[3 j + c]: sum of g, g dx, g dy for walker slot j.
+// The hill pairs p = lane, lane + 32, ... (< np) of the staged chunk against the
+// JW walkers of this warp, two hills per packed instruction; acc[j][c]: packed
+// partial sums of g, g dx, g dy for walker slot j.
 template <bool P0, bool P1>
-__device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int nq, const float (&s0)[JW],
-                                         const float (&s1)[JW], float (&acc)[32]) {
+__device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int np, const float (&s0)[JW],
+                                         const float (&s1)[JW], unsigned long long (&acc)[JW][3]) {
     constexpr float R = 12582912.0f;   // 1.5 * 2^23: adding and removing it rounds to an integer
     const int lane = threadIdx.x & 31;
-    for (int q = 0; q < nq; q++) {
-        const float4 hk = hs.hills[lane + 32 * q];   // height 0 past the slice
+    const unsigned long long R2 = f2::pk(R, R);
+    const unsigned long long ip0 = f2::pk(hb.ipS[0], hb.ipS[0]), np0 = f2::pk(-hb.pS[0], -hb.pS[0]);
+    const unsigned long long ip1 = f2::pk(hb.ipS[1], hb.ipS[1]), np1 = f2::pk(-hb.pS[1], -hb.pS[1]);
+    unsigned long long sx[JW], sy[JW];
+#pragma unroll
+    for (int j = 0; j < JW; j++) { sx[j] = f2::pk(s0[j], s0[j]); sy[j] = f2::pk(s1[j], s1[j]); }
+    const unsigned long long* hx2 = reinterpret_cast<const unsigned long long*>(hs.hx);
+    const unsigned long long* hy2 = reinterpret_cast<const unsigned long long*>(hs.hy);
+    const unsigned long long* hh2 = reinterpret_cast<const unsigned long long*>(hs.hh);
+    for (int p = lane; p < np; p += 32) {
+        const unsigned long long hx = hx2[p], hy = hy2[p], hh = hh2[p];   // height 0 past the slice
 #pragma unroll
         for (int j = 0; j < JW; j++) {
-            float dx = s0[j] - hk.x, dy = s1[j] - hk.y;
-            if (P0) dx = fmaf(-(fmaf(dx, hb.ipS[0], R) - R), hb.pS[0], dx);
-            if (P1) dy = fmaf(-(fmaf(dy, hb.ipS[1], R) - R), hb.pS[1], dy);
-            const float ex = fmaf(dx, dx, dy * dy);
-            float e;
-            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-ex));
-            const float g = ex <= hb.cut ? hk.z * e : 0.0f;
-            acc[3 * j] += g;
-            acc[3 * j + 1] = fmaf(g, dx, acc[3 * j + 1]);
-            acc[3 * j + 2] = fmaf(g, dy, acc[3 * j + 2]);
+            unsigned long long dx = f2::sub(sx[j], hx), dy = f2::sub(sy[j], hy);
+            if (P0) dx = f2::fma(f2::sub(f2::fma(dx, ip0, R2), R2), np0, dx);
+            if (P1) dy = f2::fma(f2::sub(f2::fma(dy, ip1, R2), R2), np1, dy);
+            const unsigned long long ex = f2::fma(dx, dx, f2::mul(dy, dy));
+            float ea, eb, ga, gb;
+            f2::upk(ex, ea, eb);
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ga) : "f"(-ea));
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(gb) : "f"(-eb));
+            ga = ea <= hb.cut ? ga : 0.0f;
+            gb = eb <= hb.cut ? gb : 0.0f;
+            const unsigned long long g = f2::mul(hh, f2::pk(ga, gb));
+            acc[j][0] = f2::add(acc[j][0], g);
+            acc[j][1] = f2::fma(g, dx, acc[j][1]);
+            acc[j][2] = f2::fma(g, dy, acc[j][2]);
         }
     }
 }
 
 // This CTA's hill slice for every walker. `gathered`: the data of walker block
 // 0 was issued during the coordination steps.
-__device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, unsigned long long* st) {
+__device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool cvsDone, unsigned long long* st) {
     const BHill& hb = B.hill;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nWB = (B.W + WBLK - 1) / WBLK;
@@ -242,34 +267,48 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, unsig
         cpAsyncWaitAll();
         __syncthreads();
         if (st && wb == 0 && threadIdx.x == 0) st[3] = globalTimer();
-        hillCVs(B, wb, hs);
-        __syncthreads();
-        int h0, h1;
-        hillSliceRange(B, hs, h0, h1);
-        float s0[JW], s1[JW], acc[32];
+        if (wb > 0 || !cvsDone) {
+            hillCVs(B, wb, hs);
+            __syncthreads();
+        }
+        int g0, g1;
+        hillSliceRange(B, hs, g0, g1);
+        float s0[JW], s1[JW];
 #pragma unroll
         for (int j = 0; j < JW; j++) {
             const int wl = min(warp + COORD_NW * j, nw - 1);
             s0[j] = hs.sS[wl * 2]; s1[j] = hs.sS[wl * 2 + 1];
         }
+        unsigned long long pacc[JW][3];
 #pragma unroll
-        for (int k = 0; k < 32; k++) acc[k] = 0.0f;
-        for (int k0 = h0; k0 < h1; k0 += HS) {
-            if (k0 != h0) {
+        for (int j = 0; j < JW; j++) pacc[j][0] = pacc[j][1] = pacc[j][2] = 0ull;
+        for (int c0 = g0; c0 < g1; c0 += HS / 4) {
+            if (c0 != g0) {
                 __syncthreads();
-                hillStageHills(B, k0, h1, hs);
+                hillStageHills(B, hs, c0, g1);
                 cpAsyncCommit();
                 cpAsyncWaitAll();
                 __syncthreads();
             }
-            const int nq = (min(HS, h1 - k0) + 31) / 32;
+            const int np = 2 * min(g1 - c0, HS / 4);   // hill pairs staged
             const bool p0 = hb.pS[0] > 0.0f, p1 = hb.pS[1] > 0.0f;
-            if (p0 && p1) hillEval<true, true>(hs, hb, nq, s0, s1, acc);
-            else if (p0) hillEval<true, false>(hs, hb, nq, s0, s1, acc);
-            else if (p1) hillEval<false, true>(hs, hb, nq, s0, s1, acc);
-            else hillEval<false, false>(hs, hb, nq, s0, s1, acc);
+            if (p0 && p1) hillEval<true, true>(hs, hb, np, s0, s1, pacc);
+            else if (p0) hillEval<true, false>(hs, hb, np, s0, s1, pacc);
+            else if (p1) hillEval<false, true>(hs, hb, np, s0, s1, pacc);
+            else hillEval<false, false>(hs, hb, np, s0, s1, pacc);
         }
         if (st && wb == 0 && threadIdx.x == 0) st[4] = globalTimer();
+        float acc[32];
+#pragma unroll
+        for (int j = 0; j < JW; j++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float a, b;
+                f2::upk(pacc[j][c], a, b);
+                acc[3 * j + c] = a + b;
+            }
+#pragma unroll
+        for (int k = 3 * JW; k < 32; k++) acc[k] = 0.0f;
         const float v = warpTransposeSum32(acc);   // lane 3 j + c: component c of walker slot j
         const int j = lane / 3, c = lane - 3 * j;
         const int wl = warp + COORD_NW * j;
@@ -301,10 +340,13 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
     if (s0 < s1) {
         if (hills)
-            coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook(), [&]() {
-                hillStageData(B, 0, hs);
-                cpAsyncCommit();
-            });
+            coordRun<RA, BOX, NH, HI>(
+                B.R, s0, s1, sm, NoPieceHook(),
+                [&]() {
+                    hillStageData(B, 0, hs);
+                    cpAsyncCommit();
+                },
+                [&]() { hillCVs(B, 0, hs); });   // read after the barriers of the hill slice
         else
             coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
     }
@@ -312,7 +354,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     // the finalize (a programmatic dependent launch) may be scheduled once every
     // CTA is here; it waits for this grid's completion before reading its output
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    if (hills) hillSlice(B, hs, s0 < s1, st);
+    if (hills) hillSlice(B, hs, s0 < s1, s0 < s1, st);
     if (st) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -557,7 +599,9 @@ __global__ void k_batch_deposit(BatchDev B) {
         for (int d = 0; d < hb.D; d++) c[d] = B.cvv[(size_t)w * B.nCV + hb.cv[d]];
         for (int d = 0; d < hb.D; d++) hb.centers[(size_t)k * hb.D + d] = c[d];
         hb.heights[k] = h;
-        hb.mirror[k] = make_float4((float)(c[0] * hb.u[0]), (float)(c[1] * hb.u[1]), (float)h, 0.0f);
+        hb.mirror[k] = (float)(c[0] * hb.u[0]);
+        hb.mirror[hb.cap + k] = (float)(c[1] * hb.u[1]);
+        hb.mirror[2 * hb.cap + k] = (float)h;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -892,11 +936,12 @@ Batch::Batch(const std::vector<const GluedForce*>& forces, const glued_walker_de
             h.ipS[d] = per ? (float)(1.0 / (L * u)) : 0.0f;
         }
         if (h.maxH < 1) throw Error(GLUED_E_INVALID, "batch: METAD_HILLS maxHills must be >= 1");
-        I.hMirror.alloc(sizeof(float4) * (size_t)h.maxH);
+        h.cap = (h.maxH + 3) / 4 * 4;
+        I.hMirror.alloc(sizeof(float) * 3 * (size_t)h.cap);
         I.hCenters.alloc(sizeof(double) * (size_t)h.maxH * D);
         I.hHeights.alloc(sizeof(double) * (size_t)h.maxH);
         I.hCount.alloc(sizeof(int) * 4);
-        h.mirror = I.hMirror.as<float4>(); h.centers = I.hCenters.as<double>();
+        h.mirror = I.hMirror.as<float>(); h.centers = I.hCenters.as<double>();
         h.heights = I.hHeights.as<double>(); h.count = I.hCount.as<int>();
     }
     I.walkersD.upload(I.walkersH);
@@ -1131,14 +1176,19 @@ void Batch::setHills(const double* centers, const double* heights, int n) {
     if (n < 0 || n > I.hill.maxH) throw Error(GLUED_E_INVALID, "batch: hill count out of range");
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
     const int D = I.hill.D;
-    std::vector<float4> m(n);
-    for (int k = 0; k < n; k++)
-        m[k] = make_float4((float)(centers[k * D] * I.hill.u[0]), D > 1 ? (float)(centers[k * D + 1] * I.hill.u[1]) : 0.0f,
-                           (float)heights[k], 0.0f);
+    const int cap = I.hill.cap;
+    std::vector<float> m((size_t)3 * cap, 0.0f);
+    for (int k = 0; k < n; k++) {
+        m[k] = (float)(centers[k * D] * I.hill.u[0]);
+        m[cap + k] = D > 1 ? (float)(centers[k * D + 1] * I.hill.u[1]) : 0.0f;
+        m[2 * (size_t)cap + k] = (float)heights[k];
+    }
     if (n > 0) {
         cudaCheck(cudaMemcpy(I.hill.centers, centers, sizeof(double) * (size_t)n * D, cudaMemcpyHostToDevice), "hills");
         cudaCheck(cudaMemcpy(I.hill.heights, heights, sizeof(double) * n, cudaMemcpyHostToDevice), "hills");
-        cudaCheck(cudaMemcpy(I.hill.mirror, m.data(), sizeof(float4) * n, cudaMemcpyHostToDevice), "hills");
+        for (int c = 0; c < 3; c++)
+            cudaCheck(cudaMemcpy(I.hill.mirror + (size_t)c * cap, m.data() + (size_t)c * cap, sizeof(float) * n,
+                                 cudaMemcpyHostToDevice), "hills");
     }
     cudaCheck(cudaMemcpy(I.hill.count, &n, sizeof(int), cudaMemcpyHostToDevice), "hills");
 }

@@ -72,6 +72,11 @@ __device__ __forceinline__ void cpAsync16(void* dst, const void* src, bool valid
     unsigned n = valid ? 16u : 0u;
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smemU32(dst)), "l"(src), "r"(n) : "memory");
 }
+// 16-byte global -> shared copy of which the first `bytes` (0..16, multiple of
+// 4) are read and the rest written as zeros.
+__device__ __forceinline__ void cpAsyncBytes(void* dst, const void* src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smemU32(dst)), "l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -311,10 +316,12 @@ struct NoStartHook {
 // called once by all threads when the copies issued before the call and those
 // of the first two steps have landed (after a barrier), before the first step
 // computes: cp.async copies it issues land while that step computes and are
-// complete after its end-of-step wait.
-template <int RA, int BOX, int NH, bool HI, class Hook, class Start = NoStartHook>
+// complete after its end-of-step wait. AfterFirst() is called once by all
+// threads right after the first step's end-of-step barrier (everything Start()
+// issued has landed and is visible).
+template <int RA, int BOX, int NH, bool HI, class Hook, class Start = NoStartHook, class AfterFirst = NoStartHook>
 __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook,
-                         const Start& start = Start()) {
+                         const Start& start = Start(), const AfterFirst& afterFirst = AfterFirst()) {
     using namespace crun;
     static_assert(RA % 2 == 0 && 3 * RA <= 32, "A atoms per warp");
     constexpr int TA = NW * RA;
@@ -460,6 +467,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             }
             cpAsyncWaitAll();
             __syncthreads();
+            if (s == s0) afterFirst();
             if (ls + 2 < nw) issue(ls + 2, ib2, ia2, pq2);
             // B sums over warps in fixed order
             for (int v = tid; v < CH * 3; v += blockDim.x) {
