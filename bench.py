@@ -44,51 +44,84 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+_CLOCK_SAMPLER = r"""
+import sys, time, pynvml
+pynvml.nvmlInit()
+bus, idx, out = sys.argv[1], int(sys.argv[2]), sys.argv[3]
+try:
+    h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+except Exception:
+    h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+with open(out, "w", buffering=1) as f:
+    while True:
+        t = time.time()
+        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        f.write(f"{t:.6f} {sm} {mx} {rs}\n")
+        time.sleep(0.001)
+"""
+
+
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+    """SM clocks and throttle reasons sampled during timing by a separate sampler
+    process (NVML every millisecond, independent of this process's GIL; the GPU is
+    matched to the CUDA device by PCI bus id). Only samples taken between the
+    start and the end of the timed region are summarised; the raw samples are
+    kept in gpurun_out/clocks_<pid>.txt (time, SM MHz, max SM MHz, reason bits)."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
     def __init__(self, index=0):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.csv"
+        self.t0 = self.t1 = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.txt") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.txt"
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import torch
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            if os.path.exists(self.path):
+                os.remove(self.path)
+            self.proc = subprocess.Popen([sys.executable, "-c", _CLOCK_SAMPLER, bus, str(self.index), self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            t = time.time()
+            while time.time() - t < 10.0:
+                if os.path.exists(self.path) and os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *a):
+        self.t1 = time.time()
         if self.proc:
+            time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-            self.fh.close()
 
     def summary(self):
+        rows = []
         try:
-            rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            for line in open(self.path).read().splitlines():
+                f = line.split()
+                if len(f) == 4 and self.t0 <= float(f[0]) <= self.t1:
+                    rows.append((int(f[1]), int(f[2]), int(f[3])))
         except Exception:
             rows = []
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i].strip() == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({name for r in rows for bit, name in self.REASONS.items() if r[2] & bit})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": float(max(r[1] for r in rows)),
+                "reasons": reasons, "samples": len(rows), "source": "NVML every 1 ms in a sampler process"}
 
 
 # ----------------------------------------------------------------- workloads
