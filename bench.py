@@ -218,6 +218,162 @@ def run_single(args, torch, cfg):
     return info
 
 
+def c5_inputs(torch, dtype):
+    """C5: the 30,000-atom contact map (10,000 pairs) + 50-frame path CV with a
+    2-D hill sum of 2,000 hills on (CMAP, s): centres spread over the current CV
+    values +- 3 sigma (seed 2), heights U[0.2, 1.2]; all four tensors on the
+    device, differentiable."""
+    from gluedmd_b200 import workloads as W
+    from gluedmd_b200.autograd import BiasTopology, cv_values
+    w = W.config5()
+    pos, pairs, r0 = w.positions, w.extra["pairs"], w.extra["r0"]
+    patoms, frames, lam = w.extra["patoms"], w.extra["frames"], w.extra["lam"]
+    K = 2000
+    nmw = np.c_[r0, np.full(len(r0), 6.0), np.full(len(r0), 12.0), np.ones(len(r0))]
+    sigma = (0.02 * max(1.0, len(r0) / 40.0), 0.35)
+
+    def dev(x):
+        return torch.tensor(np.asarray(x), dtype=dtype, device="cuda", requires_grad=True)
+
+    topo0 = BiasTopology.build(pairs, nmw, patoms, lam, np.zeros((K, 2)), sigma)
+    _, cm, s_, _ = cv_values(dev(pos), dev(r0), dev(frames), dev(np.ones(K)), topo0)
+    rng = np.random.default_rng(2)
+    centers = np.c_[cm + rng.uniform(-3, 3, K) * sigma[0], s_ + rng.uniform(-3, 3, K) * sigma[1]]
+    heights = rng.uniform(0.2, 1.2, K)
+    topo = BiasTopology.build(pairs, nmw, patoms, lam, centers, sigma)
+    return w, topo, [dev(pos), dev(r0), dev(frames), dev(heights)], dict(
+        pairs=pairs, r0=r0, patoms=patoms, frames=frames, lam=lam, centers=centers, heights=heights, sigma=sigma)
+
+
+C5_KERNELS_PER_STEP = 5   # forward: pair partials, path + hills; backward: pairs, path, hills + convert (+ one memset node)
+
+
+def run_c5(args, torch):
+    """C5 through the library's C ABI: glued_ad_forward + glued_ad_backward (dL/dE
+    = 1) on preallocated device buffers, captured once in a CUDA graph; one step
+    = one replay (energy, forces and the gradients w.r.t. r0, frames and hill
+    heights). The autograd wrapper (gluedmd_b200.autograd.glued_bias) issues the
+    same two calls; its result is compared with the graph's once."""
+    import ctypes
+    from ctypes import c_void_p
+    from gluedmd_b200._native import call
+    from gluedmd_b200.autograd import _spec, glued_bias
+    w, topo, (p, r, f, h), raw = c5_inputs(torch, torch.float32)
+    pd, rd, fd, hd = (t.detach() for t in (p, r, f, h))
+    out = torch.empty(7 + fd.shape[0], dtype=torch.float64, device="cuda")
+    n_part = max(1, min(1184, (topo.pairs.shape[0] + 255) // 256))
+    part = torch.empty(n_part, dtype=torch.float64, device="cuda")
+    gE = torch.ones(1, dtype=torch.float64, device="cuda")
+    acc = torch.empty(3 * pd.shape[0], dtype=torch.int64, device="cuda")
+    gp, gr, gf, gh = (torch.empty_like(t) for t in (pd, rd, fd, hd))
+    spec = _spec(topo, pd, rd, fd, hd)
+
+    def enqueue(stream):
+        call("glued_ad_forward", 0, c_void_p(stream), ctypes.byref(spec), c_void_p(out.data_ptr()),
+             c_void_p(part.data_ptr()), n_part)
+        call("glued_ad_backward", 0, c_void_p(stream), ctypes.byref(spec), c_void_p(out.data_ptr()),
+             c_void_p(gE.data_ptr()), c_void_p(acc.data_ptr()), c_void_p(gp.data_ptr()), c_void_p(gr.data_ptr()),
+             c_void_p(gf.data_ptr()), c_void_p(gh.data_ptr()))
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        enqueue(side.cuda_stream)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        enqueue(torch.cuda.current_stream().cuda_stream)
+    # the graph's result against the autograd wrapper's
+    graph.replay()
+    glued_bias(p, r, f, h, topo).backward()
+    torch.cuda.synchronize()
+    diff = float((gp - p.grad).abs().max() / p.grad.abs().max().clamp_min(1e-30))
+    if not diff < 1e-6:
+        raise RuntimeError(f"C5 graph and autograd forces differ: {diff:.3e}")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step(i):
+        graph.replay()
+
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms = time_steps(torch, step, args.steps, args.warmup, flush)
+    us = ms * 1e3 / args.steps
+    # e2e: positions from pinned host memory, energy and forces back to the host
+    host_pos = torch.tensor(w.positions, dtype=torch.float32).pin_memory()
+    host_f = torch.empty_like(host_pos).pin_memory()
+    host_e = torch.empty(1, dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def e2e_step(i):
+        pd.copy_(host_pos, non_blocking=True)
+        graph.replay()
+        host_f.copy_(gp, non_blocking=True)
+        host_e.copy_(out[:1], non_blocking=True)
+
+    for i in range(args.warmup):
+        e2e_step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        e2e_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_us = e0.elapsed_time(e1) * 1e3 / args.steps
+    return dict(us_per_step=us, e2e_us=e2e_us, clocks=clk.summary(), raw=raw, w=w,
+                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 4 + 8))
+
+
+def c5_raw_from_oracle():
+    """The C5 inputs for the reference arm: hill centres placed around the FP64
+    oracle's CV values (the GPU arm places them around its own)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from gluedmd_b200 import workloads as W
+    w = W.config5()
+    pairs, r0, patoms, frames, lam = (w.extra[k] for k in ("pairs", "r0", "patoms", "frames", "lam"))
+    P = len(pairs)
+    cm_params = [v for i in range(P) for v in (r0[i], 6.0, 12.0, 1.0)]
+    cvs = [(O.CV_CONTACTMAP, [int(x) for x in pairs.ravel()], cm_params),
+           (O.CV_PATH, [int(x) for x in patoms], [lam, len(frames)] + list(np.asarray(frames).ravel()))]
+    cvv, _ = O.OracleSystem(cvs, mode="f64", num_particles=len(w.positions),
+                            test_bias_gradients=[0.0, 0.0, 0.0]).evaluate_cvs(w.positions)
+    K = 2000
+    sigma = (0.02 * max(1.0, P / 40.0), 0.35)
+    rng = np.random.default_rng(2)
+    centers = np.c_[cvv[0] + rng.uniform(-3, 3, K) * sigma[0], cvv[1] + rng.uniform(-3, 3, K) * sigma[1]]
+    heights = rng.uniform(0.2, 1.2, K)
+    return w, dict(pairs=pairs, r0=r0, patoms=patoms, frames=np.asarray(frames), lam=lam, centers=centers,
+                   heights=heights, sigma=sigma)
+
+
+def cpu_baseline_c5(w, raw, budget_s=12.0):
+    """The oracle's FP64 restatement of the C5 step on one host thread: CVs, the
+    hill sum's dE/dCV, the chain rule to forces; bounded sample of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    P = len(raw["pairs"])
+    cm_params = [v for i in range(P) for v in (raw["r0"][i], 6.0, 12.0, 1.0)]
+    cvs = [(O.CV_CONTACTMAP, [int(x) for x in raw["pairs"].ravel()], cm_params),
+           (O.CV_PATH, [int(x) for x in raw["patoms"]], [raw["lam"], len(raw["frames"])] + list(raw["frames"].ravel()))]
+    sysm = O.OracleSystem(cvs, mode="f64", num_particles=len(w.positions), test_bias_gradients=[0.0, 0.0, 0.0])
+    c, hgt, sg = raw["centers"], raw["heights"], raw["sigma"]
+    n = 0
+    t0 = time.perf_counter()
+    while n < 1 or time.perf_counter() - t0 < budget_s and n < 50:
+        cvv, _ = sysm.evaluate_cvs(w.positions)
+        d0, d1 = cvv[0] - c[:, 0], cvv[1] - c[:, 1]
+        g = hgt * np.exp(-d0 ** 2 / (2 * sg[0] ** 2) - d1 ** 2 / (2 * sg[1] ** 2))
+        sysm.test_grad = np.array([(-g * d0 / sg[0] ** 2).sum(), (-g * d1 / sg[1] ** 2).sum(), 0.0])
+        sysm.execute(w.positions)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": dt / n * 1e6, "unit": "us/step", "cores": 1, "kind": "port",
+            "sample": f"{n} steps of the C5 workload on one host thread (FP64 oracle: CVs twice per step, "
+                      f"hill-sum dE/dCV in numpy)"}
+
+
 def cpu_baseline_single(cfg, w, budget_s=12.0):
     """Reference kernels compiled for the host (oracle/_ref) when present, else the
     oracle's FP32 restatement; bounded sample of steps on one host thread."""
@@ -405,7 +561,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -435,6 +591,14 @@ def main():
                                            "harmonic restraints, shared 50,000-hill WT MetaD"},
                     "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "walker-steps/s",
                                                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        elif args.config == "c5":
+            w, raw = c5_raw_from_oracle()
+            cb = cpu_baseline_c5(w, raw, budget_s=max(5.0, 0.5 * args.steps))
+            line = {"impl": "reference", "metric": "CV+bias+force us/step", "value": cb["value"], "unit": "us/step",
+                    "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                    "dtype": "f64", "data": "synthetic", "config": {"workload": "C5"},
+                    "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "us/step", "h2d_bytes_per_step": 0,
+                                                "d2h_bytes_per_step": 0}}
         else:
             from gluedmd_b200 import workloads as W
             w = {"c1": lambda: W.config1("grid"), "c2": W.config2, "c3": W.config3}[args.config]()
@@ -513,6 +677,33 @@ def main():
                                          "launches_per_step": info["plain_launches"],
                                          "speedup_batched_vs_plain": info["plain_ms"] / info["step_ms"]},
                 "status": info["status"], "peaks_source": src,
+            }
+            print(json.dumps(line))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    if args.config == "c5":
+        info = run_c5(args, torch)
+        us = max_over_ranks(info["us_per_step"])
+        if dist is not None:
+            dist.barrier()
+        if rank == 0:
+            cb = None
+            if not args.no_cpu_baseline and world == 1:
+                cb = cpu_baseline_c5(info["w"], info["raw"])
+            line = {
+                "metric": "CV+bias+force us/step", "value": us, "unit": "us/step", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": us / 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "C5: 30,000 atoms, contact map 10,000 pairs + path CV 50 frames x 500 atoms, "
+                                       "2-D hill sum (2,000 hills); forward + backward (forces and the gradients "
+                                       "w.r.t. r0, frames and hill heights) through the C ABI, one CUDA graph",
+                           "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+                "e2e": {"value": info["e2e_us"], "unit": "us/step", "h2d_bytes_per_step": info["h2d"],
+                        "d2h_bytes_per_step": info["d2h"]},
+                "gpu_launches": C5_KERNELS_PER_STEP * args.steps,
+                "roofline": None, "cpu_baseline": cb, "clocks": info["clocks"], "peaks_source": src,
             }
             print(json.dumps(line))
         if dist is not None:
