@@ -55,42 +55,51 @@ __device__ __forceinline__ void pairGeom(const AdSpec& S, int p, R& d, R dr[3]) 
 
 // out: [0] E, [1] CMAP, [2] s, [3] z, [4] S, [5..5+F) w_f; part: per-CTA CMAP partials
 template <class R>
-__global__ void k_ad_cmap(AdSpec S, double* part) {
+// CTAs [0, nPart): contact-map partial sums over the pairs; CTAs nPart + f: the
+// mean-square deviation sum of path frame f (path atoms gathered, frame
+// coordinates streamed coalesced), written to out[5 + f], where
+// k_ad_path_hills turns it into the frame weight. Spreading the frames over
+// CTAs keeps enough loads in flight to stream the frames from DRAM.
+__global__ void k_ad_cmap(AdSpec S, double* part, int nPart, double* out) {
     __shared__ double red[32];
     double acc = 0.0;
-    const R* r0 = static_cast<const R*>(S.r0);
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S.nPairs; p += gridDim.x * blockDim.x) {
-        R d, dr[3];
-        pairGeom<R>(S, p, d, dr);
-        R x = d / r0[p], f, dfdx;
-        ratioSwitchT<R>(x, (int)S.nmw[3 * p], (int)S.nmw[3 * p + 1], f, dfdx);
-        acc += (double)((R)S.nmw[3 * p + 2] * f);
+    if (blockIdx.x < nPart) {
+        const R* r0 = static_cast<const R*>(S.r0);
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S.nPairs; p += nPart * blockDim.x) {
+            R d, dr[3];
+            pairGeom<R>(S, p, d, dr);
+            R x = d / r0[p], f, dfdx;
+            ratioSwitchT<R>(x, (int)S.nmw[3 * p], (int)S.nmw[3 * p + 1], f, dfdx);
+            acc += (double)((R)S.nmw[3 * p + 2] * f);
+        }
+        double v[1] = {acc};
+        blockSum<1>(v, red);
+        if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    } else {
+        const int f = blockIdx.x - nPart;
+        const R* pos = static_cast<const R*>(S.pos);
+        const R* fr = static_cast<const R*>(S.frames) + (size_t)f * S.M * 3;
+#pragma unroll 4
+        for (int i = threadIdx.x; i < 3 * S.M; i += blockDim.x) {
+            const int a = S.pathAtoms[i / 3];
+            const R dx = pos[3 * a + i % 3] - fr[i];
+            acc += (double)(dx * dx);
+        }
+        double v[1] = {acc};
+        blockSum<1>(v, red);
+        if (threadIdx.x == 0) out[5 + f] = v[0];
     }
-    double v[1] = {acc};
-    blockSum<1>(v, red);
-    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
 template <class R>
-__global__ void k_ad_path_hills(AdSpec S, const double* part, int nPart, double* out) {
+__global__ void __launch_bounds__(512) k_ad_path_hills(AdSpec S, const double* part, int nPart, double* out) {
     __shared__ double red[32 * 3];
     __shared__ double sw[128];
     __shared__ double bc[4];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const R* pos = static_cast<const R*>(S.pos);
-    const R* fr = static_cast<const R*>(S.frames);
-    for (int f = warp; f < S.F; f += nw) {
-        double acc = 0.0;
-        for (int j = lane; j < S.M; j += 32) {
-            int a = S.pathAtoms[j];
-            for (int c = 0; c < 3; c++) {
-                R dx = pos[3 * a + c] - fr[((size_t)f * S.M + j) * 3 + c];
-                acc += (double)(dx * dx);
-            }
-        }
-        acc = warpSum(acc);
-        if (lane == 0) sw[f] = exp(-S.lambda * acc / S.M);
-    }
+    const int tid = threadIdx.x;
+    // frame weights from the frame MSD sums of k_ad_cmap
+    for (int f = tid; f < S.F; f += blockDim.x) sw[f] = exp(-S.lambda * out[5 + f] / S.M);
+    __syncthreads();
     if (tid == 0) {
         double cm = 0;
         for (int k = 0; k < nPart; k++) cm += part[k];
@@ -182,7 +191,7 @@ __global__ void k_ad_back_hills_and_convert(AdSpec S, const double* out, const d
 
 template <class R>
 void adForwardT(cudaStream_t st, const AdSpec& S, double* out, double* part, int nPart) {
-    k_ad_cmap<R><<<nPart, 256, 0, st>>>(S, part);
+    k_ad_cmap<R><<<nPart + S.F, 256, 0, st>>>(S, part, nPart, out);
     k_ad_path_hills<R><<<1, 512, 0, st>>>(S, part, nPart, out);
 }
 
