@@ -17,6 +17,7 @@
 
 #include <algorithm>
 
+#include "pdl.cuh"
 #include "../../include/glued_b200.h"
 #include "context.hpp"
 #include "devfn.cuh"
@@ -61,6 +62,7 @@ template <class R>
 // k_ad_path_hills turns it into the frame weight. Spreading the frames over
 // CTAs keeps enough loads in flight to stream the frames from DRAM.
 __global__ void k_ad_cmap(AdSpec S, double* part, int nPart, double* out) {
+    pdlEnter();
     __shared__ double red[32];
     double acc = 0.0;
     if (blockIdx.x < nPart) {
@@ -93,6 +95,7 @@ __global__ void k_ad_cmap(AdSpec S, double* part, int nPart, double* out) {
 
 template <class R>
 __global__ void __launch_bounds__(512) k_ad_path_hills(AdSpec S, const double* part, int nPart, double* out) {
+    pdlEnter();
     __shared__ double red[32 * 3];
     __shared__ double sw[128];
     __shared__ double bc[4];
@@ -133,6 +136,7 @@ __global__ void __launch_bounds__(512) k_ad_path_hills(AdSpec S, const double* p
 // gE: device scalar dL/dE. Position gradient accumulates into fixed-point acc.
 template <class R>
 __global__ void k_ad_back_pairs(AdSpec S, const double* out, const double* gE, long long* acc, R* gR0) {
+    pdlEnter();
     const R* r0 = static_cast<const R*>(S.r0);
     const double gC = gE[0] * out[5 + S.F];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < S.nPairs; p += gridDim.x * blockDim.x) {
@@ -156,6 +160,7 @@ __global__ void k_ad_back_pairs(AdSpec S, const double* out, const double* gE, l
 
 template <class R>
 __global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, long long* acc, R* gFrames) {
+    pdlEnter();
     const R* pos = static_cast<const R*>(S.pos);
     const R* fr = static_cast<const R*>(S.frames);
     const double gS = gE[0] * out[6 + S.F];
@@ -180,6 +185,7 @@ __global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, lo
 template <class R>
 __global__ void k_ad_back_hills_and_convert(AdSpec S, const double* out, const double* gE, const long long* acc,
                                             R* gPos, R* gH) {
+    pdlEnter();
     const double cm = out[1], s = out[2];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.K; k += gridDim.x * blockDim.x) {
         double d0 = cm - S.hillC[2 * k], d1 = s - S.hillC[2 * k + 1];
@@ -191,8 +197,8 @@ __global__ void k_ad_back_hills_and_convert(AdSpec S, const double* out, const d
 
 template <class R>
 void adForwardT(cudaStream_t st, const AdSpec& S, double* out, double* part, int nPart) {
-    k_ad_cmap<R><<<nPart + S.F, 256, 0, st>>>(S, part, nPart, out);
-    k_ad_path_hills<R><<<1, 512, 0, st>>>(S, part, nPart, out);
+    launchPdl(k_ad_cmap<R>, dim3(nPart + S.F), dim3(256), 0, st, S, part, nPart, out);
+    launchPdl(k_ad_path_hills<R>, dim3(1), dim3(512), 0, st, S, static_cast<const double*>(part), nPart, out);
 }
 
 template <class R>
@@ -200,11 +206,12 @@ void adBackwardT(cudaStream_t st, const AdSpec& S, const double* out, const doub
                  void* gR0, void* gFrames, void* gH) {
     cudaCheck(cudaMemsetAsync(acc, 0, sizeof(long long) * 3 * (size_t)S.nAtoms, st), "memset");
     int bp = (S.nPairs + 255) / 256;
-    if (bp > 0) k_ad_back_pairs<R><<<bp, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gR0));
+    if (bp > 0) launchPdl(k_ad_back_pairs<R>, dim3(bp), dim3(256), 0, st, S, out, gE, acc, static_cast<R*>(gR0));
     int bf = (S.M * S.F + 255) / 256;
-    if (bf > 0) k_ad_back_path<R><<<bf, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gFrames));
+    if (bf > 0) launchPdl(k_ad_back_path<R>, dim3(bf), dim3(256), 0, st, S, out, gE, acc, static_cast<R*>(gFrames));
     int bc = (std::max(S.K, 3 * S.nAtoms) + 255) / 256;
-    k_ad_back_hills_and_convert<R><<<bc, 256, 0, st>>>(S, out, gE, acc, static_cast<R*>(gPos), static_cast<R*>(gH));
+    launchPdl(k_ad_back_hills_and_convert<R>, dim3(bc), dim3(256), 0, st, S, out, gE, static_cast<const long long*>(acc),
+              static_cast<R*>(gPos), static_cast<R*>(gH));
 }
 
 void adForward(int dtype, cudaStream_t st, const AdSpec& S, double* out, double* part, int nPart) {
