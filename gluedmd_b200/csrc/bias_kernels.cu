@@ -14,6 +14,8 @@
 //            pass the reference's exponent <= 8 test (CommonGluedKernels.cpp:
 //            3645-3680 scans the whole grid); each grid point is written by one
 //            thread, so the deposit is deterministic.
+#include <algorithm>
+
 #include "devfn.cuh"
 #include "kernels.hpp"
 #include "pdl.cuh"
@@ -61,6 +63,52 @@ __device__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* sG, d
     }
     energies[b.slot] = V;
     for (int d = 0; d < D; d++) sG[b.cvIdx[d]] += dV[d] * b.invSp[d];
+}
+
+// PBMETAD (CommonGluedKernels.cpp:3694-3760), one thread: sub-grid d is a 1-D
+// grid over CV cvIdx[d], linearly interpolated (periodic wrap or clamp, as the
+// MetaD grid); the sub-grid energies V_d combine as
+// E = -kT (ln sum_d exp((Vmin - V_d)/kT) - ln N) + Vmin, and dE/ds_d = w_d dV_d/ds_d
+// with the softmax weights w_d = exp((Vmin - V_d)/kT) / sum. V_d and w_d are kept
+// in pbState for the deposit.
+__device__ void evalPbmetad(const BiasDev& b, const double* cvv, double* sG, double* energies) {
+    const int N = b.D;
+    double V[8], G[8];
+    for (int d = 0; d < N; d++) {
+        const double* g = b.grid + b.goff[d];
+        const int n = b.npts[d];
+        double fr = (cvv[b.cvIdx[d]] - b.origin[d]) * b.invSp[d];
+        int lo, hi;
+        double al;
+        if (b.per[d]) {
+            fr = fr - floor(fr / (double)n) * (double)n;
+            if (fr < 0.0) fr += n;
+            lo = (int)fr;
+            if (lo >= n) lo = n - 1;
+            al = fr - lo;
+            hi = (lo + 1) % n;
+        } else {
+            if (fr < 0.0) fr = 0.0;
+            if (fr > (double)(n - 1)) fr = (double)(n - 1);
+            lo = (int)fr;
+            if (lo >= n - 1) lo = n - 2;
+            al = fr - lo;
+            hi = lo + 1;
+        }
+        V[d] = g[lo] * (1.0 - al) + g[hi] * al;
+        G[d] = (g[hi] - g[lo]) * b.invSp[d];
+    }
+    double vmin = V[0];
+    for (int d = 1; d < N; d++) vmin = V[d] < vmin ? V[d] : vmin;
+    double ene = 0.0;
+    for (int d = 0; d < N; d++) ene += exp((vmin - V[d]) / b.kT);
+    energies[b.slot] = -b.kT * (log(ene) - log((double)N)) + vmin;
+    for (int d = 0; d < N; d++) {
+        const double w = exp((vmin - V[d]) / b.kT) / ene;
+        b.pbState[d] = V[d];
+        b.pbState[N + d] = w;
+        sG[b.cvIdx[d]] += w * G[d];
+    }
 }
 
 // Kernel sums of the OPES and hill-sum MetaD biases (CommonGluedKernels.cpp:2642-2700
@@ -147,6 +195,11 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
                     energies[b.slot] = V;
                 }
             } else if (b.type == BIAS_METAD) {
+                if (tid == 0) evalMetadGrid(b, cvv, sG, energies);
+            } else if (b.type == BIAS_PBMETAD) {
+                if (tid == 0) evalPbmetad(b, cvv, sG, energies);
+            } else if (b.type == BIAS_EXTERNAL) {
+                // user grid, evaluated as the MetaD grid (CommonBiasKernels.cpp:425-488)
                 if (tid == 0) evalMetadGrid(b, cvv, sG, energies);
             } else if (b.type == BIAS_OPES) {
                 // CommonGluedKernels.cpp:2642-2723.
@@ -297,6 +350,36 @@ void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double
     int blocks = (J.rows + 255) / 256;
     if (blocks > 1184) blocks = 1184;
     launchPdl(k_scatter, dim3(blocks), dim3(256), 0, s, J, u2g, dUdCV, reinterpret_cast<unsigned long long*>(force), padded);
+}
+
+// PBMETAD deposit (CommonGluedKernels.cpp:3765-3797): sub-grid d receives a
+// Gaussian at the current value of its CV with height w_d h0 exp(-V_d hif)
+// (w_d h0 without well-tempering), V_d and w_d from the last evaluation,
+// wherever the exponent is <= 8.
+__global__ void k_pbmetad_deposit(const BiasDev* __restrict__ bp, const double* __restrict__ cvv) {
+    const BiasDev& b = *bp;
+    for (int d = 0; d < b.D; d++) {
+        const double Vi = b.pbState[d], wi = b.pbState[b.D + d];
+        const double height = b.hif > 0.0 ? wi * b.h0 * exp(-Vi * b.hif) : wi * b.h0;
+        const double center = cvv[b.cvIdx[d]];
+        double* g = b.grid + b.goff[d];
+        const double s2 = 2.0 * b.sigma[d] * b.sigma[d];
+        for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < b.npts[d]; idx += gridDim.x * blockDim.x) {
+            const double pos = b.origin[d] + (double)idx / b.invSp[d];
+            double dc = pos - center;
+            if (b.per[d]) {
+                const double period = (double)b.npts[d] / b.invSp[d];
+                dc -= round(dc / period) * period;
+            }
+            const double ex = dc * dc / s2;
+            if (ex <= 8.0) g[idx] += height * exp(-ex);
+        }
+    }
+}
+
+void launchPbmetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, int maxPoints) {
+    const int blocks = std::max(1, std::min(148, (maxPoints + 255) / 256));
+    k_pbmetad_deposit<<<blocks, 256, 0, s>>>(b, cvv);
 }
 
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies) {

@@ -94,6 +94,8 @@ int biasEvalRank(int t) {
         case BIAS_HARMONIC: return 0;
         case BIAS_OPES: return 2;
         case BIAS_METAD: return 4;
+        case BIAS_PBMETAD: return 5;
+        case BIAS_EXTERNAL: return 6;
         case BIAS_METAD_HILLS: return 20;
         default: return 100;
     }
@@ -398,10 +400,11 @@ void Context::setupBiases(const GluedForce& f) {
     std::map<int, int> typeCount;
     for (int b = 0; b < nb; b++) {
         const BiasSpec& s = f.bias(b);
-        if (s.type != BIAS_HARMONIC && s.type != BIAS_METAD && s.type != BIAS_OPES && s.type != BIAS_METAD_HILLS)
+        if (s.type != BIAS_HARMONIC && s.type != BIAS_METAD && s.type != BIAS_OPES && s.type != BIAS_METAD_HILLS &&
+            s.type != BIAS_PBMETAD && s.type != BIAS_EXTERNAL)
             throw Error(GLUED_E_UNSUPPORTED, "GluedForce bias " + std::to_string(b) + ": type " + std::to_string(s.type) +
                                                  " is outside this library's hot path (supported: HARMONIC, METAD, "
-                                                 "OPES, METAD_HILLS)");
+                                                 "PBMETAD, OPES, EXTERNAL, METAD_HILLS)");
         if (s.cvs.empty() || s.cvs.size() > 8)
             throw Error(GLUED_E_INVALID, "GluedForce bias " + std::to_string(b) + ": needs 1..8 CVs");
     }
@@ -456,6 +459,60 @@ void Context::setupBiases(const GluedForce& f) {
             d.total = total;
             d.hif = gamma <= 1.0 ? 0.0 : 1.0 / ((gamma - 1.0) * kT);
             hb.grid.alloc(sizeof(double) * total);
+            d.grid = hb.grid.as<double>();
+        } else if (d.type == BIAS_PBMETAD) {
+            // N 1-D sub-grids (CommonBiasKernels.cpp:298-424):
+            // params [h0, gamma, kT, sigma_0, origin_0, max_0, sigma_1, ...],
+            // iparams [pace, bins_0, periodic_0, bins_1, periodic_1, ...]
+            needP(3 + 3 * D); needI(1 + 2 * D);
+            d.h0 = p[0];
+            const double gamma = p[1], kT = p[2];
+            d.gamma = gamma; d.kT = kT;
+            d.pace = ip[0];
+            d.hif = gamma <= 1.0 ? 0.0 : 1.0 / ((gamma - 1.0) * kT);
+            int total = 0;
+            for (int k = 0; k < D; k++) {
+                d.sigma[k] = p[3 + 3 * k];
+                const double lo = p[4 + 3 * k], hi = p[5 + 3 * k];
+                const int bins = ip[1 + 2 * k];
+                if (bins < 1) throw Error(GLUED_E_INVALID, "PBMETAD: bins must be >= 1");
+                if (!(hi > lo)) throw Error(GLUED_E_INVALID, "PBMETAD: max must exceed origin");
+                d.per[k] = ip[2 + 2 * k];
+                d.origin[k] = lo;
+                d.invSp[k] = bins / (hi - lo);
+                d.npts[k] = bins + (d.per[k] ? 0 : 1);
+                d.goff[k] = total;
+                total += d.npts[k];
+            }
+            d.total = total;
+            hb.grid.alloc(sizeof(double) * total);
+            d.grid = hb.grid.as<double>();
+            // last sub-grid energies 0, softmax weights 1/N (CommonBiasKernels.cpp:319-323)
+            std::vector<double> st(2 * D, 0.0);
+            for (int k = 0; k < D; k++) st[D + k] = 1.0 / D;
+            hb.dbls.upload(st);
+            d.pbState = hb.dbls.as<double>();
+            hb.subDeposited.assign(D, 0);
+        } else if (d.type == BIAS_EXTERNAL) {
+            // user grid, no deposition (CommonBiasKernels.cpp:425-488):
+            // params [origin_0.., max_0.., grid values], iparams [bins_0.., periodic_0..]
+            needP(2 * D); needI(2 * D);
+            if (D > 3) throw Error(GLUED_E_INVALID, "EXTERNAL grid supports at most 3 CVs (CommonGluedKernels.cpp:3589)");
+            for (int k = 0; k < D; k++) {
+                const double lo = p[k], hi = p[D + k];
+                const int bins = ip[k];
+                if (bins < 1) throw Error(GLUED_E_INVALID, "EXTERNAL: bins must be >= 1");
+                d.per[k] = ip[D + k];
+                d.origin[k] = lo;
+                d.invSp[k] = bins / (hi - lo);
+                d.npts[k] = bins + (d.per[k] ? 0 : 1);
+            }
+            d.strides[0] = 1;
+            for (int k = 1; k < D; k++) d.strides[k] = d.strides[k - 1] * d.npts[k - 1];
+            d.total = d.strides[D - 1] * d.npts[D - 1];
+            needP(2 * D + (size_t)d.total);
+            std::vector<double> g(p.begin() + 2 * D, p.begin() + 2 * D + d.total);
+            hb.grid.upload(g);
             d.grid = hb.grid.as<double>();
         } else if (d.type == BIAS_METAD_HILLS) {
             needP(3 + 3 * D); needI(2 + D);
@@ -716,7 +773,9 @@ void Context::updateState(int step) {
     if (step == lastUpdateStep_) return;
     bool any = false;
     for (auto& hb : biases_)
-        if (hb.spec.type == BIAS_OPES || hb.spec.type == BIAS_METAD || hb.spec.type == BIAS_METAD_HILLS) any = true;
+        if (hb.spec.type == BIAS_OPES || hb.spec.type == BIAS_METAD || hb.spec.type == BIAS_METAD_HILLS ||
+            hb.spec.type == BIAS_PBMETAD)
+            any = true;
     if (!any) return;
     lastUpdateStep_ = step;
     requireBound();
@@ -739,6 +798,16 @@ void Context::updateState(int step) {
             launches_ += 1;
             hb.numDeposited++;
         }
+    }
+    // PBMETAD after MetaD (CommonGluedKernels.cpp:5147-5155)
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_PBMETAD) continue;
+        if (step == 0 || step % hb.dev.pace != 0) continue;
+        int maxPoints = 0;
+        for (int k = 0; k < hb.dev.D; k++) maxPoints = std::max(maxPoints, hb.dev.npts[k]);
+        launchPbmetadDeposit(stream_, biasDev_.as<BiasDev>() + hb.depositIndex, cvv, maxPoints);
+        launches_ += 1;
+        for (auto& n : hb.subDeposited) n++;
     }
     for (auto& hb : biases_) {
         if (hb.spec.type == BIAS_METAD_HILLS) {
@@ -855,8 +924,9 @@ std::vector<float> Context::kernelSigmas(int opesIndex) {
 }
 
 // ------------------------------------------------------- bias-state blob
-// 'GPUS' v1 layout of platforms/common/src/CommonSerialization.cpp:20-177. Only
-// OPES and METAD carry state in this library; the counts of the other reference
+// 'GPUS' v1 layout of platforms/common/src/CommonSerialization.cpp:20-177. OPES,
+// METAD and PBMETAD carry state in this library; EXTERNAL is written as its count
+// only (its grid is fixed at construction); the counts of the other reference
 // sections are written as 0 so a reference reader accepts the blob. State of the
 // hill-sum extension follows the reference sections under its own 'HILL' tag,
 // which a reference reader ignores (it stops after its last section).
@@ -868,11 +938,13 @@ std::vector<char> Context::getBiasState() {
     const char magic[4] = {'G', 'P', 'U', 'S'};
     w(magic, 4);
     w32(1);
-    int nOpes = 0, nMetad = 0, nHills = 0;
+    int nOpes = 0, nMetad = 0, nHills = 0, nPb = 0, nExt = 0;
     for (auto& hb : biases_) {
         nOpes += hb.spec.type == BIAS_OPES;
         nMetad += hb.spec.type == BIAS_METAD;
         nHills += hb.spec.type == BIAS_METAD_HILLS;
+        nPb += hb.spec.type == BIAS_PBMETAD;
+        nExt += hb.spec.type == BIAS_EXTERNAL;
     }
     w32(nOpes);
     for (auto& hb : biases_) {
@@ -910,7 +982,19 @@ std::vector<char> Context::getBiasState() {
         w32(hb.numDeposited);
         w(g.data(), 8 * g.size());
     }
-    for (int k = 0; k < 9; k++) w32(0);  // PBMETAD, EXTERNAL, LINEAR, WALL, OPES_EXPANDED, EXTLAG, EDS, MAXENT, MULTITHERMAL
+    w32(nPb);
+    for (auto& hb : biases_) {
+        if (hb.spec.type != BIAS_PBMETAD) continue;
+        std::vector<double> g(hb.dev.total);
+        cudaCheck(cudaMemcpy(g.data(), hb.dev.grid, 8 * g.size(), cudaMemcpyDeviceToHost), "blob");
+        w32(hb.dev.D);
+        for (int k = 0; k < hb.dev.D; k++) {
+            w32(hb.subDeposited[k]);
+            w(g.data() + hb.dev.goff[k], 8 * (size_t)hb.dev.npts[k]);
+        }
+    }
+    w32(nExt);
+    for (int k = 0; k < 7; k++) w32(0);  // LINEAR, WALL, OPES_EXPANDED, EXTLAG, EDS, MAXENT, MULTITHERMAL
     if (nHills > 0) {
         const char tag[4] = {'H', 'I', 'L', 'L'};
         w(tag, 4);
@@ -1011,13 +1095,42 @@ void Context::setBiasState(const std::vector<char>& bytes) {
             cudaCheck(cudaMemcpy(hb.dev.grid, g.data(), 8 * g.size(), cudaMemcpyHostToDevice), "restore");
         }
     }
-    // Remaining reference sections: counts must be zero for this library's biases.
-    const char* names[9] = {"PBMetaD", "external", "linear", "wall", "OPES_EXPANDED", "extended-Lagrangian", "EDS", "MaxEnt", "OPES multithermal"};
-    for (int k = 0; k < 9 && more(); k++) {
-        if ((size_t)(end - p) >= 4 && std::memcmp(p, "HILL", 4) == 0) break;
+    auto atHill = [&]() { return (size_t)(end - p) >= 4 && std::memcmp(p, "HILL", 4) == 0; };
+    if (more() && !atHill()) {
+        int nPb = 0;
+        for (auto& hb : biases_) nPb += hb.spec.type == BIAS_PBMETAD;
+        int32_t npb;
+        rd(&npb, 4);
+        if (npb != nPb)
+            throw Error(GLUED_E_CORRUPT, "GLUED bias-state: PBMetaD bias count mismatch (expected " + std::to_string(nPb) +
+                                             ", got " + std::to_string((long long)npb) + ")");
+        for (auto& hb : biases_) {
+            if (hb.spec.type != BIAS_PBMETAD) continue;
+            int32_t nsub;
+            rd(&nsub, 4);
+            if (nsub != hb.dev.D)
+                throw Error(GLUED_E_CORRUPT, "GLUED bias-state: PBMetaD sub-grid count mismatch (expected " +
+                                                 std::to_string(hb.dev.D) + ", got " + std::to_string((long long)nsub) + ")");
+            std::vector<double> g(hb.dev.total);
+            std::vector<int> nd(hb.dev.D);
+            for (int k = 0; k < hb.dev.D; k++) {
+                int32_t n;
+                rd(&n, 4);
+                nd[k] = n;
+                rd(g.data() + hb.dev.goff[k], 8 * (size_t)hb.dev.npts[k]);
+            }
+            hb.subDeposited = nd;
+            cudaCheck(cudaMemcpy(hb.dev.grid, g.data(), 8 * g.size(), cudaMemcpyHostToDevice), "restore");
+        }
+    }
+    // Remaining reference sections: EXTERNAL, LINEAR and WALL are stateless (counts
+    // only); the others must be zero for this library's biases.
+    const char* names[8] = {"external", "linear", "wall", "OPES_EXPANDED", "extended-Lagrangian", "EDS", "MaxEnt", "OPES multithermal"};
+    for (int k = 0; k < 8 && more(); k++) {
+        if (atHill()) break;
         int32_t n;
         rd(&n, 4);
-        if (n != 0 && k != 1 && k != 2 && k != 3)
+        if (n != 0 && k > 2)
             throw Error(GLUED_E_CORRUPT, std::string("GLUED bias-state: ") + names[k] + " bias count mismatch (expected 0, got " + std::to_string((long long)n) + ")");
     }
     if ((size_t)(end - p) >= 8 && std::memcmp(p, "HILL", 4) == 0) {

@@ -48,6 +48,7 @@ struct HostBias {
     // owned buffers
     DBuf grid, centers, sigmas, logW, ints, dbls, hCenters, hHeights, mean, m2, sigma0;
     int numDeposited = 0;   // MetaD
+    std::vector<int> subDeposited;   // PBMETAD: deposits per sub-grid
     int numKernelsCPU = 0;  // OPES: CPU mirror for the maxKernels guard (:5107-5110)
     int nSamplesCPU = 0;    // OPES adaptive: mirror of the GPU warm-up counter
     std::vector<double> sigma0Host;

@@ -140,6 +140,10 @@ struct BiasDev {
     double* grid;
     int total;
     int pace;
+    // PBMETAD: sub-grid d is grid[goff[d] .. goff[d] + npts[d]); pbState = the
+    // sub-grid energies [D] and softmax weights [D] of the last evaluation
+    int goff[8];
+    double* pbState;
     // hills table (METAD_HILLS): centers [maxH][D], heights [maxH]
     double* hCenters;
     double* hHeights;

@@ -47,6 +47,7 @@ void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* c
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
                    int padded);
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
+void launchPbmetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, int maxPoints);
 void launchHillsDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);
 void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies,
                        int* mergeFlag, double* partial, int nPartial);

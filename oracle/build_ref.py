@@ -33,7 +33,7 @@ KERNELS = [
     "kDistanceKernelSrc", "kAngleKernelSrc", "kDihedralKernelSrc", "kCOMDistanceKernelSrc",
     "kGyrationKernelSrc", "kPathKernelSrc", "kRMSDKernelSrc", "kCoordinationKernelSrc",
     "kContactMapKernelSrc", "kPCAKernelSrc", "kScatterKernelSrc", "kHarmonicKernelSrc",
-    "kOPESKernelSrc", "kMetaDKernelSrc",
+    "kOPESKernelSrc", "kMetaDKernelSrc", "kPBMetaDKernelSrc",
 ]
 
 SHIM = r"""

@@ -641,6 +641,70 @@ void orc_metad_deposit(double* grid, int D, int total, const double* origin, con
     }
 }
 
+// PBMETAD: N 1-D sub-grids (concatenated, sub-grid d at goff[d]) over the CVs
+// idx[d], each linearly interpolated with periodic wrap or clamping
+// (CommonGluedKernels.cpp:3698-3734), combined by log-sum-exp
+// E = -kT (ln sum_d exp((Vmin - V_d)/kT) - ln N) + Vmin with dE/ds_d = w_d dV_d/ds_d,
+// w_d the softmax weights (:3736-3763). V_d and w_d are returned for the deposit.
+double orc_pbmetad_eval(const double* cvv, const int* idx, int N, const double* grid, const int* goff,
+                        const double* origin, const double* invSp, const int* npts, const int* per, double kT,
+                        double* grad, double* Vout, double* Wout) {
+    double G[8];
+    for (int d = 0; d < N; d++) {
+        const double* g = grid + goff[d];
+        const int n = npts[d];
+        double fr = (cvv[idx[d]] - origin[d]) * invSp[d];
+        int lo, hi;
+        if (per[d]) {
+            fr = fr - std::floor(fr / (double)n) * (double)n;
+            if (fr < 0.0) fr += (double)n;
+            lo = (int)fr;
+            if (lo >= n) lo = n - 1;
+            hi = (lo + 1) % n;
+        } else {
+            if (fr < 0.0) fr = 0.0;
+            if (fr > (double)(n - 1)) fr = (double)(n - 1);
+            lo = (int)fr;
+            if (lo >= n - 1) lo = n - 2;
+            hi = lo + 1;
+        }
+        const double al = fr - lo;
+        Vout[d] = g[lo] * (1.0 - al) + g[hi] * al;
+        G[d] = (g[hi] - g[lo]) * invSp[d];
+    }
+    double vmin = Vout[0];
+    for (int d = 1; d < N; d++)
+        if (Vout[d] < vmin) vmin = Vout[d];
+    double sum = 0.0;
+    for (int d = 0; d < N; d++) sum += std::exp((vmin - Vout[d]) / kT);
+    for (int d = 0; d < N; d++) {
+        Wout[d] = std::exp((vmin - Vout[d]) / kT) / sum;
+        grad[idx[d]] += Wout[d] * G[d];
+    }
+    return -kT * (std::log(sum) - std::log((double)N)) + vmin;
+}
+
+// PBMETAD deposit (CommonGluedKernels.cpp:3765-3797, pace gate :5147-5155): each
+// sub-grid d gets a 1-D Gaussian at its CV value with height w_d h0 exp(-V_d hif)
+// (w_d h0 when hif = 0), V_d and w_d from the last evaluation, exponent <= 8.
+void orc_pbmetad_deposit(double* grid, const int* goff, int N, const double* origin, const double* invSp,
+                         const int* npts, const int* per, const double* cvv, const int* idx, const double* sigma,
+                         const double* V, const double* W, double h0, double hif) {
+    for (int d = 0; d < N; d++) {
+        const double height = hif > 0.0 ? W[d] * h0 * std::exp(-V[d] * hif) : W[d] * h0;
+        double* g = grid + goff[d];
+        for (int i = 0; i < npts[d]; i++) {
+            double dc = origin[d] + (double)i / invSp[d] - cvv[idx[d]];
+            if (per[d]) {
+                const double L = (double)npts[d] / invSp[d];
+                dc -= std::round(dc / L) * L;
+            }
+            const double ex = dc * dc / (2.0 * sigma[d] * sigma[d]);
+            if (ex <= 8.0) g[i] += height * std::exp(-ex);
+        }
+    }
+}
+
 // Direct hill sum V(s) = sum_k h_k exp(-sum_d dc^2 / (2 sigma_d^2)), exponent > 8
 // truncated like the grid deposit, periodic wrap with period L_d (L_d <= 0 means
 // non-periodic). No reference counterpart (the reference MetaD is grid-only).

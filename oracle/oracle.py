@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libglued_oracle.so")
 # CV / bias type codes (openmmapi/include/GluedForce.h:27-95).
 CV_DISTANCE, CV_ANGLE, CV_DIHEDRAL, CV_COM_DISTANCE, CV_GYRATION = 1, 2, 3, 4, 5
 CV_COORDINATION, CV_RMSD, CV_PATH, CV_CONTACTMAP, CV_PCA = 6, 7, 10, 13, 21
-BIAS_HARMONIC, BIAS_METAD, BIAS_OPES = 1, 3, 5
+BIAS_HARMONIC, BIAS_METAD, BIAS_PBMETAD, BIAS_OPES, BIAS_EXTERNAL = 1, 3, 4, 5, 6
 # Extensions of this build (no reference counterpart).
 CV_RMSD_KABSCH = 107
 CV_COORDINATION_CUTOFF = 106
@@ -188,6 +188,35 @@ class OracleSystem:
                           per=np.array(per, np.int32), pace=pace, total=total,
                           grid=np.zeros(total), hif=(0.0 if gamma <= 1.0 else 1.0 / ((gamma - 1.0) * kT)),
                           deposited=0)
+            elif t == BIAS_PBMETAD:
+                # CommonBiasKernels.cpp:298-424: N 1-D sub-grids, one energy slot
+                h0, gamma, kT = p[0], p[1], p[2]
+                sigma = [p[3 + 3 * d] for d in range(D)]
+                origin = [p[4 + 3 * d] for d in range(D)]
+                mx = [p[5 + 3 * d] for d in range(D)]
+                bins = [ip[1 + 2 * d] for d in range(D)]
+                per = [ip[2 + 2 * d] for d in range(D)]
+                npts = [bins[d] + (0 if per[d] else 1) for d in range(D)]
+                goff = np.concatenate([[0], np.cumsum(npts)[:-1]]).astype(np.int32)
+                st.update(h0=h0, gamma=gamma, kT=kT, sigma=np.array(sigma), origin=np.array(origin),
+                          inv=np.array([bins[d] / (mx[d] - origin[d]) for d in range(D)]),
+                          npts=np.array(npts, np.int32), per=np.array(per, np.int32), goff=goff,
+                          grid=np.zeros(int(sum(npts))), pace=ip[0],
+                          hif=(0.0 if gamma <= 1.0 else 1.0 / ((gamma - 1.0) * kT)),
+                          V=np.zeros(D), W=np.full(D, 1.0 / D), deposited=[0] * D)
+            elif t == BIAS_EXTERNAL:
+                # CommonBiasKernels.cpp:425-488: fixed user grid, evaluated as the MetaD grid
+                origin = p[:D]; mx = p[D:2 * D]
+                bins = ip[:D]; per = ip[D:2 * D]
+                inv = [bins[d] / (mx[d] - origin[d]) for d in range(D)]
+                npts = [bins[d] + (0 if per[d] else 1) for d in range(D)]
+                strides = [1] * D
+                for d in range(1, D):
+                    strides[d] = strides[d - 1] * npts[d - 1]
+                total = strides[-1] * npts[-1]
+                st.update(origin=np.array(origin), inv=np.array(inv), npts=np.array(npts, np.int32),
+                          strides=np.array(strides, np.int32), per=np.array(per, np.int32), total=total,
+                          grid=np.array(p[2 * D:2 * D + total], dtype=np.float64))
             elif t == BIAS_METAD_HILLS:
                 h0 = p[0]; sigma = p[1:1 + D]; gamma = p[1 + D]; kT = p[2 + D]
                 lo = p[3 + D:3 + 2 * D]; hi = p[3 + 2 * D:3 + 3 * D]
@@ -345,7 +374,7 @@ class OracleSystem:
         C = _p(np.ascontiguousarray(cvv, dtype=np.float64), _D)
         cvv = np.ascontiguousarray(cvv, dtype=np.float64)
         G = _p(grad, _D)
-        for typ in (BIAS_HARMONIC, BIAS_OPES, BIAS_METAD, BIAS_METAD_HILLS):
+        for typ in (BIAS_HARMONIC, BIAS_OPES, BIAS_METAD, BIAS_PBMETAD, BIAS_EXTERNAL, BIAS_METAD_HILLS):
             for st in self.bias_state:
                 if st["type"] != typ:
                     continue
@@ -358,7 +387,12 @@ class OracleSystem:
                     e = L.orc_opes_eval(C, _p(idx, _I), st["D"], _p(st["centers"], _D), _p(st["sigmas"], _D),
                                         _p(st["logw"], _D), int(st["ist"][0]), _D(st["invGF"]), _D(st["kT"]),
                                         _D(st["dst"][0]), _D(st["cut2"]), _D(st["eps"]), _D(st["barrier"]), G)
-                elif typ == BIAS_METAD:
+                elif typ == BIAS_PBMETAD:
+                    L.orc_pbmetad_eval.restype = _D
+                    e = L.orc_pbmetad_eval(C, _p(idx, _I), st["D"], _p(st["grid"], _D), _p(st["goff"], _I),
+                                           _p(st["origin"], _D), _p(st["inv"], _D), _p(st["npts"], _I),
+                                           _p(st["per"], _I), _D(st["kT"]), G, _p(st["V"], _D), _p(st["W"], _D))
+                elif typ in (BIAS_METAD, BIAS_EXTERNAL):
                     L.orc_metad_eval.restype = _D
                     e = L.orc_metad_eval(C, _p(idx, _I), st["D"], _p(st["grid"], _D), _p(st["origin"], _D),
                                          _p(st["inv"], _D), _p(st["npts"], _I), _p(st["strides"], _I),
@@ -405,7 +439,7 @@ class OracleSystem:
         L = lib()
         if not self.cv_ready or step == self.last_update_step:
             return
-        if not any(st["type"] in (BIAS_OPES, BIAS_METAD, BIAS_METAD_HILLS) for st in self.bias_state):
+        if not any(st["type"] in (BIAS_OPES, BIAS_METAD, BIAS_PBMETAD, BIAS_METAD_HILLS) for st in self.bias_state):
             return
         self.last_update_step = step
         cvv = np.ascontiguousarray(self.cv_values, dtype=np.float64)
@@ -447,6 +481,14 @@ class OracleSystem:
                 center = np.array([cvv[i] for i in st["idx"]])
                 st["centers"] = np.vstack([st["centers"], center[None, :]])
                 st["heights"] = np.append(st["heights"], h)
+        for st in self.bias_state:
+            if st["type"] != BIAS_PBMETAD or step == 0 or step % st["pace"] != 0:
+                continue
+            L.orc_pbmetad_deposit(_p(st["grid"], _D), _p(st["goff"], _I), st["D"], _p(st["origin"], _D),
+                                  _p(st["inv"], _D), _p(st["npts"], _I), _p(st["per"], _I), C,
+                                  _p(st["idx"], _I), _p(st["sigma"], _D), _p(st["V"], _D), _p(st["W"], _D),
+                                  _D(st["h0"]), _D(st["hif"]))
+            st["deposited"] = [n + 1 for n in st["deposited"]]
 
     def load_blob(self, blob: bytes):
         """Restore OPES / MetaD / hill-sum state from a 'GPUS' v1 bias-state blob
@@ -480,7 +522,20 @@ class OracleSystem:
                 st["grid"][:] = np.frombuffer(blob, "<f8", count=st["total"], offset=p)
                 p += 8 * st["total"]
                 st["deposited"] = nd
-        p += 36
+        if p < len(blob) and blob[p:p + 4] != b"HILL":
+            npb, = struct.unpack_from("<i", blob, p); p += 4
+            pbs = [s_ for s_ in self.bias_state if s_["type"] == BIAS_PBMETAD]
+            assert npb == len(pbs)
+            for st in pbs:
+                nsub, = struct.unpack_from("<i", blob, p); p += 4
+                assert nsub == st["D"]
+                for d in range(nsub):
+                    nd, = struct.unpack_from("<i", blob, p); p += 4
+                    n, o = int(st["npts"][d]), int(st["goff"][d])
+                    st["grid"][o:o + n] = np.frombuffer(blob, "<f8", count=n, offset=p)
+                    p += 8 * n
+                    st["deposited"][d] = nd
+        p += 32  # EXTERNAL, LINEAR, WALL, OPES_EXPANDED, EXTLAG, EDS, MAXENT, MULTITHERMAL counts
         if blob[p:p + 4] == b"HILL":
             p += 8
             for st in [s_ for s_ in self.bias_state if s_["type"] == BIAS_METAD_HILLS]:

@@ -18,7 +18,7 @@ import numpy as np
 
 from oracle import (OracleSystem, CV_DISTANCE, CV_ANGLE, CV_DIHEDRAL, CV_COM_DISTANCE, CV_GYRATION,
                     CV_COORDINATION, CV_RMSD, CV_PATH, CV_CONTACTMAP, CV_PCA, BIAS_HARMONIC,
-                    BIAS_METAD, BIAS_OPES)
+                    BIAS_METAD, BIAS_OPES, BIAS_PBMETAD, BIAS_EXTERNAL)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _libs = {}
@@ -160,7 +160,7 @@ class RefSystem(OracleSystem):
         energies = np.zeros(nslot)
         cvv = np.ascontiguousarray(np.resize(cvv, max(1, self.num_cvs)), dtype=np.float64)
         C, G, E = _p(cvv, _D), _p(grad, _D), _p(energies, _D)
-        for typ in (BIAS_HARMONIC, BIAS_OPES, BIAS_METAD):
+        for typ in (BIAS_HARMONIC, BIAS_OPES, BIAS_METAD, BIAS_PBMETAD, BIAS_EXTERNAL):
             for st in self.bias_state:
                 if st["type"] != typ:
                     continue
@@ -173,6 +173,19 @@ class RefSystem(OracleSystem):
                     L.opesEvalBias(C, _p(idx, _I), _p(st["centers"], _D), _p(st["sigmas"], _D), _p(st["logw"], _D),
                                    _p(nk, _I), st["D"], _D(st["invGF"]), _D(st["kT"]), _p(su, _D), _p(sw, _D),
                                    _D(st["cut2"]), _D(st["eps"]), _D(st["barrier"]), G, E, st["slot"])
+                elif typ == BIAS_PBMETAD:
+                    # pbmetaDSubgridEval per sub-grid, then pbmetaDCombine
+                    N = st["D"]
+                    le, lg = np.zeros(N), np.zeros(N)
+                    for d in range(N):
+                        o = int(st["goff"][d])
+                        sub = st["grid"][o:o + int(st["npts"][d])]
+                        L.pbmetaDSubgridEval(C, _p(idx[d:d + 1], _I), _p(sub, _D), _p(st["origin"][d:d + 1], _D),
+                                             _p(st["inv"][d:d + 1], _D), _p(st["npts"][d:d + 1], _I),
+                                             _p(st["per"][d:d + 1], _I), _p(le, _D), _p(lg, _D), d)
+                    L.pbmetaDCombine(_p(le, _D), _p(lg, _D), _p(idx, _I), N, _D(st["kT"]), E, st["slot"], G,
+                                     _p(st["W"], _D))
+                    st["V"][:] = le
                 else:
                     L.metaDEvalBias(C, _p(idx, _I), _p(st["grid"], _D), _p(st["origin"], _D), _p(st["inv"], _D),
                                     _p(st["npts"], _I), _p(st["strides"], _I), _p(st["per"], _I), st["D"], G, E,
@@ -238,3 +251,16 @@ class RefSystem(OracleSystem):
                            _p(st["strides"], _I), _p(st["per"], _I), st["D"], st["total"], _p(center, _D),
                            _p(sig, _D), _p(E, _D), st["slot"], _D(st["h0"]), _D(st["hif"]))
             st["deposited"] += 1
+        for st in self.bias_state:
+            if st["type"] != BIAS_PBMETAD or step == 0 or step % st["pace"] != 0:
+                continue
+            for d in range(st["D"]):
+                o, n = int(st["goff"][d]), int(st["npts"][d])
+                sub = np.ascontiguousarray(st["grid"][o:o + n])
+                center = np.array([cvv[st["idx"][d]]])
+                sig = np.array([st["sigma"][d]])
+                L.pbmetaDDeposit(_p(sub, _D), _p(st["origin"][d:d + 1], _D), _p(st["inv"][d:d + 1], _D),
+                                 _p(st["npts"][d:d + 1], _I), _p(st["per"][d:d + 1], _I), n, _p(center, _D),
+                                 _p(sig, _D), _p(st["V"], _D), d, _D(st["h0"]), _D(st["hif"]), _p(st["W"], _D))
+                st["grid"][o:o + n] = sub
+            st["deposited"] = [k + 1 for k in st["deposited"]]
