@@ -1,9 +1,10 @@
 """Multi-GPU plumbing for the batched path: one process per GPU.
 
 Walkers are independent, so they shard across ranks with no data-path
-collective (weak scaling: each rank evaluates its own walkers). The only
-collectives are the timing reductions of the benchmark (max over ranks) and
-the barriers around the timed region. NCCL on GPUs, gloo for the CPU tests.
+collective (weak scaling: each rank evaluates its own walkers). The
+collectives are the timing reductions of the benchmark (max over ranks), the
+barriers around the timed region, and the periodic bias-state sync between
+walker groups (``sync_bias_state``). NCCL on GPUs, gloo for the CPU tests.
 """
 from __future__ import annotations
 
@@ -49,3 +50,24 @@ def sum_over_ranks(x, device="cpu"):
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def sync_bias_state(blob, force, baselines=None, group=None):
+    """Cross-rank bias sync of one walker group per rank (the CPU-mediated merge of
+    python/MultiGPUManager.py:1076-1113, with ranks in place of device groups).
+
+    Every rank passes its group's ``getBiasState()`` blob; the blobs are gathered
+    on every rank (``all_gather_object``, rank order) and each rank computes the
+    same incremental additive merge, so all ranks return the identical merged
+    blob, to load with ``setBiasState``, and the baselines to pass back at the
+    next sync. Without an initialized process group the blob is returned as is.
+    Every rank must call this at the same step.
+    """
+    from .merger import BiasStateMerger
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return bytes(blob), [BiasStateMerger._parse(bytes(blob), force)]
+    world = dist.get_world_size(group)
+    blobs = [None] * world
+    dist.all_gather_object(blobs, bytes(blob), group=group)
+    return BiasStateMerger.merge_additive_incremental(blobs, force, baselines)
