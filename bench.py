@@ -1,6 +1,6 @@
 """Benchmark of the per-step CV -> bias -> force-scatter path on B200.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--config c4|c2|c1|c3] [--impl ours|reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--config c4|c2|c1|c1pb|c3|c5] [--impl ours|reference]
 
 A step is one pass of the hot path over one batch of synthetic input:
 updateState(step) (pace-gated deposition) followed by execute(forces) for every
@@ -168,7 +168,8 @@ def time_steps(torch, step_fn, steps, warmup, flush):
 def run_single(args, torch, cfg):
     from gluedmd_b200 import workloads as W, _native
     import ctypes
-    w = {"c1": lambda: W.config1("grid"), "c2": W.config2, "c3": W.config3}[cfg]()
+    w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"), "c2": W.config2,
+             "c3": W.config3}[cfg]()
     ctx, f = build_single(w, torch, "cuda")
     nc = ctx.glued_context_for(f)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -382,7 +383,7 @@ def cpu_baseline_single(cfg, w, budget_s=12.0):
     from ref_runner import RefSystem
     kind = "reference" if RefSystem.available() else "port"
     cls = RefSystem if kind == "reference" else O.OracleSystem
-    biases = [b for b in w.biases if b[0] in (1, 3, 5)]
+    biases = [b for b in w.biases if b[0] in (1, 3, 4, 5, 6)]
     sysm = cls(w.cvs, biases, masses=w.masses, periodic=w.pbc, mode="f32", num_particles=len(w.positions))
     if w.blob:
         sysm.load_blob(w.blob)
@@ -561,7 +562,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c1pb", "c2", "c3", "c4", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -601,7 +602,8 @@ def main():
                                                 "d2h_bytes_per_step": 0}}
         else:
             from gluedmd_b200 import workloads as W
-            w = {"c1": lambda: W.config1("grid"), "c2": W.config2, "c3": W.config3}[args.config]()
+            w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"), "c2": W.config2,
+             "c3": W.config3}[args.config]()
             cb = cpu_baseline_single(args.config, w, budget_s=max(5.0, 0.5 * args.steps))
             line = {"impl": "reference", "metric": "CV+bias+force us/step", "value": cb["value"], "unit": "us/step",
                     "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,

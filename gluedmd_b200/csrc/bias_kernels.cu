@@ -1,12 +1,18 @@
 // Bias evaluation, chain-rule scatter and MetaD deposition.
 //
-// k_biases : every bias of the context in the reference's evaluation order
-//            (harmonic, OPES, MetaD grid, then this library's hill-sum MetaD;
-//            CommonGluedKernels.cpp:4955-5026) inside one CTA. dU/dCV is
-//            accumulated in shared memory and written once, so no separate
-//            clearing pass is needed (the reference relies on OpenMM's autoclear,
-//            :4244). Kernel/hill sums are split over all threads and reduced by a
-//            fixed tree in FP64.
+// k_biases : every bias of the context inside one CTA, added into dU/dCV in
+//            the reference's evaluation order (harmonic, OPES, MetaD grid,
+//            PBMETAD, EXTERNAL, then this library's hill-sum MetaD;
+//            CommonGluedKernels.cpp:4955-5026). The bias records are copied to
+//            shared memory before the wait for the previous kernel (the host
+//            writes them only between steps). The single-thread biases
+//            (harmonic, MetaD, PBMETAD, EXTERNAL) are evaluated concurrently,
+//            one warp each, into per-bias contributions that thread 0 then adds
+//            in evaluation order, so dU/dCV is summed in the same order as a
+//            sequential pass. dU/dCV is accumulated in shared memory and written
+//            once, so no separate clearing pass is needed (the reference relies
+//            on OpenMM's autoclear, :4244). Kernel/hill sums are split over all
+//            threads and reduced by a fixed tree in FP64.
 // k_scatter: F[atom] -= dU/dCV * dCV/dx as 2^32 fixed point with three 64-bit
 //            integer atomics per Jacobian row (CommonGluedKernels.cpp:2430-2456);
 //            integer addition keeps the result order-independent.
@@ -23,12 +29,17 @@
 
 namespace glued {
 
-__device__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* sG, double* energies) {
-    // CommonGluedKernels.cpp:3574-3636, one thread.
-    int lo[8], hi[8];
-    double al[8];
+// MetaD / EXTERNAL grid (CommonGluedKernels.cpp:3574-3636), one thread, D <= 3
+// (checked at setup): multilinear interpolation over the 2^D cell corners with
+// periodic wrap or clamping. All corner values are loaded before the arithmetic.
+// Writes the energy and dE/ds_d into out[d].
+__device__ __noinline__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* energies, double* out) {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    double al[3] = {0, 0, 0};
     const int D = b.D;
-    for (int d = 0; d < D; d++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (d >= D) break;
         double fr = (cvv[b.cvIdx[d]] - b.origin[d]) * b.invSp[d];
         int N = b.npts[d];
         if (N <= 1) { lo[d] = hi[d] = 0; al[d] = 0; }
@@ -48,66 +59,101 @@ __device__ void evalMetadGrid(const BiasDev& b, const double* cvv, double* sG, d
             hi[d] = lo[d] + 1;
         }
     }
-    double V = 0, dV[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < (1 << D); c++) {
-        int flat = 0;
-        for (int d = 0; d < D; d++) flat += (((c >> d) & 1) ? hi[d] : lo[d]) * b.strides[d];
-        double val = b.grid[flat], w = 1;
-        for (int d = 0; d < D; d++) w *= ((c >> d) & 1) ? al[d] : (1.0 - al[d]);
-        V += w * val;
-        for (int d = 0; d < D; d++) {
+    const int nc = 1 << D;
+    double val[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        if (c < nc) {
+            int flat = 0;
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                if (d < D) flat += (((c >> d) & 1) ? hi[d] : lo[d]) * b.strides[d];
+            val[c] = b.grid[flat];
+        }
+    }
+    double V = 0, dV[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        if (c >= nc) break;
+        double w = 1;
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            if (d < D) w *= ((c >> d) & 1) ? al[d] : (1.0 - al[d]);
+        V += w * val[c];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (d >= D) break;
             double sg = ((c >> d) & 1) ? 1.0 : -1.0, wo = 1;
-            for (int e = 0; e < D; e++) if (e != d) wo *= ((c >> e) & 1) ? al[e] : (1.0 - al[e]);
-            dV[d] += sg * wo * val;
+#pragma unroll
+            for (int e = 0; e < 3; e++)
+                if (e < D && e != d) wo *= ((c >> e) & 1) ? al[e] : (1.0 - al[e]);
+            dV[d] += sg * wo * val[c];
         }
     }
     energies[b.slot] = V;
-    for (int d = 0; d < D; d++) sG[b.cvIdx[d]] += dV[d] * b.invSp[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (d < D) out[d] = dV[d] * b.invSp[d];
 }
 
 // PBMETAD (CommonGluedKernels.cpp:3694-3760), one thread: sub-grid d is a 1-D
 // grid over CV cvIdx[d], linearly interpolated (periodic wrap or clamp, as the
 // MetaD grid); the sub-grid energies V_d combine as
 // E = -kT (ln sum_d exp((Vmin - V_d)/kT) - ln N) + Vmin, and dE/ds_d = w_d dV_d/ds_d
-// with the softmax weights w_d = exp((Vmin - V_d)/kT) / sum. V_d and w_d are kept
-// in pbState for the deposit.
-__device__ void evalPbmetad(const BiasDev& b, const double* cvv, double* sG, double* energies) {
+// with the softmax weights w_d = exp((Vmin - V_d)/kT) / sum, written to out[d].
+// V_d and w_d are kept in pbState for the deposit.
+__device__ __noinline__ void evalPbmetad(const BiasDev& b, const double* cvv, double* energies, double* out) {
     const int N = b.D;
-    double V[8], G[8];
-    for (int d = 0; d < N; d++) {
+    // vlo / vhi hold the cell values, then V_d / dV_d/ds_d
+    double vlo[8], vhi[8], al[8];
+    double* const V = vlo;
+    double* const G = vhi;
+    // all sub-grid cells first, so their loads are in flight together
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        if (d >= N) break;
         const double* g = b.grid + b.goff[d];
         const int n = b.npts[d];
         double fr = (cvv[b.cvIdx[d]] - b.origin[d]) * b.invSp[d];
         int lo, hi;
-        double al;
         if (b.per[d]) {
             fr = fr - floor(fr / (double)n) * (double)n;
             if (fr < 0.0) fr += n;
             lo = (int)fr;
             if (lo >= n) lo = n - 1;
-            al = fr - lo;
             hi = (lo + 1) % n;
         } else {
             if (fr < 0.0) fr = 0.0;
             if (fr > (double)(n - 1)) fr = (double)(n - 1);
             lo = (int)fr;
             if (lo >= n - 1) lo = n - 2;
-            al = fr - lo;
             hi = lo + 1;
         }
-        V[d] = g[lo] * (1.0 - al) + g[hi] * al;
-        G[d] = (g[hi] - g[lo]) * b.invSp[d];
+        al[d] = fr - lo;
+        vlo[d] = g[lo];
+        vhi[d] = g[hi];
+    }
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        if (d >= N) break;
+        const double v = vlo[d] * (1.0 - al[d]) + vhi[d] * al[d];
+        G[d] = (vhi[d] - vlo[d]) * b.invSp[d];
+        V[d] = v;
     }
     double vmin = V[0];
-    for (int d = 1; d < N; d++) vmin = V[d] < vmin ? V[d] : vmin;
+#pragma unroll
+    for (int d = 1; d < 8; d++)
+        if (d < N) vmin = V[d] < vmin ? V[d] : vmin;
     double ene = 0.0;
+#pragma unroll 1
     for (int d = 0; d < N; d++) ene += exp((vmin - V[d]) / b.kT);
     energies[b.slot] = -b.kT * (log(ene) - log((double)N)) + vmin;
+#pragma unroll 1
     for (int d = 0; d < N; d++) {
         const double w = exp((vmin - V[d]) / b.kT) / ene;
         b.pbState[d] = V[d];
         b.pbState[N + d] = w;
-        sG[b.cvIdx[d]] += w * G[d];
+        out[d] = w * G[d];
     }
 }
 
@@ -167,40 +213,71 @@ __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__
     if (tid < 9) part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 9 + tid] = acc[tid];
 }
 
-__global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ biases, int nb,
+__device__ __forceinline__ bool singleLaneBias(int t) {
+    return t == BIAS_HARMONIC || t == BIAS_METAD || t == BIAS_PBMETAD || t == BIAS_EXTERNAL;
+}
+
+// Shared memory: sG[numCVs] | contrib[nb][8] | (stage) records[nb]. SINGLE: the
+// context has single-lane biases (the instantiation without them carries none of
+// their code, which matters when every step starts with cold caches).
+template <bool SINGLE>
+__global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbiases, int nb, int stage,
                                                  const double* __restrict__ cvv, int numCVs,
                                                  const double* __restrict__ testGrad, double* __restrict__ dUdCV,
                                                  double* __restrict__ energies, const double* __restrict__ sumPart) {
-    pdlEnter();
-    extern __shared__ double sG[];
+    extern __shared__ __align__(16) double sm[];
     __shared__ double red[32 * 9];
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
+    double* sG = sm;
+    double* contrib = sm + ((numCVs + 1) & ~1);
+    const BiasDev* biases = gbiases;
+    if (stage) {
+        // records are written by the host between steps only: copy them while the
+        // previous kernel finishes
+        BiasDev* rec = reinterpret_cast<BiasDev*>(contrib + 8 * nb);
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(gbiases);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(rec);
+        const int words = nb * (int)(sizeof(BiasDev) / 8);
+        for (int i = tid; i < words; i += nt) dst[i] = src[i];
+        biases = rec;
+    }
+    pdlEnter();
     for (int i = tid; i < numCVs; i += nt) sG[i] = testGrad ? testGrad[i] : 0.0;
     __syncthreads();
     if (!testGrad) {
-        for (int bi = 0; bi < nb; bi++) {
-            const BiasDev& b = biases[bi];
-            const int D = b.D;
-            if (b.type == BIAS_HARMONIC) {
-                // CommonGluedKernels.cpp:2513-2540; k and s0 stored as float.
-                if (tid == 0) {
+        // single-lane biases, one warp each (CommonGluedKernels.cpp:2513-2540,
+        // :3574-3636, :3698-3763; EXTERNAL through the MetaD grid,
+        // CommonBiasKernels.cpp:425-488)
+        if constexpr (SINGLE) {
+            for (int bi = warp; bi < nb; bi += nt >> 5) {
+                const BiasDev& b = biases[bi];
+                if (lane != 0 || !singleLaneBias(b.type)) continue;
+                double* out = contrib + 8 * bi;
+                if (b.type == BIAS_HARMONIC) {
+                    // k and s0 stored as float
                     const double TWO_PI = 6.283185307179586;
                     double V = 0;
-                    for (int d = 0; d < D; d++) {
+                    for (int d = 0; d < b.D; d++) {
                         double ds = cvv[b.cvIdx[d]] - (double)b.hs0[d];
                         if (b.periodicFlag) ds -= TWO_PI * round(ds / TWO_PI);
                         V += 0.5 * (double)b.hk[d] * ds * ds;
-                        sG[b.cvIdx[d]] += (double)b.hk[d] * ds;
+                        out[d] = (double)b.hk[d] * ds;
                     }
                     energies[b.slot] = V;
+                } else if (b.type == BIAS_PBMETAD) {
+                    evalPbmetad(b, cvv, energies, out);
+                } else {
+                    evalMetadGrid(b, cvv, energies, out);
                 }
-            } else if (b.type == BIAS_METAD) {
-                if (tid == 0) evalMetadGrid(b, cvv, sG, energies);
-            } else if (b.type == BIAS_PBMETAD) {
-                if (tid == 0) evalPbmetad(b, cvv, sG, energies);
-            } else if (b.type == BIAS_EXTERNAL) {
-                // user grid, evaluated as the MetaD grid (CommonBiasKernels.cpp:425-488)
-                if (tid == 0) evalMetadGrid(b, cvv, sG, energies);
+            }
+            __syncthreads();
+        }
+        for (int bi = 0; bi < nb; bi++) {
+            const BiasDev& b = biases[bi];
+            const int D = b.D;
+            if (SINGLE && singleLaneBias(b.type)) {
+                if (tid == 0)
+                    for (int d = 0; d < D; d++) sG[b.cvIdx[d]] += contrib[8 * bi + d];
             } else if (b.type == BIAS_OPES) {
                 // CommonGluedKernels.cpp:2642-2723.
                 if (tid == 0 && b.adaptiveStride > 0) {
@@ -234,8 +311,8 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
                         }
                     }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
         for (int bi = 0; bi < nb; bi++) {
             const BiasDev& b = biases[bi];
@@ -253,6 +330,7 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ bias
             __syncthreads();
         }
     }
+    __syncthreads();
     for (int i = tid; i < numCVs; i += nt) dUdCV[i] = sG[i];
 }
 
@@ -338,10 +416,22 @@ __global__ void k_hills_deposit(const BiasDev* __restrict__ bp, const double* __
 }
 
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
-                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums) {
+                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums,
+                  bool singleLane) {
     if (kernelSums && !testGrad && nb > 0) launchPdl(k_kernel_sums, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
-    size_t smem = sizeof(double) * (size_t)(numCVs > 0 ? numCVs : 1);
-    launchPdl(k_biases, dim3(1), dim3(512), smem, s, biases, nb, cvv, numCVs, testGrad, dUdCV, energies, sumPart);
+    // sG (rounded to an even count, so what follows is 16-byte aligned), the
+    // per-bias contributions, then the staged records when they fit in 48 KB
+    static_assert(sizeof(BiasDev) % 8 == 0, "bias records are copied as 8-byte words");
+    size_t smem = sizeof(double) * ((size_t)((numCVs + 1) & ~1) + 8 * (size_t)nb);
+    if (smem == 0) smem = 16;
+    int stage = smem + sizeof(BiasDev) * (size_t)nb <= 48 * 1024 ? 1 : 0;
+    if (stage) smem += sizeof(BiasDev) * (size_t)nb;
+    if (singleLane)
+        launchPdl(k_biases<true>, dim3(1), dim3(512), smem, s, biases, nb, stage, cvv, numCVs, testGrad, dUdCV,
+                  energies, sumPart);
+    else
+        launchPdl(k_biases<false>, dim3(1), dim3(512), smem, s, biases, nb, stage, cvv, numCVs, testGrad, dUdCV,
+                  energies, sumPart);
 }
 
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,

@@ -598,6 +598,11 @@ void Context::setupBiases(const GluedForce& f) {
     kernelSums_ = false;
     for (auto& hb : biases_)
         if (hb.spec.type == BIAS_OPES || hb.spec.type == BIAS_METAD_HILLS) kernelSums_ = true;
+    singleLane_ = false;
+    for (auto& hb : biases_)
+        if (hb.spec.type == BIAS_HARMONIC || hb.spec.type == BIAS_METAD || hb.spec.type == BIAS_PBMETAD ||
+            hb.spec.type == BIAS_EXTERNAL)
+            singleLane_ = true;
     sumPart_.alloc(sizeof(double) * (size_t)std::max(nb, 1) * KSUM_CTAS * 9);
 }
 
@@ -677,7 +682,7 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
     if (want(4))
         launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
                      testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>(),
-                     sumPart_.as<double>(), kernelSums_);
+                     sumPart_.as<double>(), kernelSums_, singleLane_);
     if (includeForces && want(5)) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
 }
 

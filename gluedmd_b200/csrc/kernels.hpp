@@ -43,7 +43,8 @@ bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool
 // into sumPart[nb][KSUM_CTAS][9] first (kernelSums), then k_biases combines them.
 constexpr int KSUM_CTAS = 64;
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
-                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums);
+                  const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums,
+                  bool singleLane);
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
                    int padded);
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);

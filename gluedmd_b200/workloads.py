@@ -25,7 +25,7 @@ import numpy as np
 KT300 = 2.494338785
 CV_DISTANCE, CV_ANGLE, CV_DIHEDRAL, CV_COM_DISTANCE, CV_GYRATION = 1, 2, 3, 4, 5
 CV_COORDINATION, CV_RMSD, CV_PATH, CV_CONTACTMAP = 6, 7, 10, 13
-BIAS_HARMONIC, BIAS_METAD, BIAS_OPES, BIAS_METAD_HILLS = 1, 3, 5, 103
+BIAS_HARMONIC, BIAS_METAD, BIAS_PBMETAD, BIAS_OPES, BIAS_EXTERNAL, BIAS_METAD_HILLS = 1, 3, 4, 5, 6, 103
 
 
 @dataclass
@@ -169,11 +169,12 @@ def grid_from_hills(centers, heights, sigma, origin, maxv, bins, periodic):
     return grid.ravel()  # C order over reversed axes == column-major over (i0, i1, ...)
 
 
-def blob(opes=(), metad=(), hills=()):
+def blob(opes=(), metad=(), hills=(), pbmetad=(), n_external=0):
     """'GPUS' v1 bias-state blob (CommonSerialization.cpp:20-177 layout).
-    opes : list of dict(nk, sum_uprob, nsamples, mean, m2, centers, sigmas, logw)
-    metad: list of (numDeposited, grid)
-    hills: list of (centers (n,D), heights (n,)) -- extension section 'HILL'."""
+    opes   : list of dict(nk, sum_uprob, nsamples, mean, m2, centers, sigmas, logw)
+    metad  : list of (numDeposited, grid)
+    pbmetad: list of [(numDeposited, sub-grid), ...] per bias
+    hills  : list of (centers (n,D), heights (n,)) -- extension section 'HILL'."""
     out = bytearray(b"GPUS") + struct.pack("<i", 1)
     out += struct.pack("<i", len(opes))
     for o in opes:
@@ -184,7 +185,12 @@ def blob(opes=(), metad=(), hills=()):
     out += struct.pack("<i", len(metad))
     for nd, g in metad:
         out += struct.pack("<i", int(nd)) + np.ascontiguousarray(g, dtype="<f8").tobytes()
-    out += struct.pack("<9i", *([0] * 9))
+    out += struct.pack("<i", len(pbmetad))
+    for subs in pbmetad:
+        out += struct.pack("<i", len(subs))
+        for nd, g in subs:
+            out += struct.pack("<i", int(nd)) + np.ascontiguousarray(g, dtype="<f8").tobytes()
+    out += struct.pack("<8i", int(n_external), *([0] * 7))
     if hills:
         out += b"HILL" + struct.pack("<i", len(hills))
         for c, h in hills:
@@ -211,6 +217,19 @@ def config1(form="grid", n_hills=2000, bins=256):
         biases = [(BIAS_METAD, [0, 1], params, ip)]
         g = grid_from_hills(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
         b = blob(metad=[(n_hills, g)])
+    elif form == "pbmetad":
+        # PBMETAD on the two dihedrals (two periodic 1-D sub-grids holding the
+        # hills' projections, half height each) + an EXTERNAL grid equal to the
+        # 2-D MetaD grid of the same hills
+        params = [h0, gamma, KT300]
+        for d in range(2):
+            params += [sigma[d], lo[d], hi[d]]
+        biases = [(BIAS_PBMETAD, [0, 1], params, [500, bins, 1, bins, 1])]
+        subs = [(n_hills, grid_from_hills(centers[:, d:d + 1], 0.5 * heights, sigma[d:d + 1], lo[d:d + 1],
+                                          hi[d:d + 1], [bins], [1])) for d in range(2)]
+        g = grid_from_hills(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
+        biases.append((BIAS_EXTERNAL, [0, 1], lo + hi + list(g), [bins, bins, 1, 1]))
+        b = blob(pbmetad=[subs], n_external=1)
     else:
         params = [h0] + sigma + [gamma, KT300] + lo + hi
         ip = [500, n_hills + 100000, 1, 1]

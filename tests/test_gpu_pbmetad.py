@@ -176,3 +176,22 @@ def test_mixed_bias_types_vs_oracle():
         assert O.max_rel_force_err(F, r["forces"]) < FORCE_TOL, step
     g, nd = _pb_grid_from_blob(f.getBiasState(), cvs, biases, 6)
     assert nd == orc.bias_state[1]["deposited"] == [9, 9]
+
+
+def test_c1_pbmetad_workload_vs_oracle():
+    """The bench's C1-pbmetad workload (PBMETAD sub-grids loaded from a blob, a
+    256x256 EXTERNAL grid) at its positions and four perturbations of them."""
+    from gluedmd_b200 import workloads as W
+    w = W.config1("pbmetad")
+    n = len(w.positions)
+    orc = O.OracleSystem(w.cvs, w.biases, masses=w.masses, periodic=True, mode="f64", num_particles=n)
+    orc.load_blob(w.blob)
+    ctx, f = _gpu().make_context(w.positions, w.cvs, w.biases, masses=w.masses, pbc=True, box=w.box, blob=w.blob)
+    rng = np.random.default_rng(6)
+    for k in range(5):
+        pos = w.positions + (0 if k == 0 else rng.normal(scale=0.05, size=w.positions.shape))
+        ctx.setPositions(pos)
+        e, F = ctx.computeForces()
+        r = orc.execute(pos, np.asarray(w.box).ravel())
+        assert abs(e - r["energy"]) < 1e-5 * max(1.0, abs(r["energy"])), (k, e, r["energy"])
+        assert O.max_rel_force_err(F, r["forces"]) < FORCE_TOL, k
