@@ -352,6 +352,11 @@ void Context::buildPlan(const GluedForce& f) {
         const int n = (gi.type == CV_COM_DISTANCE ? gi.s2 : gi.s1) - gi.s0;
         groupCached_ = std::max(groupCached_, n);
     }
+    // large COM distance / gyration / RMSD / PCA groups: one CTA cluster per CV
+    groupClustered_ = !groups.empty() && groupCached_ >= 1024;
+    for (const GroupItem& gi : groups)
+        if (gi.type != CV_COM_DISTANCE && gi.type != CV_GYRATION && gi.type != CV_RMSD && gi.type != CV_PCA)
+            groupClustered_ = false;
     G_.atoms = gAtoms_.as<int>(); G_.slots = gSlots_.as<int>();
     G_.mass = gMass_.as<float>(); G_.ref = gRef_.as<float>();
     G_.ev = gEv_.as<float>(); G_.cmPairs = cmPairs_.as<int2>(); G_.cmParams = cmParams_.as<float4>();
@@ -675,7 +680,7 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
     const int* u2g = u2g_.as<int>();
     auto want = [&](int p) { return onlyPhase < 0 || onlyPhase == p; };
     if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
-    if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_);
+    if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_);
     if (want(2) || want(3))
         launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv,
                     onlyPhase < 0 ? 3 : (onlyPhase == 2 ? 1 : 2));

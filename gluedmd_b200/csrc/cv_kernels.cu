@@ -5,11 +5,18 @@
 //                  PCA, path, contact map, Kabsch RMSD) with deterministic block
 //                  reductions instead of the reference's one-thread loops
 //                  (CommonGluedKernels.cpp:456-881, :1236-1323, :1633-1681)
+//   k_group_cvs_cluster: COM distance, gyration, RMSD and PCA over a cluster of
+//                  GROUP_CLUSTER CTAs per CV when the groups are large: each CTA
+//                  gathers and processes a contiguous slice of the atoms, and the
+//                  per-CTA sums are added through distributed shared memory in
+//                  rank order, so every CTA holds the same totals
 //   k_test_force : setTestForce modes 1-3 (CommonGluedKernels.cpp:114-164)
 //   k_invert_index: user -> GPU slot map from OpenMM's atomIndexArray
 // Values go to cvValues (double); Jacobian gradients to the float SoA table whose
 // atom / CV columns are written once when the plan is built.
 #include <algorithm>
+
+#include <cooperative_groups.h>
 
 #include "context.hpp"
 #include "devfn.cuh"
@@ -408,9 +415,197 @@ void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const S
     if (n > 0) launchPdl(k_simple_cvs, dim3((n + 127) / 128), dim3(128), 0, s, posq, u2g, items, n, box, cvv, J);
 }
 
+// Cluster form of the slice-able group CVs (CommonGluedKernels.cpp:456-639,
+// :796-881, :1633-1681). The atoms of the CV, [s0, s1) or [s0, s2) for a COM
+// distance, are split into GROUP_CLUSTER contiguous slices, one per CTA of the
+// cluster; a CTA gathers its slice into shared memory, sums it with the fixed
+// block tree, and clusterSum adds the CTAs' sums in rank order through
+// distributed shared memory. Each reduction has its own buffer, so one cluster
+// barrier per reduction suffices; a last barrier keeps every CTA's buffers alive
+// until the others have read them.
+constexpr int GROUP_CLUSTER = 8;
+
+namespace cg = cooperative_groups;
+
+template <int NV>
+__device__ __forceinline__ void clusterSum(double (&v)[NV], double* part, double* bcast) {
+    cg::cluster_group cluster = cg::this_cluster();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) part[k] = v[k];
+    cluster.sync();
+    if (threadIdx.x == 0) {
+        double t[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) t[k] = 0.0;
+        for (int r = 0; r < GROUP_CLUSTER; r++) {
+            const double* remote = cluster.map_shared_rank(part, r);
+#pragma unroll
+            for (int k = 0; k < NV; k++) t[k] += remote[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) bcast[k] = t[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = bcast[k];
+    __syncthreads();
+}
+
+__global__ void __cluster_dims__(GROUP_CLUSTER, 1, 1) __launch_bounds__(GROUP_THREADS)
+    k_group_cvs_cluster(const float4* __restrict__ posq, const GroupDev G, const BoxDev* __restrict__ boxp,
+                        double* __restrict__ cvv, JacDev J) {
+    pdlEnter();
+    extern __shared__ float4 sPos[];
+    __shared__ double red[32 * 8];
+    __shared__ double part[2][8];
+    __shared__ double bcast[8];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const GroupItem it = G.items[blockIdx.x / GROUP_CLUSTER];
+    const BoxDev box = *boxp;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int a0 = it.s0, a1 = it.type == CV_COM_DISTANCE ? it.s2 : it.s1;
+    const int L = (a1 - a0 + GROUP_CLUSTER - 1) / GROUP_CLUSTER;
+    const int b0 = min(a0 + rank * L, a1), b1 = min(b0 + L, a1);
+    const bool cached = L <= GROUP_CACHE;
+    const bool withMass = it.type == CV_COM_DISTANCE || it.type == CV_GYRATION;
+    if (cached) {
+        const int n = b1 - b0;
+        for (int base = tid; base < n; base += nt * GATHER_U) {
+            int slot[GATHER_U];
+            float m[GATHER_U];
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++) {
+                const int j = base + nt * u;
+                slot[u] = j < n ? __ldg(G.slots + b0 + j) : -1;
+                m[u] = (withMass && j < n) ? __ldg(G.mass + b0 + j) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < GATHER_U; u++)
+                if (slot[u] >= 0) {
+                    float4 p = __ldg(posq + slot[u]);
+                    p.w = m[u];
+                    sPos[base + nt * u] = p;
+                }
+        }
+        __syncthreads();
+    }
+    auto pos = [&](int j) -> F3 {
+        if (cached) { const float4 p = sPos[j - b0]; return f3(p.x, p.y, p.z); }
+        return loadPos(posq, nullptr, G.slots[j]);
+    };
+    auto massAt = [&](int j) -> float { return cached ? sPos[j - b0].w : G.mass[j]; };
+    const bool lead = rank == 0 && tid == 0;
+
+    if (it.type == CV_COM_DISTANCE) {
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 p = pos(j);
+            double m = massAt(j);
+            int o = j < it.s1 ? 0 : 3;
+            v[o] += m * p.x; v[o + 1] += m * p.y; v[o + 2] += m * p.z;
+        }
+        blockSum<6>(v, red);
+        clusterSum<6>(v, part[0], bcast);
+        float i1 = 1.0f / it.f0, i2 = 1.0f / it.f1;
+        F3 c1 = f3((float)v[0] * i1, (float)v[1] * i1, (float)v[2] * i1);
+        F3 c2 = f3((float)v[3] * i2, (float)v[4] * i2, (float)v[5] * i2);
+        F3 d = minImage(sub3(c2, c1), box);
+        float dist = sqrtf(dot3(d, d));
+        float inv = dist > 1e-10f ? 1.0f / dist : 0.0f;
+        if (lead) cvv[it.cv] = (double)dist;
+        for (int j = b0 + tid; j < b1; j += nt) {
+            bool g1 = j < it.s1;
+            float w = massAt(j) / (g1 ? it.f0 : it.f1);
+            float sc = g1 ? -inv * w : inv * w;
+            int r = it.jac0 + j;
+            J.gx[r] = d.x * sc; J.gy[r] = d.y * sc; J.gz[r] = d.z * sc;
+        }
+    } else if (it.type == CV_GYRATION) {
+        double v[3] = {0, 0, 0};
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 p = pos(j);
+            double m = massAt(j);
+            v[0] += m * p.x; v[1] += m * p.y; v[2] += m * p.z;
+        }
+        blockSum<3>(v, red);
+        clusterSum<3>(v, part[0], bcast);
+        float iM = 1.0f / it.f0;
+        F3 com = f3((float)v[0] * iM, (float)v[1] * iM, (float)v[2] * iM);
+        double q[1] = {0};
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 d = minImage(sub3(pos(j), com), box);
+            q[0] += (double)massAt(j) * (double)dot3(d, d);
+        }
+        blockSum<1>(q, red);
+        clusterSum<1>(q, part[1], bcast);
+        float rg = (float)sqrt(q[0] / (double)it.f0);
+        float irg = rg > 1e-10f ? 1.0f / rg : 0.0f;
+        if (lead) cvv[it.cv] = (double)rg;
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 d = minImage(sub3(pos(j), com), box);
+            float w = massAt(j) / it.f0;
+            int r = it.jac0 + j;
+            J.gx[r] = w * d.x * irg; J.gy[r] = w * d.y * irg; J.gz[r] = w * d.z * irg;
+        }
+    } else if (it.type == CV_RMSD) {
+        double q[1] = {0};
+#pragma unroll 4
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 p = pos(j);
+            F3 d = f3(p.x - G.ref[3 * j], p.y - G.ref[3 * j + 1], p.z - G.ref[3 * j + 2]);
+            q[0] += (double)dot3(d, d);
+        }
+        blockSum<1>(q, red);
+        clusterSum<1>(q, part[0], bcast);
+        int na = it.s1 - it.s0;
+        float rmsd = (float)sqrt(q[0] / na);
+        float sc = (rmsd > 1e-10f ? 1.0f / rmsd : 0.0f) / (float)na;
+        if (lead) cvv[it.cv] = (double)rmsd;
+#pragma unroll 4
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 p = pos(j);
+            int r = it.jac0 + j;
+            J.gx[r] = (p.x - G.ref[3 * j]) * sc; J.gy[r] = (p.y - G.ref[3 * j + 1]) * sc;
+            J.gz[r] = (p.z - G.ref[3 * j + 2]) * sc;
+        }
+    } else {  // CV_PCA
+        double q[1] = {0};
+#pragma unroll 4
+        for (int j = b0 + tid; j < b1; j += nt) {
+            F3 p = pos(j);
+            float dx = p.x - G.ref[3 * j], dy = p.y - G.ref[3 * j + 1], dz = p.z - G.ref[3 * j + 2];
+            q[0] += (double)(dx * G.ev[3 * j] + dy * G.ev[3 * j + 1] + dz * G.ev[3 * j + 2]);
+        }
+        blockSum<1>(q, red);
+        clusterSum<1>(q, part[0], bcast);
+        if (lead) cvv[it.cv] = q[0];
+        for (int j = b0 + tid; j < b1; j += nt) {
+            int r = it.jac0 + j;
+            J.gx[r] = G.ev[3 * j]; J.gy[r] = G.ev[3 * j + 1]; J.gz[r] = G.ev[3 * j + 2];
+        }
+    }
+    cluster.sync();
+}
+
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
-                    double* cvv, const JacDev& J, int maxCached) {
+                    double* cvv, const JacDev& J, int maxCached, bool clustered) {
     if (G.numItems <= 0) return;
+    if (clustered) {
+        const int slice = (std::max(maxCached, 1) + GROUP_CLUSTER - 1) / GROUP_CLUSTER;
+        const size_t smem = sizeof(float4) * (size_t)std::min(slice, GROUP_CACHE);
+        static bool cattr = false;
+        if (!cattr) {
+            cudaCheck(cudaFuncSetAttribute((const void*)k_group_cvs_cluster,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(float4) * GROUP_CACHE)), "group CV shared memory");
+            cattr = true;
+        }
+        launchPdl(k_group_cvs_cluster, dim3(G.numItems * GROUP_CLUSTER), dim3(GROUP_THREADS), smem, s, posq, G,
+                  box, cvv, J);
+        return;
+    }
     const size_t smem = sizeof(float4) * (size_t)std::min(std::max(maxCached, 1), GROUP_CACHE);
     static bool attr = false;
     if (!attr) {
