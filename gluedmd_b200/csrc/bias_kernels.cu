@@ -161,34 +161,52 @@ __device__ __noinline__ void evalPbmetad(const BiasDev& b, const double* cvv, do
 // for OPES), spread over KSUM_CTAS CTAs per bias: each CTA sums a contiguous
 // range of kernels (per thread, then a fixed block tree) into 9 FP64 partials
 // {dV/ds_0..7 terms, value}; k_biases sums the partials in CTA order.
+//
+// The kernel tables (count, centres, sigmas, log-weights; hill centres and
+// heights) are written only by the deposit kernels of updateState, which have
+// completed before this launch can start (the kernel it depends on has passed
+// its own wait, or is a plain launch); so the record, the count and each
+// thread's first OPES kernel are loaded before the wait, and only the CV values
+// of the kernel before are read after it.
 __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__ biases,
                                                       const double* __restrict__ cvv, double* __restrict__ part) {
-    pdlEnter();
     __shared__ double red[32 * 9];
     const BiasDev& b = biases[blockIdx.y];
-    if (b.type != BIAS_OPES && b.type != BIAS_METAD_HILLS) return;  // uniform over the CTA
+    const int type = b.type;
+    if (type != BIAS_OPES && type != BIAS_METAD_HILLS) {
+        pdlEnter();
+        return;  // uniform over the CTA
+    }
     const int tid = threadIdx.x, nt = blockDim.x;
     const int D = b.D;
-    const int K = b.type == BIAS_OPES ? *b.numKernels : *b.hCount;
+    const int K = type == BIAS_OPES ? *b.numKernels : *b.hCount;
     const int k0 = (int)((long long)K * blockIdx.x / gridDim.x);
     const int k1 = (int)((long long)K * (blockIdx.x + 1) / gridDim.x);
+    double pc[8], ps[8], plw = 0.0;
+    const int kf = k0 + tid;
+    if (type == BIAS_OPES && kf < k1) {
+        for (int d = 0; d < D; d++) { pc[d] = b.centers[kf * D + d]; ps[d] = b.sigmas[kf * D + d]; }
+        plw = b.logW[kf];
+    }
+    pdlEnter();
     double s[8];
     for (int d = 0; d < D; d++) s[d] = cvv[b.cvIdx[d]];
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (b.type == BIAS_OPES) {
+    if (type == BIAS_OPES) {
         const double kfloor = exp(-0.5 * b.cutoff2);
-        for (int k = k0 + tid; k < k1; k += nt) {
+        for (int k = kf; k < k1; k += nt) {
+            const bool first = k == kf;
             double n2 = 0, dc[8], is2[8];
             for (int d = 0; d < D; d++) {
-                dc[d] = s[d] - b.centers[k * D + d];
-                double sg = b.sigmas[k * D + d];
+                dc[d] = s[d] - (first ? pc[d] : b.centers[k * D + d]);
+                double sg = first ? ps[d] : b.sigmas[k * D + d];
                 is2[d] = 1.0 / (sg * sg);
                 n2 += dc[d] * dc[d] * is2[d];
             }
             if (!(n2 < b.cutoff2)) continue;
             double G = exp(-0.5 * n2), kern = G - kfloor;
             if (kern <= 0.0) continue;
-            double h = exp(b.logW[k]);
+            double h = exp(first ? plw : b.logW[k]);
             if (!(h > 0.0 && h < 1e308)) continue;
             acc[8] += h * kern;
             for (int d = 0; d < D; d++) acc[d] += h * G * (-dc[d] * is2[d]);
@@ -241,6 +259,14 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbia
         for (int i = tid; i < words; i += nt) dst[i] = src[i];
         biases = rec;
     }
+    // OPES kernel counts and sum_uprob are written by the deposits only (see
+    // k_kernel_sums): read them before the wait, one thread per bias
+    __shared__ int sK[16];
+    __shared__ double sSu[16];
+    if (tid < nb && tid < 16 && gbiases[tid].type == BIAS_OPES) {
+        sK[tid] = *gbiases[tid].numKernels;
+        sSu[tid] = *gbiases[tid].sumUprob;
+    }
     pdlEnter();
     for (int i = tid; i < numCVs; i += nt) sG[i] = testGrad ? testGrad[i] : 0.0;
     __syncthreads();
@@ -289,7 +315,7 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbia
                         b.runM2[d] += dl * (x - b.runMean[d]);
                     }
                 }
-                const int K = *b.numKernels;
+                const int K = bi < 16 ? sK[bi] : *b.numKernels;
                 if (K == 0) {
                     if (tid == 0) energies[b.slot] = -b.barrier;
                 } else {
@@ -300,7 +326,7 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbia
                     blockSum<9>(acc, red);
                     if (tid == 0) {
                         double prob = acc[8];
-                        double su = *b.sumUprob;
+                        double su = bi < 16 ? sSu[bi] : *b.sumUprob;
                         double pz = su > 0.0 ? prob * (double)K / su : 0.0;
                         if (!(pz >= 0.0)) pz = 0.0;
                         double arg = pz + b.eps;
