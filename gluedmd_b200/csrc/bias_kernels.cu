@@ -360,14 +360,25 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbia
     for (int i = tid; i < numCVs; i += nt) dUdCV[i] = sG[i];
 }
 
+// The atom and CV columns of the Jacobian rows are written once when the plan is
+// built and the user -> slot map at bind / reorder, long before this launch: the
+// first row of every thread resolves its slot before the wait; the gradients and
+// dU/dCV of this step are read after it.
 __global__ void k_scatter(JacDev J, const int* __restrict__ u2g, const double* __restrict__ dUdCV,
                           unsigned long long* __restrict__ force, int padded) {
+    const int rf = blockIdx.x * blockDim.x + threadIdx.x;
+    int cvf = 0, af = 0;
+    if (rf < J.rows) {
+        cvf = J.cv[rf];
+        af = u2g[J.atom[rf]];
+    }
     pdlEnter();
     const double S = 4294967296.0;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < J.rows; r += gridDim.x * blockDim.x) {
-        double g = dUdCV[J.cv[r]];
+    for (int r = rf; r < J.rows; r += gridDim.x * blockDim.x) {
+        const bool first = r == rf;
+        double g = dUdCV[first ? cvf : J.cv[r]];
         if (g == 0.0) continue;  // adds zero in the reference
-        int a = u2g[J.atom[r]];
+        int a = first ? af : u2g[J.atom[r]];
         long long fx = (long long)(-(g * (double)J.gx[r]) * S);
         long long fy = (long long)(-(g * (double)J.gy[r]) * S);
         long long fz = (long long)(-(g * (double)J.gz[r]) * S);
