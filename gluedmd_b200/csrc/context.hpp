@@ -121,6 +121,7 @@ private:
     DBuf biasDev_, mergeFlag_, uprobPartial_, sumPart_;
     bool kernelSums_ = false;
     bool groupClustered_ = false;   // group CVs as one CTA cluster per CV
+    bool groupBeside_ = false;      // group CVs beside the coordination grid
     bool singleLane_ = false;   // any harmonic / MetaD / PBMETAD / EXTERNAL bias
     JacDev J_{};
     int numSimple_ = 0;

@@ -121,11 +121,19 @@ constexpr int GROUP_CACHE = 8192;
 constexpr int GROUP_THREADS = 512;
 constexpr int GATHER_U = 16;
 
+// LATE: launched as the programmatic dependent of the plain-launched coordination
+// grid, on the SMs that grid leaves free; everything it reads was complete before
+// that grid started and it writes nothing the grid reads, so it computes first and
+// waits for the grid only at its end (which keeps the chain's completion order).
+template <bool LATE>
 __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __restrict__ posq,
                                                              const int* __restrict__ u2g, GroupDev G,
                                                              const BoxDev* __restrict__ boxp,
                                                              double* __restrict__ cvv, JacDev J) {
-    pdlEnter();
+    if constexpr (LATE)
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    else
+        pdlEnter();
     extern __shared__ float4 sPos[];
     __shared__ double red[32 * 16];
     __shared__ float wbuf[128];
@@ -381,6 +389,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
             J.gx[r] = (float)g[0]; J.gy[r] = (float)g[1]; J.gz[r] = (float)g[2];
         }
     }
+    if constexpr (LATE) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // setTestForce: mode 1 constant (scale,0,0); mode 2 (userAtom*scale,0,0);
@@ -590,7 +599,7 @@ __global__ void __cluster_dims__(GROUP_CLUSTER, 1, 1) __launch_bounds__(GROUP_TH
 }
 
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
-                    double* cvv, const JacDev& J, int maxCached, bool clustered) {
+                    double* cvv, const JacDev& J, int maxCached, bool clustered, bool late) {
     if (G.numItems <= 0) return;
     if (clustered) {
         const int slice = (std::max(maxCached, 1) + GROUP_CLUSTER - 1) / GROUP_CLUSTER;
@@ -609,11 +618,15 @@ void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const Gr
     const size_t smem = sizeof(float4) * (size_t)std::min(std::max(maxCached, 1), GROUP_CACHE);
     static bool attr = false;
     if (!attr) {
-        cudaCheck(cudaFuncSetAttribute((const void*)k_group_cvs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(sizeof(float4) * GROUP_CACHE)), "group CV shared memory");
+        for (const void* fn : {(const void*)k_group_cvs<false>, (const void*)k_group_cvs<true>})
+            cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(float4) * GROUP_CACHE)), "group CV shared memory");
         attr = true;
     }
-    launchPdl(k_group_cvs, dim3(G.numItems), dim3(GROUP_THREADS), smem, s, posq, u2g, G, box, cvv, J);
+    if (late)
+        launchPdl(k_group_cvs<true>, dim3(G.numItems), dim3(GROUP_THREADS), smem, s, posq, u2g, G, box, cvv, J);
+    else
+        launchPdl(k_group_cvs<false>, dim3(G.numItems), dim3(GROUP_THREADS), smem, s, posq, u2g, G, box, cvv, J);
 }
 
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,

@@ -13,7 +13,8 @@ void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const S
                      const BoxDev* box, double* cvv, const JacDev& J);
 // maxCached: the largest atom range of a cached group CV (shared memory size).
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
-                    double* cvv, const JacDev& J, int maxCached, bool clustered);
+                    double* cvv, const JacDev& J, int maxCached, bool clustered,
+                    bool late);
 void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, long long* force, int padded,
                      int numAtoms, int mode, double scale, const BoxDev* box);
 // Coordination runs (coord_run.cuh). parts: bit 0 = pair runs, bit 1 = finalize

@@ -85,3 +85,32 @@ def test_cluster_forces_repeatable():
     e1, F1 = ctx.computeForces()
     e2, F2 = ctx.computeForces()
     assert np.array_equal(F1, F2)
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_group_cvs_beside_coordination(periodic):
+    """Coordination with a few single-CTA group CVs: the group kernel runs beside
+    the coordination grid on the SMs it leaves free (launched after it, waiting
+    for it only at its end); values and forces vs the FP64 oracle, and bitwise
+    repeatable."""
+    rng = np.random.default_rng(12)
+    n, box = 6000, 4.0
+    pos = rng.uniform(0, box, (n, 3))
+    perm = [int(x) for x in rng.permutation(n)]
+    A, B = perm[:300], perm[300:1500]
+    r = perm[1500:2300]
+    cvs = [(O.CV_COORDINATION, [len(A)] + A + B, [0.35, 6, 12]),
+           (O.CV_RMSD, r, list((pos[r] + rng.normal(0, 0.1, (len(r), 3))).ravel())),
+           (O.CV_GYRATION, perm[2300:2900], []),
+           (O.CV_COM_DISTANCE, perm[2900:3100] + perm[3100:3500], [200])]
+    masses = rng.uniform(1, 16, n)
+    g = [0.01, 0.8, -0.6, 0.4]
+    ref = O.OracleSystem(cvs, masses=masses, periodic=periodic, mode="f64", test_bias_gradients=g,
+                         num_particles=n).execute(pos, np.diag([box] * 3).ravel())
+    import gpu_util
+    ctx, f = gpu_util.make_context(pos, cvs, masses=masses, pbc=periodic, box=np.diag([box] * 3), grad=g)
+    e, F = ctx.computeForces()
+    np.testing.assert_allclose(np.array(f.getLastCVValues(ctx)), ref["cv_values"], rtol=1e-5, atol=1e-5)
+    assert O.max_rel_force_err(F, ref["forces"]) < FORCE_TOL
+    _, F2 = ctx.computeForces()
+    assert np.array_equal(F, F2)
