@@ -48,18 +48,20 @@ __global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
 
 // Fixed-point sums -> float Jacobian rows (one thread per row and component),
 // every accumulator read is cleared; CN values = sums of the run pieces' partials
-// in step order.
+// in step order. The item of each row comes from the item table, written when
+// the plan is built, and is looked up before the wait.
 __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* __restrict__ cvv, int totalRows) {
-    pdlEnter();
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid < 3 * totalRows) {
-        const int comp = gid % 3;
-        const int row = gid / 3;
-        int ii = 0, base = 0;
-        while (ii < numItems - 1 && row >= base + R.items[ii].nA + R.items[ii].nB) {
+    int ii = 0, base = 0;
+    if (gid < 3 * totalRows)
+        while (ii < numItems - 1 && gid / 3 >= base + R.items[ii].nA + R.items[ii].nB) {
             base += R.items[ii].nA + R.items[ii].nB;
             ii++;
         }
+    pdlEnter();
+    if (gid < 3 * totalRows) {
+        const int comp = gid % 3;
+        const int row = gid / 3;
         const CoordItem& it = R.items[ii];
         unsigned long long* a = R.acc + 3 * (size_t)row + comp;
         const long long v = (long long)*a;
