@@ -377,10 +377,14 @@ void Context::buildPlan(const GluedForce& f) {
         cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
         const int occ = coordRunOccupancy(coordKind_, periodic_ ? 1 : 0, true);
         coordGrid_ = sms * occ;
-        // a few single-CTA group CVs run beside the coordination grid, on SMs it
-        // leaves free (one CTA per SM fills an SM's registers)
+        // the distance/angle/dihedral kernel (up to 256 CVs) and a few single-CTA
+        // group CVs run beside the coordination grid, on SMs it leaves free (one
+        // coordination CTA per SM fills an SM's registers)
+        const int simpleCtas = (numSimple_ + 127) / 128;
+        simpleBeside_ = numSimple_ > 0 && simpleCtas <= 2 && occ == 1 && sms > 8;
         groupBeside_ = G_.numItems > 0 && G_.numItems <= 4 && !groupClustered_ && occ == 1 && sms > 8;
-        if (groupBeside_) coordGrid_ = sms - G_.numItems;
+        const int beside = (simpleBeside_ ? simpleCtas : 0) + (groupBeside_ ? G_.numItems : 0);
+        if (beside > 0) coordGrid_ = sms - beside;
         coordGrid_ = std::max(1, std::min(coordGrid_, (int)coordStepsH_.size()));
         std::vector<int> begin = balanceRanges((int)coordStepsH_.size(), coordGrid_, {});
         const int pieces = buildCoordPieces(coordStepsH_, begin, coord);
@@ -678,21 +682,24 @@ void Context::setBox(const double box[9]) {
 // ---------------------------------------------------------------- execute
 // Launch groups of one force evaluation, in order:
 //   0 simple CVs, 1 group CVs, 2 coordination pairs, 3 coordination finalize,
-//   4 biases, 5 scatter; with groupBeside_ the group CVs come after the pairs
-//   and run on the SMs the pair grid leaves free. onlyPhase >= 0 enqueues a
-//   single group (profiling).
+//   4 biases, 5 scatter; with simpleBeside_ / groupBeside_ those CV kernels come
+//   after the pairs and run on the SMs the pair grid leaves free. onlyPhase >= 0
+//   enqueues a single group (profiling).
 void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) {
     const BoxDev* box = box_.as<BoxDev>();
     double* cvv = cvv_.as<double>();
     const int* u2g = u2g_.as<int>();
     auto want = [&](int p) { return onlyPhase < 0 || onlyPhase == p; };
-    if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_);
-    if (groupBeside_ && onlyPhase < 0) {
-        // coordination pairs, the group CVs beside them, then the finalize
+    if ((simpleBeside_ || groupBeside_) && onlyPhase < 0) {
+        // coordination pairs, the CV kernels that fit beside them, then the finalize
+        if (!simpleBeside_) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, false);
+        if (!groupBeside_) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, false);
         launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 1);
-        launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, true);
+        if (simpleBeside_) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, true);
+        if (groupBeside_) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, true);
         launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 2);
     } else {
+        if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, false);
         if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, false);
         if (want(2) || want(3))
             launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv,

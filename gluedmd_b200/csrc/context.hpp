@@ -122,6 +122,7 @@ private:
     bool kernelSums_ = false;
     bool groupClustered_ = false;   // group CVs as one CTA cluster per CV
     bool groupBeside_ = false;      // group CVs beside the coordination grid
+    bool simpleBeside_ = false;     // distance/angle/dihedral beside the coordination grid
     bool singleLane_ = false;   // any harmonic / MetaD / PBMETAD / EXTERNAL bias
     JacDev J_{};
     int numSimple_ = 0;

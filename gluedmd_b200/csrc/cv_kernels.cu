@@ -34,12 +34,9 @@ __global__ void k_invert_index(const int* __restrict__ atomIndex, int* __restric
     }
 }
 
-__global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restrict__ u2g,
-                             const SimpleItem* __restrict__ items, int n, const BoxDev* __restrict__ boxp,
-                             double* __restrict__ cvv, JacDev J) {
-    pdlEnter();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ void simpleCvItem(const float4* __restrict__ posq, const int* __restrict__ u2g,
+                                             const SimpleItem* __restrict__ items, int i,
+                                             const BoxDev* __restrict__ boxp, double* __restrict__ cvv, JacDev& J) {
     const BoxDev box = *boxp;
     SimpleItem it = items[i];
     int r = it.jac0;
@@ -90,6 +87,21 @@ __global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restr
         J.gx[r + 2] = -(jA.x + jB.x + jD.x); J.gy[r + 2] = -(jA.y + jB.y + jD.y); J.gz[r + 2] = -(jA.z + jB.z + jD.z);
         J.gx[r + 3] = jD.x; J.gy[r + 3] = jD.y; J.gz[r + 3] = jD.z;
     }
+}
+
+// LATE: launched beside the plain-launched coordination grid, as for the group
+// CVs (k_group_cvs): computes first, waits for the grid only at its end.
+template <bool LATE>
+__global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restrict__ u2g,
+                             const SimpleItem* __restrict__ items, int n, const BoxDev* __restrict__ boxp,
+                             double* __restrict__ cvv, JacDev J) {
+    if constexpr (LATE)
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    else
+        pdlEnter();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) simpleCvItem(posq, u2g, items, i, boxp, cvv, J);
+    if constexpr (LATE) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // ---------------------------------------------------------------- group CVs
@@ -420,8 +432,12 @@ void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n) {
 }
 
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
-                     const BoxDev* box, double* cvv, const JacDev& J) {
-    if (n > 0) launchPdl(k_simple_cvs, dim3((n + 127) / 128), dim3(128), 0, s, posq, u2g, items, n, box, cvv, J);
+                     const BoxDev* box, double* cvv, const JacDev& J, bool late) {
+    if (n <= 0) return;
+    if (late)
+        launchPdl(k_simple_cvs<true>, dim3((n + 127) / 128), dim3(128), 0, s, posq, u2g, items, n, box, cvv, J);
+    else
+        launchPdl(k_simple_cvs<false>, dim3((n + 127) / 128), dim3(128), 0, s, posq, u2g, items, n, box, cvv, J);
 }
 
 // Cluster form of the slice-able group CVs (CommonGluedKernels.cpp:456-639,

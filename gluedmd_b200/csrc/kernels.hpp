@@ -10,7 +10,8 @@ namespace glued {
 
 void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n);
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
-                     const BoxDev* box, double* cvv, const JacDev& J);
+                     const BoxDev* box, double* cvv, const JacDev& J,
+                     bool late);
 // maxCached: the largest atom range of a cached group CV (shared memory size).
 void launchGroupCVs(cudaStream_t s, const float4* posq, const int* u2g, const GroupDev& G, const BoxDev* box,
                     double* cvv, const JacDev& J, int maxCached, bool clustered,
