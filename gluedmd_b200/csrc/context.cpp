@@ -645,6 +645,7 @@ void Context::atomsReordered() {
     launchInvertIndex(stream_, atomIndex_, u2g_.as<int>(), numParticles_);
     launchComposeSlots(stream_, coordAtoms_.as<int>(), u2g_.as<int>(), coordSlots_.as<int>(), coordAtomsN_);
     launchComposeSlots(stream_, gAtoms_.as<int>(), u2g_.as<int>(), gSlots_.as<int>(), gAtomsN_);
+    launchComposeSimpleSlots(stream_, simple_.as<SimpleItem>(), u2g_.as<int>(), numSimple_);
     cudaCheck(cudaGetLastError(), "invert index");
 }
 

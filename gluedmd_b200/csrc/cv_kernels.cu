@@ -34,6 +34,16 @@ __global__ void k_invert_index(const int* __restrict__ atomIndex, int* __restric
     }
 }
 
+// slot[k] = u2g[atoms[k]] for the distance / angle / dihedral items: the posq
+// row of each atom, rebuilt whenever OpenMM reorders atoms, so the CV kernel
+// reads positions without the map.
+__global__ void k_compose_simple_slots(SimpleItem* __restrict__ items, const int* __restrict__ u2g, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int na = items[i].type == CV_DISTANCE ? 2 : items[i].type == CV_ANGLE ? 3 : 4;
+    for (int k = 0; k < na; k++) items[i].slot[k] = u2g[items[i].atoms[k]];
+}
+
 __device__ __forceinline__ void simpleCvItem(const float4* __restrict__ posq, const int* __restrict__ u2g,
                                              const SimpleItem* __restrict__ items, int i,
                                              const BoxDev* __restrict__ boxp, double* __restrict__ cvv, JacDev& J) {
@@ -41,16 +51,16 @@ __device__ __forceinline__ void simpleCvItem(const float4* __restrict__ posq, co
     SimpleItem it = items[i];
     int r = it.jac0;
     if (it.type == CV_DISTANCE) {
-        F3 d = minImage(sub3(loadPos(posq, u2g, it.atoms[1]), loadPos(posq, u2g, it.atoms[0])), box);
+        F3 d = minImage(sub3(loadPos(posq, nullptr, it.slot[1]), loadPos(posq, nullptr, it.slot[0])), box);
         float dist = sqrtf(dot3(d, d));
         float inv = dist > 1e-10f ? 1.0f / dist : 0.0f;
         cvv[it.cv] = (double)dist;
         J.gx[r] = -d.x * inv; J.gy[r] = -d.y * inv; J.gz[r] = -d.z * inv;
         J.gx[r + 1] = d.x * inv; J.gy[r + 1] = d.y * inv; J.gz[r + 1] = d.z * inv;
     } else if (it.type == CV_ANGLE) {
-        F3 pb = loadPos(posq, u2g, it.atoms[1]);
-        F3 d1 = minImage(sub3(loadPos(posq, u2g, it.atoms[0]), pb), box);
-        F3 d2 = minImage(sub3(loadPos(posq, u2g, it.atoms[2]), pb), box);
+        F3 pb = loadPos(posq, nullptr, it.slot[1]);
+        F3 d1 = minImage(sub3(loadPos(posq, nullptr, it.slot[0]), pb), box);
+        F3 d2 = minImage(sub3(loadPos(posq, nullptr, it.slot[2]), pb), box);
         float r1 = sqrtf(dot3(d1, d1)), r2 = sqrtf(dot3(d2, d2));
         float i1 = r1 > 1e-10f ? 1.0f / r1 : 0.0f, i2 = r2 > 1e-10f ? 1.0f / r2 : 0.0f;
         F3 n1 = f3(d1.x * i1, d1.y * i1, d1.z * i1), n2 = f3(d2.x * i2, d2.y * i2, d2.z * i2);
@@ -66,8 +76,8 @@ __device__ __forceinline__ void simpleCvItem(const float4* __restrict__ posq, co
         J.gx[r + 1] = -(jA.x + jC.x); J.gy[r + 1] = -(jA.y + jC.y); J.gz[r + 1] = -(jA.z + jC.z);
         J.gx[r + 2] = jC.x; J.gy[r + 2] = jC.y; J.gz[r + 2] = jC.z;
     } else {  // dihedral, Blondel-Karplus
-        F3 pa = loadPos(posq, u2g, it.atoms[0]), pb = loadPos(posq, u2g, it.atoms[1]);
-        F3 pc = loadPos(posq, u2g, it.atoms[2]), pd = loadPos(posq, u2g, it.atoms[3]);
+        F3 pa = loadPos(posq, nullptr, it.slot[0]), pb = loadPos(posq, nullptr, it.slot[1]);
+        F3 pc = loadPos(posq, nullptr, it.slot[2]), pd = loadPos(posq, nullptr, it.slot[3]);
         F3 b1 = minImage(sub3(pb, pa), box), b2 = minImage(sub3(pc, pb), box), b3 = minImage(sub3(pd, pc), box);
         F3 t = cross3(b1, b2), u = cross3(b2, b3);
         float d = sqrtf(dot3(b2, b2));
@@ -429,6 +439,10 @@ __global__ void k_test_force(const float4* __restrict__ posq, const int* __restr
 // ------------------------------------------------------------------ launchers
 void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n) {
     if (n > 0) k_invert_index<<<(n + 255) / 256, 256, 0, s>>>(atomIndex, u2g, n);
+}
+
+void launchComposeSimpleSlots(cudaStream_t s, SimpleItem* items, const int* u2g, int n) {
+    if (n > 0) k_compose_simple_slots<<<(n + 127) / 128, 128, 0, s>>>(items, u2g, n);
 }
 
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,

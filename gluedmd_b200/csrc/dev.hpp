@@ -33,7 +33,8 @@ struct SimpleItem {
     int type;
     int cv;
     int jac0;
-    int atoms[4];
+    int atoms[4];   // user atom indices
+    int slot[4];    // their posq rows (rebuilt on reorder)
 };
 
 // CVs reduced by one CTA each. Field use per type:

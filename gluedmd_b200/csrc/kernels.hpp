@@ -9,6 +9,7 @@
 namespace glued {
 
 void launchInvertIndex(cudaStream_t s, const int* atomIndex, int* u2g, int n);
+void launchComposeSimpleSlots(cudaStream_t s, SimpleItem* items, const int* u2g, int n);
 void launchSimpleCVs(cudaStream_t s, const float4* posq, const int* u2g, const SimpleItem* items, int n,
                      const BoxDev* box, double* cvv, const JacDev& J,
                      bool late);
