@@ -93,8 +93,23 @@ __global__ void k_ad_cmap(AdSpec S, double* part, int nPart, double* out) {
     }
 }
 
+// Positions, frames and the hill table are the caller's inputs, complete before
+// the first kernel of the step passed its wait; the kernels after it load their
+// share of them before their own wait and read only the previous kernel's
+// output after it.
+constexpr int AD_HP = 4;   // hills per thread loaded before the wait
+
 template <class R>
 __global__ void __launch_bounds__(512) k_ad_path_hills(AdSpec S, const double* part, int nPart, double* out) {
+    const R* h = static_cast<const R*>(S.heights);
+    double pc0[AD_HP], pc1[AD_HP], ph[AD_HP];
+#pragma unroll
+    for (int u = 0; u < AD_HP; u++) {
+        const int k = threadIdx.x + u * blockDim.x;
+        pc0[u] = k < S.K ? S.hillC[2 * k] : 0.0;
+        pc1[u] = k < S.K ? S.hillC[2 * k + 1] : 0.0;
+        ph[u] = k < S.K ? (double)h[k] : 0.0;
+    }
     pdlEnter();
     __shared__ double red[32 * 3];
     __shared__ double sw[128];
@@ -115,15 +130,19 @@ __global__ void __launch_bounds__(512) k_ad_path_hills(AdSpec S, const double* p
     }
     __syncthreads();
     const double cm = bc[0], s = bc[1];
-    const R* h = static_cast<const R*>(S.heights);
     double v[3] = {0, 0, 0};
-    for (int k = tid; k < S.K; k += blockDim.x) {
-        double d0 = cm - S.hillC[2 * k], d1 = s - S.hillC[2 * k + 1];
-        double g = (double)h[k] * exp(-d0 * d0 / (2 * S.sig[0] * S.sig[0]) - d1 * d1 / (2 * S.sig[1] * S.sig[1]));
+    auto hill = [&](double c0, double c1, double hk) {
+        double d0 = cm - c0, d1 = s - c1;
+        double g = hk * exp(-d0 * d0 / (2 * S.sig[0] * S.sig[0]) - d1 * d1 / (2 * S.sig[1] * S.sig[1]));
         v[0] += g;
         v[1] += -g * d0 / (S.sig[0] * S.sig[0]);
         v[2] += -g * d1 / (S.sig[1] * S.sig[1]);
-    }
+    };
+#pragma unroll
+    for (int u = 0; u < AD_HP; u++)
+        if (tid + u * (int)blockDim.x < S.K) hill(pc0[u], pc1[u], ph[u]);
+    for (int k = tid + AD_HP * blockDim.x; k < S.K; k += blockDim.x)
+        hill(S.hillC[2 * k], S.hillC[2 * k + 1], (double)h[k]);
     blockSum<3>(v, red);
     if (tid == 0) {
         out[0] = v[0]; out[1] = cm; out[2] = s; out[3] = bc[2]; out[4] = bc[3];
@@ -160,9 +179,18 @@ __global__ void k_ad_back_pairs(AdSpec S, const double* out, const double* gE, l
 
 template <class R>
 __global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, long long* acc, R* gFrames) {
-    pdlEnter();
     const R* pos = static_cast<const R*>(S.pos);
     const R* fr = static_cast<const R*>(S.frames);
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    double dx0[3] = {0, 0, 0};
+    int a0 = 0;
+    if (t0 < S.M * S.F) {
+        const int f = t0 / S.M, j = t0 % S.M;
+        a0 = S.pathAtoms[j];
+        for (int c = 0; c < 3; c++)
+            dx0[c] = (double)pos[3 * a0 + c] - (double)fr[((size_t)f * S.M + j) * 3 + c];
+    }
+    pdlEnter();
     const double gS = gE[0] * out[6 + S.F];
     const double s = out[2], Ssum = out[4];
     const double* w = out + 5;
@@ -170,10 +198,11 @@ __global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, lo
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < S.M * S.F; t += gridDim.x * blockDim.x) {
         // thread per (frame, atom): d s / d ref_fj = sc (f+1-s) w_f (x_j - ref_fj)
         int f = t / S.M, j = t % S.M;
-        int a = S.pathAtoms[j];
+        const bool first = t == t0;
+        int a = first ? a0 : S.pathAtoms[j];
         double k = gS * sc * ((f + 1) - s) * w[f];
         for (int c = 0; c < 3; c++) {
-            double dx = (double)pos[3 * a + c] - (double)fr[((size_t)f * S.M + j) * 3 + c];
+            double dx = first ? dx0[c] : (double)pos[3 * a + c] - (double)fr[((size_t)f * S.M + j) * 3 + c];
             gFrames[((size_t)f * S.M + j) * 3 + c] = (R)(k * dx);
             // d s / d x_j = -(that), summed over frames into the atom's gradient
             long long q = __double2ll_rn(-k * dx * kFix);
@@ -185,10 +214,13 @@ __global__ void k_ad_back_path(AdSpec S, const double* out, const double* gE, lo
 template <class R>
 __global__ void k_ad_back_hills_and_convert(AdSpec S, const double* out, const double* gE, const long long* acc,
                                             R* gPos, R* gH) {
+    const int k0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const double c00 = k0 < S.K ? S.hillC[2 * k0] : 0.0, c01 = k0 < S.K ? S.hillC[2 * k0 + 1] : 0.0;
     pdlEnter();
     const double cm = out[1], s = out[2];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.K; k += gridDim.x * blockDim.x) {
-        double d0 = cm - S.hillC[2 * k], d1 = s - S.hillC[2 * k + 1];
+    for (int k = k0; k < S.K; k += gridDim.x * blockDim.x) {
+        const bool first = k == k0;
+        double d0 = cm - (first ? c00 : S.hillC[2 * k]), d1 = s - (first ? c01 : S.hillC[2 * k + 1]);
         gH[k] = (R)(gE[0] * exp(-d0 * d0 / (2 * S.sig[0] * S.sig[0]) - d1 * d1 / (2 * S.sig[1] * S.sig[1])));
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * S.nAtoms; i += gridDim.x * blockDim.x)
