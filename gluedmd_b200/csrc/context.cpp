@@ -344,6 +344,8 @@ void Context::buildPlan(const GluedForce& f) {
     gAtoms_.upload(gAtoms); gMass_.upload(gMass); gRef_.upload(gRef); gEv_.upload(gEv);
     cmPairs_.upload(cmPairs); cmParams_.upload(cmParams);
     G_.items = groupItems_.as<GroupItem>(); G_.numItems = (int)groups.size();
+    G_.nInl = std::min((int)groups.size(), 8);
+    for (int k = 0; k < G_.nInl; k++) G_.inl[k] = groups[k];
     gSlots_.alloc(sizeof(int) * std::max((size_t)1, gAtoms.size()));
     gAtomsN_ = (int)gAtoms.size();
     groupCached_ = 1;

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
     __shared__ double red[32 * 16];
     __shared__ float wbuf[128];
     __shared__ double bc[16];
-    const GroupItem it = G.items[blockIdx.x];
+    const GroupItem it = (int)blockIdx.x < G.nInl ? G.inl[blockIdx.x] : G.items[blockIdx.x];
     const BoxDev box = *boxp;
     const int tid = threadIdx.x, nt = blockDim.x;
     // atoms read through pos(j): cached when the group fits
@@ -501,7 +501,8 @@ __global__ void __cluster_dims__(GROUP_CLUSTER, 1, 1) __launch_bounds__(GROUP_TH
     __shared__ double bcast[8];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
-    const GroupItem it = G.items[blockIdx.x / GROUP_CLUSTER];
+    const int gi = blockIdx.x / GROUP_CLUSTER;
+    const GroupItem it = gi < G.nInl ? G.inl[gi] : G.items[gi];
     const BoxDev box = *boxp;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int a0 = it.s0, a1 = it.type == CV_COM_DISTANCE ? it.s2 : it.s1;

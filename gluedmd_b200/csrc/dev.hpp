@@ -64,6 +64,10 @@ struct GroupDev {
     const float* ev;       // PCA eigenvectors, xyz per atom
     const int2* cmPairs;
     const float4* cmParams;  // r0, n, m, w
+    // the first GROUP_INLINE items again, inside the kernel's parameter block:
+    // read from the constant bank instead of global memory
+    GroupItem inl[8];
+    int nInl;
 };
 
 // Coordination CVs: all-pairs tiles with deterministic partial sums.
