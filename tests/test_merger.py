@@ -219,3 +219,24 @@ def test_two_rank_gloo_bias_sync():
     # deltas since the shared state: +1 on rank 0, +2 on rank 1; counts 20 - 21 each
     assert nd2 == 21 + (20 - 21) * 2
     np.testing.assert_array_equal(np.frombuffer(g2, "<f8"), np.arange(6) * 3.0 + 3.0)
+
+
+def test_workload_blob_round_trips_through_merger():
+    """The C1-pbmetad bench workload's bias state (written by the workload
+    builder): the merger parses it against the workload's biases, repacks it byte
+    for byte, and the oracle reads the same sub-grids from it."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+    import oracle as O
+    from gluedmd_b200 import workloads as W
+    w = W.config1("pbmetad")
+    force = FakeForce([(t, c, p, ip) for t, c, p, ip in w.biases])
+    parsed = M._parse(w.blob, force)
+    assert M._pack(parsed) == w.blob
+    assert parsed["n_external"] == 1 and len(parsed["pbmetad"]) == 1 and len(parsed["pbmetad"][0]) == 2
+    s = O.OracleSystem(w.cvs, w.biases, masses=w.masses, periodic=True, mode="f64", num_particles=len(w.positions))
+    s.load_blob(w.blob)
+    st = [b for b in s.bias_state if b["type"] == O.BIAS_PBMETAD][0]
+    grids = np.concatenate([np.frombuffer(g, "<f8") for _, g in parsed["pbmetad"][0]])
+    assert np.array_equal(st["grid"], grids)
+    assert st["deposited"] == [nd for nd, _ in parsed["pbmetad"][0]]
