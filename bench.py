@@ -67,17 +67,19 @@ class Clocks:
     """SM clocks and throttle reasons sampled during timing by a separate sampler
     process (NVML every millisecond, independent of this process's GIL; the GPU is
     matched to the CUDA device by PCI bus id). Only samples taken between the
-    start and the end of the timed region are summarised; the raw samples are
-    kept in gpurun_out/clocks_<pid>.txt (time, SM MHz, max SM MHz, reason bits)."""
+    start and the end of the timed region are summarised; the raw samples (time,
+    SM MHz, max SM MHz, reason bits) go to a file in the system temporary
+    directory, or to $GLUED_BENCH_CLOCKS_DIR when that is set."""
 
     REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
     def __init__(self, index=0):
+        import tempfile
         self.index = index
         self.proc = None
         self.t0 = self.t1 = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.txt") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks_{os.getpid()}.txt"
+        d = os.environ.get("GLUED_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, f"glued_bench_clocks_{os.getpid()}.txt")
 
     def __enter__(self):
         import torch
@@ -172,6 +174,12 @@ def run_single(args, torch, cfg):
              "c3": W.config3}[cfg]()
     ctx, f = build_single(w, torch, "cuda")
     nc = ctx.glued_context_for(f)
+    # correctness of this exact workload against the FP64 oracle (untimed)
+    e_chk, F_chk = ctx.computeForces()
+    P = _checker()
+    perr = P.check_single(w, e_chk, F_chk, np.array(f.getLastCVValues(ctx)))
+    perr.pop("ref")
+    parity = P.summary([perr], "one force evaluation of the timed workload, before the timed steps")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def step(i):
@@ -215,7 +223,8 @@ def run_single(args, torch, cfg):
     e2e_us = e0.elapsed_time(e1) * 1e3 / args.steps
     info = dict(workload=w.name, us_per_step=us, phases_ms=dict(zip(names, phases)), dominant=names[dom],
                 dom_ms=phases[dom], kernels_per_step=kernels_per_step, e2e_us=e2e_us,
-                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 8 + 8), clocks=clk.summary(), w=w)
+                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 8 + 8), clocks=clk.summary(), w=w,
+                parity=parity)
     return info
 
 
@@ -292,6 +301,16 @@ def run_c5(args, torch):
     diff = float((gp - p.grad).abs().max() / p.grad.abs().max().clamp_min(1e-30))
     if not diff < 1e-6:
         raise RuntimeError(f"C5 graph and autograd forces differ: {diff:.3e}")
+    # energy and forces of this exact workload against the FP64 oracle (untimed)
+    P = _checker()
+    E_ref, F_ref, cv_ref = P.c5_reference(w.positions, raw["pairs"], raw["r0"], raw["patoms"], raw["frames"],
+                                          raw["lam"], raw["centers"], raw["heights"], raw["sigma"])
+    F_gpu = -gp.double().cpu().numpy()
+    import oracle as _O
+    parity = {"max_rel_force_err": _O.max_rel_force_err(F_gpu, F_ref),
+              "energy_rel_err": P.rel_energy_err(float(out[0].item()), E_ref),
+              "oracle": "FP64 (oracle/glued_oracle.cpp, double)",
+              "checked": "one graph replay (forward + backward) of the timed workload, before the timed steps"}
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def step(i):
@@ -323,7 +342,7 @@ def run_c5(args, torch):
     torch.cuda.synchronize()
     e2e_us = e0.elapsed_time(e1) * 1e3 / args.steps
     return dict(us_per_step=us, e2e_us=e2e_us, clocks=clk.summary(), raw=raw, w=w,
-                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 4 + 8))
+                h2d=int(host_pos.numel() * 4), d2h=int(host_f.numel() * 4 + 8), parity=parity)
 
 
 def c5_raw_from_oracle():
@@ -403,14 +422,42 @@ def cpu_baseline_single(cfg, w, budget_s=12.0):
 def c4_inputs(n_walkers=64, n_hills=50000):
     from gluedmd_b200 import workloads as W
     ws, hill = W.config4_walkers(n_walkers=n_walkers, n_hills=n_hills)
-    for w in ws:
-        w["cn0"] = W.coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"])
+    W.config4_restraints(ws)
     return ws, hill
 
 
 def c4_biases(w, hill):
-    from gluedmd_b200.batch import c4_biases as cb
-    return cb(w, hill["params"], hill["iparams"], cn0=w["cn0"])
+    from gluedmd_b200.batch import c4_walker_biases
+    return c4_walker_biases(w, hill)
+
+
+# Workload descriptions shared by both arms (the reference arm prints the same
+# string; its bias form differs where the reference has no hill-sum kernel).
+C4_WORKLOAD = ("C4: 64 walkers 1k-50k atoms (log-uniform), dist/angle/dihedral + 256x1024 coordination, "
+               "harmonic restraints, shared 50,000-hill WT MetaD")
+C4_FORM_OURS = "hill sum over the 50,000 shared hills"
+C4_FORM_REF = "256x256 grid holding the 50,000 hills (the reference has no hill-sum kernel)"
+C5_WORKLOAD = ("C5: 30,000 atoms, contact map 10,000 pairs + path CV 50 frames x 500 atoms, 2-D hill sum "
+               "(2,000 hills); forward + backward (forces and the gradients w.r.t. r0, frames and hill heights)")
+
+
+def _checker():
+    """The FP64 oracle as the correctness checker (outside every timed region)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import parity
+    return parity
+
+
+def parity_c4(b, pool, ws, hill):
+    """One batched step in the tuning the timed run uses, every walker's forces,
+    CV values and energy against the FP64 oracle (max over walkers)."""
+    P = _checker()
+    pool.force.zero_()
+    b.execute()
+    E, cv = b.energies(), b.cv_values()
+    errs = [P.check_walker(w, c4_biases(w, hill), hill["centers"], hill["heights"], E[i],
+                           pool.walkers[i].forces(), cv[i]) for i, w in enumerate(ws)]
+    return P.summary(errs, f"all {len(ws)} walkers, one step in the timed tiling, before the timed steps")
 
 
 def run_c4(args, torch, ws, hill):
@@ -421,6 +468,7 @@ def run_c4(args, torch, ws, hill):
     b = Batch(forces, walkers)
     b.set_hills(hill["centers"], hill["heights"])
     tune = b.autotune()
+    parity = parity_c4(b, pool, ws, hill)
     for wk in walkers:
         wk.force.zero_()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -506,7 +554,7 @@ def run_c4(args, torch, ws, hill):
                 plain_value=W_ * 1e3 / plain_ms, plain_launches=plain_launches, e2e_value=W_ * 1e3 / e2e_ms,
                 h2d=int(h2d), d2h=int(d2h), launches_per_step=launches / float(args.steps + args.warmup),
                 flops=flops, clocks=clk.summary(), tune=tune, status=status, hills=b.num_hills(),
-                graphed=True, runs_us=runs_us, finalize_us=fin_us)
+                graphed=True, runs_us=runs_us, finalize_us=fin_us, parity=parity)
 
 
 def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
@@ -588,8 +636,7 @@ def main():
             line = {"impl": "reference", "metric": "walker-steps/s (CV+bias+force, 64 walkers)", "value": cb["value"],
                     "unit": "walker-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                     "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-                    "config": {"workload": "C4: 64 walkers 1k-50k atoms, dist/angle/dihedral + 256x1024 coordination, "
-                                           "harmonic restraints, shared 50,000-hill WT MetaD"},
+                    "config": {"workload": C4_WORKLOAD, "bias_form": C4_FORM_REF},
                     "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "walker-steps/s",
                                                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         elif args.config == "c5":
@@ -597,7 +644,7 @@ def main():
             cb = cpu_baseline_c5(w, raw, budget_s=max(5.0, 0.5 * args.steps))
             line = {"impl": "reference", "metric": "CV+bias+force us/step", "value": cb["value"], "unit": "us/step",
                     "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-                    "dtype": "f64", "data": "synthetic", "config": {"workload": "C5"},
+                    "dtype": "f64", "data": "synthetic", "config": {"workload": C5_WORKLOAD},
                     "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "us/step", "h2d_bytes_per_step": 0,
                                                 "d2h_bytes_per_step": 0}}
         else:
@@ -659,22 +706,23 @@ def main():
                     "algorithmic": f"64 x 262144 pairs x {FLOP_PAIR:.0f} flop + 64 x {info['hills']} hills x {FLOP_HILL:.0f} flop",
                     "whole_step_frac": info["flops"] / (info["step_ms"] * 1e-3) / 1e12 / fp32.value,
                     "finalize_us": info["finalize_us"]}
-            cb = None
+            cb = cb1 = None
             if not args.no_cpu_baseline and world == 1:
                 cb = cpu_reference_c4(ws, hill, steps_budget_s=15.0)
+                cb1 = cpu_reference_c4(ws, hill, steps_budget_s=8.0, threads=1)
             value = world * info["walkers"] * 1e3 / step_ms
             line = {
                 "metric": "walker-steps/s (CV+bias+force, 64 walkers)", "value": value, "unit": "walker-steps/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "C4: 64 walkers 1k-50k atoms (log-uniform), dist/angle/dihedral + 256x1024 "
-                                       "coordination, harmonic restraints, shared 50,000-hill WT MetaD",
+                "config": {"workload": C4_WORKLOAD, "bias_form": C4_FORM_OURS,
                            "walkers_per_gpu": info["walkers"], "l2": "flushed between steps (256 MB write)",
                            "parallelism": f"walkers x{world} GPUs (no data-path collective)", "tuning": info["tune"]},
                 "e2e": {"value": world * info["e2e_value"], "unit": "walker-steps/s", "h2d_bytes_per_step": info["h2d"],
                         "d2h_bytes_per_step": info["d2h"]},
                 "gpu_launches": int(round(info["launches_per_step"] * args.steps)),
-                "roofline": roof, "cpu_baseline": cb, "clocks": info["clocks"],
+                "roofline": roof, "cpu_baseline": cb, "cpu_baseline_1thread": cb1, "clocks": info["clocks"],
+                "parity": info["parity"],
                 "plain_per_walker_gpu": {"value": world * info["plain_value"], "unit": "walker-steps/s",
                                          "launches_per_step": info["plain_launches"],
                                          "speedup_batched_vs_plain": info["plain_ms"] / info["step_ms"]},
@@ -698,14 +746,13 @@ def main():
                 "metric": "CV+bias+force us/step", "value": us, "unit": "us/step", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": us / 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "C5: 30,000 atoms, contact map 10,000 pairs + path CV 50 frames x 500 atoms, "
-                                       "2-D hill sum (2,000 hills); forward + backward (forces and the gradients "
-                                       "w.r.t. r0, frames and hill heights) through the C ABI, one CUDA graph",
+                "config": {"workload": C5_WORKLOAD, "form": "through the C ABI, one CUDA graph",
                            "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
                 "e2e": {"value": info["e2e_us"], "unit": "us/step", "h2d_bytes_per_step": info["h2d"],
                         "d2h_bytes_per_step": info["d2h"]},
                 "gpu_launches": C5_KERNELS_PER_STEP * args.steps,
                 "roofline": None, "cpu_baseline": cb, "clocks": info["clocks"], "peaks_source": src,
+                "parity": info["parity"],
             }
             print(json.dumps(line))
         if dist is not None:
@@ -748,7 +795,7 @@ def main():
                 "d2h_bytes_per_step": info["d2h"]},
         "gpu_launches": int(round(info["kernels_per_step"] * args.steps)),
         "roofline": roof, "cpu_baseline": cb, "clocks": info["clocks"],
-        "phases_ms": info["phases_ms"], "peaks_source": src,
+        "phases_ms": info["phases_ms"], "peaks_source": src, "parity": info["parity"],
     }
     print(json.dumps(line))
     if dist is not None:

@@ -195,12 +195,20 @@ def force_for(cvs, biases, pbc=True):
     return f
 
 
-def c4_biases(walker, hill_params, hill_iparams, restraint_k=100.0, cn0=None):
+def c4_biases(walker, hill_params, hill_iparams, restraint_k=100.0, cn0=None, d0=None):
     """Per-walker biases of the 64-walker workload: harmonic restraints on the
-    distance (CV 0) and coordination (CV 3) at their initial values, and the shared
-    hill-sum MetaD on (dihedral, angle) = CVs (2, 1)."""
-    b = [(1, [0], [restraint_k, walker["d0"]], [0])]
+    distance (CV 0, centre d0, default the walker's initial distance) and the
+    coordination (CV 3, centre cn0; none when cn0 is None), and the shared hill-sum
+    MetaD on (dihedral, angle) = CVs (2, 1)."""
+    b = [(1, [0], [restraint_k, walker["d0"] if d0 is None else d0], [0])]
     if cn0 is not None:
         b.append((1, [3], [restraint_k, cn0], [0]))
     b.append((103, [2, 1], hill_params, hill_iparams))
     return b
+
+
+def c4_walker_biases(walker, hill):
+    """c4_biases with the restraint centres workloads.config4_restraints stored
+    in the walker (the benchmark's definition of the 64-walker workload)."""
+    k, d, cn = walker["restraint"]
+    return c4_biases(walker, hill["params"], hill["iparams"], restraint_k=k, cn0=cn, d0=d)

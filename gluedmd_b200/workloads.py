@@ -215,7 +215,7 @@ def config1(form="grid", n_hills=2000, bins=256):
         params = [h0] + sigma + [gamma, KT300] + lo + hi
         ip = [500, bins, bins, 1, 1]
         biases = [(BIAS_METAD, [0, 1], params, ip)]
-        g = grid_from_hills(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
+        g = grid_from_hills_windowed(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
         b = blob(metad=[(n_hills, g)])
     elif form == "pbmetad":
         # PBMETAD on the two dihedrals (two periodic 1-D sub-grids holding the
@@ -227,7 +227,7 @@ def config1(form="grid", n_hills=2000, bins=256):
         biases = [(BIAS_PBMETAD, [0, 1], params, [500, bins, 1, bins, 1])]
         subs = [(n_hills, grid_from_hills(centers[:, d:d + 1], 0.5 * heights, sigma[d:d + 1], lo[d:d + 1],
                                           hi[d:d + 1], [bins], [1])) for d in range(2)]
-        g = grid_from_hills(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
+        g = grid_from_hills_windowed(centers, heights, sigma, lo, hi, [bins, bins], [1, 1])
         biases.append((BIAS_EXTERNAL, [0, 1], lo + hi + list(g), [bins, bins, 1, 1]))
         b = blob(pbmetad=[subs], n_external=1)
     else:
@@ -280,7 +280,7 @@ def config2(n_hills=20000, bins=256, with_bias=True):
     hr = np.random.default_rng(5)
     centers = np.stack([hr.uniform(lo[0], hi[0], n_hills), hr.uniform(lo[1], hi[1], n_hills)], 1)
     heights = wt_hill_heights(centers, sigma, [0.0, 0.0], 1.2, 10.0, KT300)
-    g = grid_from_hills(centers, heights, sigma, lo, hi, [bins, bins], [0, 0])
+    g = grid_from_hills_windowed(centers, heights, sigma, lo, hi, [bins, bins], [0, 0])
     params = [1.2] + sigma + [10.0, KT300] + lo + hi
     biases = [(BIAS_METAD, [0, 1], params, [500, bins, bins, 0, 0])]
     extra.update(cn0=cn0, rmsd0=rmsd0)
@@ -298,6 +298,18 @@ def _opes_pair_sum(centers, sigmas, logw, cutoff2, chunk=1024):
         n2 = (d * d).sum(-1)
         tot += np.where(n2 < cutoff2, h[None, :] * (np.exp(-0.5 * n2) - eps), 0.0).sum()
     return tot
+
+
+def _c3_cv_estimate(pos, sel, L):
+    """(COM distance of the two halves of sel, gyration of sel) with unit masses,
+    minimum-image displacements: the C3 CV values, used only to order the kernels."""
+    half = len(sel) // 2
+    d = pos[sel[half:]].mean(0) - pos[sel[:half]].mean(0)
+    d -= np.round(d / L) * L
+    c = pos[sel].mean(0)
+    r = pos[sel] - c
+    r -= np.round(r / L) * L
+    return np.array([np.linalg.norm(d), math.sqrt((r * r).sum(1).mean())])
 
 
 def config3(n_kernels=10000):
@@ -331,6 +343,12 @@ def config3(n_kernels=10000):
         np.fill_diagonal(n2[:, s:s + 1024], np.inf)
         keep[s:s + 1024] &= ~(n2 < 1.0).any(1)
     centers, sig = centers[keep], sig[keep]
+    # deposition order of a run converging on the current state: the kernels
+    # nearest the initial CV values (in sigma units) come last and so carry the
+    # largest log-weights, which makes the bias and its forces non-trivial there
+    s0 = _c3_cv_estimate(pos, sel, L)
+    order = np.argsort(-np.sqrt((((centers - s0) / sig) ** 2).sum(1)), kind="stable")
+    centers, sig = centers[order], sig[order]
     nk = len(centers)
     trace = np.cumsum(kr.normal(0.0, 0.3, nk)) - 2.0 * gamma * kT * np.linspace(1, 0, nk)
     logw = trace / kT
@@ -351,7 +369,8 @@ def config4_walkers(n_walkers=64, n_hills=50000, coord=(256, 1024)):
     angle and dihedral on seeded atoms and a 256 x 1,024 coordination (groups may
     overlap in walkers smaller than 1,280 atoms; identical-atom pairs are skipped
     by the r^2 < 1e-20 rule). Distance and coordination carry harmonic restraints
-    (k = 100) at their initial value. All walkers share one WT hill-sum MetaD on
+    (k = 100) whose centres config4_restraints places just off the initial values.
+    All walkers share one WT hill-sum MetaD on
     (dihedral, angle): 50,000 hills, centres U over [-pi, pi) x [0, pi] (seed 9),
     sigma 0.35 rad, h0 1.2, gamma 10, kT(300 K), heights by the WT recursion."""
     sizes = np.exp(np.random.default_rng(8).uniform(math.log(1000), math.log(50000), n_walkers)).astype(int)
@@ -378,6 +397,23 @@ def config4_walkers(n_walkers=64, n_hills=50000, coord=(256, 1024)):
     hill_params = [1.2] + sigma + [10.0, KT300, -math.pi, 0.0, math.pi, math.pi]
     hill_iparams = [500, n_hills + 100000, 1, 0]
     return walkers, dict(centers=centers, heights=heights, params=hill_params, iparams=hill_iparams)
+
+
+def config4_restraints(walkers, restraint_k=100.0):
+    """Harmonic restraint centres of the 64-walker workload, stored in each walker
+    dict as ``restraint = (k, distance centre, coordination centre)``.
+
+    The centres sit away from the walkers' initial CV values: distance d0 + 0.05 nm,
+    coordination 1.01 CN0 + 2 with CN0 the FP64 coordination number of the initial
+    positions. With a centre equal to the current value, dU/dCV = k (s - s0) is a
+    difference of nearly equal numbers and the restraint forces are rounding noise
+    of the CV; offset, they are forces of order k * 0.05 and k * (0.01 CN0 + 2) that a
+    comparison with the FP64 oracle can resolve."""
+    for w in walkers:
+        if "cn_fp64" not in w:
+            w["cn_fp64"] = coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"])
+        w["restraint"] = (float(restraint_k), w["d0"] + 0.05, 1.01 * w["cn_fp64"] + 2.0)
+    return walkers
 
 
 def config5(n_pairs=10000, n_frames=50, n_path_atoms=500, n_hills=2000):
