@@ -16,7 +16,7 @@ c_int, c_double, c_float, c_char_p, c_void_p, c_size_t, c_ll = (
 P = ctypes.POINTER
 
 GLUED_E = {-1: "invalid argument", -2: "CUDA error", -3: "invalid state", -4: "corrupt bias state",
-           -5: "unsupported", -6: "timeout"}
+           -5: "unsupported"}
 
 
 class GluedError(RuntimeError):

@@ -307,12 +307,16 @@ __global__ void __launch_bounds__(512) k_biases(const BiasDev* __restrict__ gbia
             } else if (b.type == BIAS_OPES) {
                 // CommonGluedKernels.cpp:2642-2723.
                 if (tid == 0 && b.adaptiveStride > 0) {
-                    // every-execute Welford update (CommonGluedKernels.cpp:3009-3027, :4976-4981)
+                    // every-execute Welford update (CommonGluedKernels.cpp:3009-3027, :4976-4981).
+                    // Each operation rounded on its own (no FMA contraction): the
+                    // statistics set the adaptive bandwidth, which enters the
+                    // merge decisions that must match the oracle bit for bit.
                     int n = ++b.nSamples[0];
                     for (int d = 0; d < D; d++) {
-                        double x = cvv[b.cvIdx[d]], dl = x - b.runMean[d];
-                        b.runMean[d] += dl / n;
-                        b.runM2[d] += dl * (x - b.runMean[d]);
+                        double x = cvv[b.cvIdx[d]], dl = __dsub_rn(x, b.runMean[d]);
+                        double mean = __dadd_rn(b.runMean[d], __ddiv_rn(dl, (double)n));
+                        b.runMean[d] = mean;
+                        b.runM2[d] = __dadd_rn(b.runM2[d], __dmul_rn(dl, __dsub_rn(x, mean)));
                     }
                 }
                 const int K = bi < 16 ? sK[bi] : *b.numKernels;

@@ -344,7 +344,7 @@ void Context::buildPlan(const GluedForce& f) {
     gAtoms_.upload(gAtoms); gMass_.upload(gMass); gRef_.upload(gRef); gEv_.upload(gEv);
     cmPairs_.upload(cmPairs); cmParams_.upload(cmParams);
     G_.items = groupItems_.as<GroupItem>(); G_.numItems = (int)groups.size();
-    G_.nInl = std::min((int)groups.size(), 8);
+    G_.nInl = std::min((int)groups.size(), GROUP_INLINE);
     for (int k = 0; k < G_.nInl; k++) G_.inl[k] = groups[k];
     gSlots_.alloc(sizeof(int) * std::max((size_t)1, gAtoms.size()));
     gAtomsN_ = (int)gAtoms.size();
@@ -925,13 +925,14 @@ std::vector<double> Context::opesMetrics(int opesIndex) {
         if (k++ != opesIndex) continue;
         if (bound_) cudaCheck(cudaStreamSynchronize(stream_), "sync");
         double dd[4];
-        int ii[4];
         cudaCheck(cudaMemcpy(dd, hb.dev.sumUprob, sizeof(double) * 4, cudaMemcpyDeviceToHost), "metrics");
-        cudaCheck(cudaMemcpy(ii, hb.dev.numKernels, sizeof(int) * 4, cudaMemcpyDeviceToHost), "metrics");
-        int nker;
+        // each counter through its own pointer: a secondary walker's numKernels
+        // points into the primary's table, its deposit counter stays its own
+        int nker = 0, steps = 0;
         cudaCheck(cudaMemcpy(&nker, hb.dev.numKernels, sizeof(int), cudaMemcpyDeviceToHost), "metrics");
+        cudaCheck(cudaMemcpy(&steps, hb.dev.stepCount, sizeof(int), cudaMemcpyDeviceToHost), "metrics");
         double sumUp = hb.numKernelsCPU > 0 ? dd[0] : 0.0;
-        double counter = (double)ii[2];
+        double counter = (double)steps;
         double KDEnorm = hb.dev.variant == 2 ? counter : dd[1];
         double zed = (nker > 0 && KDEnorm > 0.0) ? sumUp / (KDEnorm * (double)nker) : 1.0;
         double rct = (counter > 0.0 && dd[1] > 0.0) ? hb.dev.kT * std::log(dd[1] / counter) : 0.0;

@@ -43,7 +43,7 @@ __device__ __forceinline__ void imageT(float& dx, float& dy, float& dz, const Bo
 
 struct SwitchConst {
     float ir0, ir0sq, c;           // 1/r0, 1/r0^2, -n/r0^2
-    float n, m, preRes, preDf, preSec;
+    float n, m;
     float r2hi;                    // pairs need r2 < r2hi: min(cutoff^2, (1000 r0)^2)
     int ni, mi;
 };
@@ -72,24 +72,30 @@ __device__ __forceinline__ void pairSwitch(float r2, bool valid, const SwitchCon
         f = valid ? ff : 0.0f;
         g = valid ? dfdx * s.ir0 / r : 0.0f;
     } else {
-        float r = sqrtf(r2);
-        float x = r * s.ir0;
-        float ff, dfdr;
-        float dx1 = x - 1.0f;
-        if (fabsf(dx1) < 1e-4f) {
-            ff = s.preRes + dx1 * (s.preDf + 0.5f * dx1 * s.preSec);
-            dfdr = (s.preDf + dx1 * s.preSec) * s.ir0;
-        } else if (x < 1e-10f) {
-            ff = 1.0f; dfdr = 0.0f;
+        // Non-integer exponents: the reference formula with its Taylor branch
+        // within 1e-4 of x = 1 (CommonGluedKernels.cpp:983-1003), in FP64: in FP32
+        // the quotient (1 - x^n)/(1 - x^m) loses up to ~1e-2 relative accuracy
+        // through cancellation just outside the Taylor window.
+        const double r = sqrt((double)r2);
+        const double x = r * (double)s.ir0;
+        const double n = s.n, m = s.m;
+        double ff, dfdx;
+        const double dx1 = x - 1.0;
+        if (fabs(dx1) < 1e-4) {
+            const double pre = n / m, df = 0.5 * n * (n - m) / m;
+            const double sec = n * (m * m - 3.0 * m * (n - 1.0) + n * (2.0 * n - 3.0)) / (6.0 * m);
+            ff = pre + dx1 * (df + 0.5 * dx1 * sec);
+            dfdx = df + dx1 * sec;
+        } else if (x < 1e-10) {
+            ff = 1.0; dfdx = 0.0;
         } else {
-            float xn = powf(x, s.n), xm = powf(x, s.m);
-            float den = 1.0f - xm;
-            ff = (1.0f - xn) / den;
-            float dfx = (s.m * (xm / x) - s.n * (xn / x) + (s.n - s.m) * (xn * xm / x)) / (den * den);
-            dfdr = dfx * s.ir0;
+            const double xn = pow(x, n), xm = pow(x, m);
+            const double den = 1.0 - xm;
+            ff = (1.0 - xn) / den;
+            dfdx = (m * (xm / x) - n * (xn / x) + (n - m) * (xn * xm / x)) / (den * den);
         }
-        f = valid ? ff : 0.0f;
-        g = valid ? dfdr / r : 0.0f;
+        f = valid ? (float)ff : 0.0f;
+        g = valid ? (float)(dfdx * (double)s.ir0 / r) : 0.0f;
     }
 }
 
@@ -108,9 +114,6 @@ __device__ __forceinline__ void coordTile(const float4* __restrict__ posq, const
         float hi = xmax * xmax * 1.0000002f;
         s.r2hi = it.rc2 > 0.0f ? fminf(it.rc2, hi) : hi;
     }
-    s.preRes = s.n / s.m;
-    s.preDf = 0.5f * s.n * (s.n - s.m) / s.m;
-    s.preSec = s.n * (s.m * s.m - 3.0f * s.m * (s.n - 1.0f) + s.n * (2.0f * s.n - 3.0f)) / (6.0f * s.m);
 
     float ax[RA], ay[RA], az[RA], gax[RA], gay[RA], gaz[RA];
     bool aval[RA];

@@ -391,10 +391,12 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
             jacobi4(F, V, w);
             int im = 0;
             for (int i = 1; i < 4; i++) if (w[i] > w[im]) im = i;
+            // q rotates x onto y (correlation x y^T); bc[0..8] is its transpose,
+            // the rotation that takes the reference y onto x
             double q0 = V[0][im], q1 = V[1][im], q2 = V[2][im], q3 = V[3][im];
-            bc[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3; bc[1] = 2 * (q1 * q2 - q0 * q3); bc[2] = 2 * (q1 * q3 + q0 * q2);
-            bc[3] = 2 * (q1 * q2 + q0 * q3); bc[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3; bc[5] = 2 * (q2 * q3 - q0 * q1);
-            bc[6] = 2 * (q1 * q3 - q0 * q2); bc[7] = 2 * (q2 * q3 + q0 * q1); bc[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+            bc[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3; bc[1] = 2 * (q1 * q2 + q0 * q3); bc[2] = 2 * (q1 * q3 - q0 * q2);
+            bc[3] = 2 * (q1 * q2 - q0 * q3); bc[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3; bc[5] = 2 * (q2 * q3 + q0 * q1);
+            bc[6] = 2 * (q1 * q3 + q0 * q2); bc[7] = 2 * (q2 * q3 - q0 * q1); bc[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
             double msd = fmax(0.0, (c[9] - 2 * w[im]) / na);
             double rmsd = sqrt(msd);
             bc[9] = rmsd > 1e-10 ? 1.0 / (na * rmsd) : 0.0;

@@ -54,6 +54,10 @@ struct GroupItem {
     float f0, f1;
 };
 
+// Group items carried in the group kernels' parameter block (read from the
+// constant bank instead of global memory).
+constexpr int GROUP_INLINE = 8;
+
 struct GroupDev {
     const GroupItem* items;
     int numItems;
@@ -66,7 +70,7 @@ struct GroupDev {
     const float4* cmParams;  // r0, n, m, w
     // the first GROUP_INLINE items again, inside the kernel's parameter block:
     // read from the constant bank instead of global memory
-    GroupItem inl[8];
+    GroupItem inl[GROUP_INLINE];
     int nInl;
 };
 

@@ -23,7 +23,7 @@ enum CVType {
     CV_PUCKERING = 16, CV_DIPOLE = 17, CV_VOLUME = 18, CV_CELL = 19, CV_SECONDARY_STRUCTURE = 20,
     CV_PCA = 21, CV_ERMSD = 22, CV_ENERGY = 23,
     // Extensions of this library (no reference counterpart):
-    // coordination with a hard cutoff (params [r0, n, m, rc]) evaluated on a cell grid,
+    // coordination with a hard cutoff (params [r0, n, m, rc]: pairs at r >= rc are left out),
     // and RMSD after optimal superposition (FP64 quaternion eigensolve).
     CV_COORDINATION_CUTOFF = 106, CV_RMSD_KABSCH = 107,
 };

@@ -12,11 +12,13 @@
 //
 // The kernels are the partial-sum coordination tile (coord_tile.cuh: one CTA
 // per 64-atom A tile and B split, float partials) and a fixed-order reduction of
-// its partials; the results agree with the context path (fixed-point step runs,
-// coord_run.cuh) to FP32 rounding.
+// its partials. They are not the context path's kernels (fixed-point step runs,
+// coord_run.cuh), but they evaluate the same switch in the same precision per
+// kind (S_n/S_m for integer exponents in FP32, the reference formula in FP64
+// for non-integer ones), so the two agree to the rounding of FP32 partial sums.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/glued_b200.h"
@@ -34,25 +36,18 @@ constexpr int kTA = 8 * kRA;
 // handle for cudaGetSymbolAddress; kernels receive the device address.
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
-std::mutex g_mu;
-void* g_scratch[256] = {};
-
-// Device address of the scratch array on the current device, looked up once per
-// device (the first call on a device may load the module).
+// Device address of the scratch array in the current device's context, looked
+// up on every call: the lookup allocates nothing and costs little once the
+// module is loaded (the first call on a device may load it), and a cached
+// address would go stale when the context is torn down and recreated
+// (cudaDeviceReset) between calls.
 void* scratchOnCurrentDevice() {
-    int dev = -1;
-    cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= 256) throw Error(GLUED_E_INVALID, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
-        if (e != cudaSuccess || p == nullptr)
-            throw Error(GLUED_E_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
-                                          cudaGetErrorString(e));
-        g_scratch[dev] = p;
-    }
-    return g_scratch[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+    if (e != cudaSuccess || p == nullptr)
+        throw Error(GLUED_E_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                                      cudaGetErrorString(e));
+    return p;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -112,7 +107,11 @@ void coordinationNoAlloc(cudaStream_t stream, const void* posq, const int* group
     if (!posq || !groupA || !groupB || !cnOut || !gradOut)
         throw Error(GLUED_E_INVALID, "coordination (no-alloc): null argument");
     if (nA < 1 || nB < 1) throw Error(GLUED_E_INVALID, "coordination (no-alloc): both groups need at least one atom");
-    if (!(r0 > 0.0)) throw Error(GLUED_E_INVALID, "coordination (no-alloc): r0 must be > 0");
+    if (!(std::isfinite(r0) && r0 > 0.0)) throw Error(GLUED_E_INVALID, "coordination (no-alloc): r0 must be finite and > 0");
+    // n == m is allowed: the switch is then 1 for every pair (the reference
+    // formula's quotient and its Taylor branch at x = 1 both give n/m = 1)
+    if (!(std::isfinite(n) && std::isfinite(m) && n > 0.0 && m > 0.0))
+        throw Error(GLUED_E_INVALID, "coordination (no-alloc): n and m must be finite and > 0");
     if (periodic && !box9) throw Error(GLUED_E_INVALID, "coordination (no-alloc): periodic needs box vectors");
     // Same tiling rule as the context path (Context::buildPlan).
     const long long pairs = (long long)nA * nB;

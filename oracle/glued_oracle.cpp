@@ -390,11 +390,13 @@ void cv_rmsd_kabsch_f64(const double* pos, const int* atoms, const float* ref, i
     int im = 0;
     for (int i = 1; i < 4; i++) if (w[i] > w[im]) im = i;
     double q0 = V[0][im], q1 = V[1][im], q2 = V[2][im], q3 = V[3][im];
-    // Rotation that maps y (reference) onto x: x ~ Rot * y.
+    // With the correlation matrix Rm = sum x y^T, the top eigenvector q is the
+    // rotation that takes x onto y; its transpose takes y (reference) onto x:
+    // x ~ Rot * y with Rot = R(q)^T.
     double Rot[3][3] = {
-        {q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3, 2 * (q1 * q2 - q0 * q3), 2 * (q1 * q3 + q0 * q2)},
-        {2 * (q1 * q2 + q0 * q3), q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3, 2 * (q2 * q3 - q0 * q1)},
-        {2 * (q1 * q3 - q0 * q2), 2 * (q2 * q3 + q0 * q1), q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3}};
+        {q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3, 2 * (q1 * q2 + q0 * q3), 2 * (q1 * q3 - q0 * q2)},
+        {2 * (q1 * q2 - q0 * q3), q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3, 2 * (q2 * q3 + q0 * q1)},
+        {2 * (q1 * q3 + q0 * q2), 2 * (q2 * q3 - q0 * q1), q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3}};
     double msd = std::max(0.0, (G - 2 * w[im]) / na);
     double rmsd = std::sqrt(msd);
     *value = rmsd;

@@ -546,6 +546,33 @@ class OracleSystem:
                 st["heights"] = np.frombuffer(blob, "<f8", count=n, offset=p).copy()
                 p += 8 * n
 
+    def _opes_states(self):
+        return [st for st in self.bias_state if st["type"] == BIAS_OPES]
+
+    def opes_metrics(self, opes_index):
+        """[zed, rct, nker, neff] of the opes_index-th OPES bias
+        (CommonGluedKernels.cpp:5164-5210): zed = sum_uprob / (KDEnorm nker) with
+        KDEnorm the deposit counter for variant 2 (EXPLORE) and sum_weights
+        otherwise; rct = kT ln(sum_weights / counter); neff = (1 + sum_w)^2 /
+        (1 + sum_w2). State layout: dst = [sum_uprob, sum_weights, sum_w, sum_w2],
+        ist = [numKernels, nSamples, counter, numAllocated]."""
+        st = self._opes_states()[opes_index]
+        nker = int(st["ist"][0])
+        sum_up = float(st["dst"][0]) if nker > 0 else 0.0
+        counter = float(st["ist"][2])
+        kde = counter if st["variant"] == 2 else float(st["dst"][1])
+        zed = sum_up / (kde * nker) if (nker > 0 and kde > 0.0) else 1.0
+        rct = st["kT"] * math.log(st["dst"][1] / counter) if (counter > 0.0 and st["dst"][1] > 0.0) else 0.0
+        sw, sw2 = float(st["dst"][2]), float(st["dst"][3])
+        return [zed, rct, float(nker), (1.0 + sw) * (1.0 + sw) / (1.0 + sw2)]
+
+    def kernel_sigmas(self, opes_index):
+        """Kernel bandwidths of the live kernels, narrowed to float
+        (CommonGluedKernels.cpp:5212-5232)."""
+        st = self._opes_states()[opes_index]
+        nk = int(st["ist"][0])
+        return np.asarray(st["sigmas"][:nk * st["D"]], dtype=np.float32)
+
     def welford(self):
         """Per-execute Welford update for fully adaptive OPES (CommonGluedKernels.cpp:4976-4981)."""
         L = lib()

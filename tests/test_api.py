@@ -101,7 +101,11 @@ def test_xml_rejects_bad_input():
     assert f.usesPeriodicBoundaryConditions() and f.getNumCollectiveVariables() == 1
 
 
-REF_GLUED = "/root/reference/python/glued.py"
+# The reference tree's location comes from the oracle's build recipe
+# (GLUED_REFERENCE, else the recipe's default); the test is skipped without it.
+from build_ref import DEFAULT_REF  # noqa: E402
+
+REF_GLUED = os.path.join(DEFAULT_REF, "python", "glued.py")
 
 
 @pytest.mark.skipif(not os.path.exists(REF_GLUED), reason="reference tree not present")

@@ -115,7 +115,10 @@ def test_fixed_point_io(mode):
 
 def test_metad_grid_replay_vs_oracle():
     """Pace-gated WT grid deposits and evaluation over 40 steps (C1-like, 64x64
-    periodic grid): energies, dU/dCV and the grid itself vs the FP64 oracle."""
+    periodic grid), the oracle depositing at its own FP64 CV values: energies agree
+    to 1e-5 relative and the blob carries the 'GPUS' v1 header. The grid array and
+    numDeposited are compared exactly in
+    test_gpu_paths.py::test_metad_grid_and_deposit_count_replay."""
     cvs, biases = metad_system(pace=2)
     rng = np.random.default_rng(7)
     orc = O.OracleSystem(cvs, biases, mode="f64", num_particles=6)
@@ -128,8 +131,7 @@ def test_metad_grid_replay_vs_oracle():
         orc.update_state(step)
         e, F = ctx.computeForces()
         r = orc.execute(pos)
-        # CV values differ in the last float bits, so compare with the oracle fed
-        # the product's CV values for the bias part
+        # the oracle's own FP64 CV values: agreement to the FP32 CV resolution
         assert abs(e - r["energy"]) < 1e-5 * max(1.0, abs(r["energy"]))
     blob = f.getBiasState()
     import struct
@@ -258,6 +260,8 @@ def test_opes_energy_vs_oracle():
         assert abs(e - res[0].sum()) < 1e-6 * max(1.0, abs(e))
     m = f.getOPESMetrics(ctx, 0)
     assert m[2] == orc.bias_state[0]["ist"][0]
+    # zed, rct, nker, neff (CommonGluedKernels.cpp:5164-5210)
+    np.testing.assert_allclose(m, orc.opes_metrics(0), rtol=1e-10, atol=1e-12)
 
 
 def test_bias_state_round_trip():
