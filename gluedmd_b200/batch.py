@@ -145,15 +145,15 @@ class Batch:
         return v.value
 
     def phase_times(self):
-        """One step with each launch bracketed by CUDA events and every CTA
-        time-stamped (microseconds); see glued_batch_phase_times."""
-        out = (c_double * 24)()
+        """One step between CUDA events, every CTA time-stamped (microseconds);
+        see glued_batch_phase_times."""
+        out = (c_double * 26)()
         call("glued_batch_phase_times", self._h, out)
-        keys = ["runs_us", "finalize_us", "stage_med_us", "stage_max_us", "coord_end_min_us",
+        keys = ["step_us", "device_span_us", "stage_med_us", "stage_max_us", "coord_end_min_us",
                 "coord_end_med_us", "coord_end_max_us", "runs_end_med_us", "runs_end_max_us",
-                "fin_cta_med_us", "fin_cta_max_us", "fin_end_max_us", "coord_steps", "grid", "parts",
+                "fin_cta_med_us", "fin_cta_max_us", "fin_start_us", "coord_steps", "grid", "parts",
                 "finalize_grid", "fin_record_us", "fin_cn_us", "fin_energy_us", "fin_coord_scatter_us",
-                "fin_simple_rows_us", "hill_wait_us", "hill_eval_us", "hill_reduce_us"]
+                "fin_simple_rows_us", "hill_wait_us", "hill_eval_us", "hill_reduce_us", "runs_us", "finalize_us"]
         self.phase_times_last = dict(zip(keys, out[:]))
         return dict(self.phase_times_last)
 

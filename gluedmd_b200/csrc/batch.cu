@@ -1008,7 +1008,9 @@ void Batch::execute() {
 
 // Autotuner: the finalize CTAs per walker and its launch mode are timed on the
 // live walkers with CUDA events (forces go to a scratch buffer) and the fastest
-// combination is kept.
+// combination is kept. Every timed step starts with L2 flushed (a 192 MB memset
+// between steps), as in an MD loop where the engine's own kernels run between
+// force evaluations; the flush buffer is freed before returning.
 BatchTuning Batch::autotune() {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
@@ -1018,9 +1020,11 @@ BatchTuning Batch::autotune() {
     std::vector<BWalker> tmp = I.walkersH;
     for (auto& w : tmp) w.force = I.scratchForce.as<unsigned long long>();
     cudaCheck(cudaMemcpy(I.walkersD.p, tmp.data(), sizeof(BWalker) * tmp.size(), cudaMemcpyHostToDevice), "tune");
-    cudaEvent_t a, b;
-    cudaCheck(cudaEventCreate(&a), "event");
-    cudaCheck(cudaEventCreate(&b), "event");
+    DBuf flush;
+    flush.alloc((size_t)192 << 20);
+    constexpr int reps = 8;
+    cudaEvent_t ev[2 * reps];
+    for (auto& e : ev) cudaCheck(cudaEventCreate(&e), "event");
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
     const int base = I.minParts();
@@ -1031,19 +1035,24 @@ BatchTuning Batch::autotune() {
             I.tune = t;
             I.plan();
             for (int r = 0; r < 2; r++) I.launch(I.stream);
-            cudaCheck(cudaEventRecord(a, I.stream), "event");
-            const int reps = 8;
-            for (int r = 0; r < reps; r++) I.launch(I.stream);
-            cudaCheck(cudaEventRecord(b, I.stream), "event");
-            cudaCheck(cudaEventSynchronize(b), "event");
+            for (int r = 0; r < reps; r++) {
+                cudaCheck(cudaMemsetAsync(flush.p, r & 0xff, flush.bytes, I.stream), "flush");
+                cudaCheck(cudaEventRecord(ev[2 * r], I.stream), "event");
+                I.launch(I.stream);
+                cudaCheck(cudaEventRecord(ev[2 * r + 1], I.stream), "event");
+            }
+            cudaCheck(cudaEventSynchronize(ev[2 * reps - 1]), "event");
             float ms = 0;
-            cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
+            for (int r = 0; r < reps; r++) {
+                float x = 0;
+                cudaCheck(cudaEventElapsedTime(&x, ev[2 * r], ev[2 * r + 1]), "event");
+                ms += x;
+            }
             ms /= reps;
             I.launches += (long long)(reps + 2) * I.launchesPerStep();
             if (ms < bestMs) { bestMs = ms; best = t; }
         }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    for (auto& e : ev) cudaEventDestroy(e);
     cudaCheck(cudaMemcpy(I.walkersD.p, I.walkersH.data(), sizeof(BWalker) * I.walkersH.size(), cudaMemcpyHostToDevice), "tune");
     I.tune = best;
     I.plan();
@@ -1072,19 +1081,35 @@ void Batch::phaseTimes(double* out) {
     cudaCheck(cudaMemsetAsync(st.p, 0, st.bytes, I.stream), "stamps");
     I.dev.stamps = st.as<unsigned long long>();
     I.dev.fstamps = st.as<unsigned long long>() + RS * (size_t)I.grid;
-    cudaEvent_t e[3];
+    // events around the whole step only: an event between the two launches
+    // would hold the finalize back until the runs grid has drained (no
+    // programmatic dependent launch), which the step graph does not do
+    cudaEvent_t e[2];
     for (auto& x : e) cudaCheck(cudaEventCreate(&x), "event");
     cudaCheck(cudaEventRecord(e[0], I.stream), "event");
     I.launchRuns(I.stream);
-    cudaCheck(cudaEventRecord(e[1], I.stream), "event");
     I.launchFinalize(I.stream);
-    cudaCheck(cudaEventRecord(e[2], I.stream), "event");
+    cudaCheck(cudaEventRecord(e[1], I.stream), "event");
     I.dev.stamps = nullptr;
     I.dev.fstamps = nullptr;
-    cudaCheck(cudaEventSynchronize(e[2]), "event");
-    float a = 0, b = 0;
+    cudaCheck(cudaEventSynchronize(e[1]), "event");
+    float a = 0;
     cudaCheck(cudaEventElapsedTime(&a, e[0], e[1]), "event");
-    cudaCheck(cudaEventElapsedTime(&b, e[1], e[2]), "event");
+    // a second step with each launch between events: the kernels' own durations
+    // (the finalize then starts after the runs grid has drained)
+    cudaEvent_t k[3];
+    for (auto& x : k) cudaCheck(cudaEventCreate(&x), "event");
+    cudaCheck(cudaEventRecord(k[0], I.stream), "event");
+    I.launchRuns(I.stream);
+    cudaCheck(cudaEventRecord(k[1], I.stream), "event");
+    I.launchFinalize(I.stream);
+    cudaCheck(cudaEventRecord(k[2], I.stream), "event");
+    cudaCheck(cudaEventSynchronize(k[2]), "event");
+    float kr = 0, kf = 0;
+    cudaCheck(cudaEventElapsedTime(&kr, k[0], k[1]), "event");
+    cudaCheck(cudaEventElapsedTime(&kf, k[1], k[2]), "event");
+    for (auto& x : k) cudaEventDestroy(x);
+    I.launches += I.launchesPerStep();
     for (auto& x : e) cudaEventDestroy(x);
     I.launches += I.launchesPerStep();
     I.ready = true;
@@ -1103,10 +1128,13 @@ void Batch::phaseTimes(double* out) {
         for (int g = 0; g < fg; g++)
             for (int k = 0; k < FS; k++) I.lastStamps.push_back(h[RS * (size_t)I.grid + FS * (size_t)g + k]);
     }
-    unsigned long long t0 = ~0ull, f0 = ~0ull;
+    unsigned long long t0 = ~0ull, f0 = ~0ull, f1 = 0;
     for (int g = 0; g < I.grid; g++) t0 = std::min(t0, h[RS * (size_t)g]);
-    for (int g = 0; g < fg; g++) f0 = std::min(f0, h[RS * (size_t)I.grid + FS * (size_t)g]);
-    std::vector<double> stage, coord, end, hw, he, hr, fdur, fend, fph[5];
+    for (int g = 0; g < fg; g++) {
+        f0 = std::min(f0, h[RS * (size_t)I.grid + FS * (size_t)g]);
+        f1 = std::max(f1, h[RS * (size_t)I.grid + FS * (size_t)g + 5]);
+    }
+    std::vector<double> stage, coord, end, hw, he, hr, fdur, fph[5];
     for (int g = 0; g < I.grid; g++) {
         const unsigned long long* r = h.data() + RS * (size_t)g;
         stage.push_back((r[1] - r[0]) * 1e-3);
@@ -1119,17 +1147,17 @@ void Batch::phaseTimes(double* out) {
     for (int g = 0; g < fg; g++) {
         const unsigned long long* r = h.data() + RS * (size_t)I.grid + FS * (size_t)g;
         fdur.push_back((r[5] - r[0]) * 1e-3);
-        fend.push_back((r[5] - f0) * 1e-3);
         for (int k = 0; k < 5; k++) fph[k].push_back((r[k + 1] - r[k]) * 1e-3);
     }
-    out[0] = a * 1e3; out[1] = b * 1e3;
+    out[0] = a * 1e3; out[1] = (double)(f1 - t0) * 1e-3;
     out[2] = pct(stage, 50); out[3] = pct(stage, 100);
     out[4] = pct(coord, 0); out[5] = pct(coord, 50); out[6] = pct(coord, 100);
     out[7] = pct(end, 50); out[8] = pct(end, 100);
-    out[9] = pct(fdur, 50); out[10] = pct(fdur, 100); out[11] = pct(fend, 100);
+    out[9] = pct(fdur, 50); out[10] = pct(fdur, 100); out[11] = (double)(f0 - t0) * 1e-3;
     out[12] = (double)I.steps.size(); out[13] = (double)I.grid; out[14] = (double)I.parts; out[15] = (double)fg;
-    for (int k = 0; k < 5; k++) out[16 + k] = pct(fph[k], 50);
+    for (int q = 0; q < 5; q++) out[16 + q] = pct(fph[q], 50);
     out[21] = pct(hw, 50); out[22] = pct(he, 50); out[23] = pct(hr, 50);
+    out[24] = kr * 1e3; out[25] = kf * 1e3;
 }
 
 long long Batch::phaseStamps(unsigned long long* out, long long cap) {

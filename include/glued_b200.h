@@ -262,9 +262,10 @@ int glued_batch_set_stream(glued_batch* b, void* stream);
 /* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
  * fewest that cover the walker's coordination rows), finalize launch (0: a
  * programmatic dependent launch of the runs kernel, 1: a plain stream-ordered
- * launch), 0}. autotune times the candidates on the live walkers (forces of the
- * trial launches go to a scratch buffer), keeps the fastest and returns it in
- * tune (synchronizing).                                                        */
+ * launch), 0}. autotune times the candidates on the
+ * live walkers, each timed step after an L2 flush (forces of the trial launches
+ * go to a scratch buffer; a 192 MB flush buffer is allocated for the call and
+ * freed), keeps the fastest and returns it in tune (synchronizing).            */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);
@@ -288,18 +289,21 @@ int glued_batch_get_hills(glued_batch* b, double* centers, double* heights, int 
  * destroyed.                                                                   */
 int glued_batch_status(glued_batch* b, int* status);
 int glued_batch_launch_count(glued_batch* b, long long* count);
-/* Profiling: runs one regular step (forces are accumulated as by execute), each
- * launch bracketed by CUDA events and every CTA time-stamped. out[24], times in
- * microseconds: {runs kernel, finalize kernel (events); staging prologue of a
- * runs CTA (median, max); end of a CTA's coordination steps after the first runs
- * CTA started (min, median, max); end of a runs CTA incl. its hill slice
- * (median, max); finalize CTA duration (median, max); last finalize CTA end
- * after the first one started; coordination steps, runs grid, finalize CTAs per
+/* Profiling: runs one regular step (forces are accumulated as by execute), as
+ * the step graph launches it, between two CUDA events, every CTA time-stamped,
+ * then a second step with each launch between CUDA events (forces accumulated
+ * again). out[26], times in microseconds: {the step (events); last finalize CTA end
+ * after the first runs CTA started; staging prologue of a runs CTA (median,
+ * max); end of a CTA's coordination steps after the first runs CTA started
+ * (min, median, max); end of a runs CTA incl. its hill slice (median, max);
+ * finalize CTA duration (median, max); first finalize CTA start after the first
+ * runs CTA started; coordination steps, runs grid, finalize CTAs per
  * walker, finalize grid; median durations of the finalize phases: loads and
  * walker record, CN and distance/angle/dihedral CVs, dU/dCV and energies,
  * coordination scatter, distance/angle/dihedral rows; median durations of the
  * runs CTAs' hill phases: wait for the staged data, hill-table evaluation,
- * lane reduction and store}. No reference counterpart.                        */
+ * lane reduction and store; second step: runs kernel, finalize kernel (events)}.
+ * No reference counterpart.                                                    */
 int glued_batch_phase_times(glued_batch* b, double* out);
 /* Raw records of the last glued_batch_phase_times call: per runs CTA {SM id,
  * coordination steps, %globaltimer at entry, staging issued, coordination done,
