@@ -147,27 +147,28 @@ class Batch:
     def phase_times(self):
         """One step between CUDA events, every CTA time-stamped (microseconds);
         see glued_batch_phase_times."""
-        out = (c_double * 26)()
+        out = (c_double * 28)()
         call("glued_batch_phase_times", self._h, out)
         keys = ["step_us", "device_span_us", "stage_med_us", "stage_max_us", "coord_end_min_us",
                 "coord_end_med_us", "coord_end_max_us", "runs_end_med_us", "runs_end_max_us",
                 "fin_cta_med_us", "fin_cta_max_us", "fin_start_us", "coord_steps", "grid", "parts",
                 "finalize_grid", "fin_record_us", "fin_cn_us", "fin_energy_us", "fin_coord_scatter_us",
-                "fin_simple_rows_us", "hill_wait_us", "hill_eval_us", "hill_reduce_us", "runs_us", "finalize_us"]
+                "fin_simple_rows_us", "hill_wait_us", "hill_eval_us", "hill_reduce_us", "runs_us", "finalize_us",
+                "first_step_ready_us", "first_step_us"]
         self.phase_times_last = dict(zip(keys, out[:]))
         return dict(self.phase_times_last)
 
     def phase_stamps(self):
-        """Raw records of the last phase_times call: (runs [grid, 8] = SM id,
-        coordination steps, six %globaltimer stamps in ns; finalize [CTAs, 6])."""
+        """Raw records of the last phase_times call: (runs [grid, 10] = SM id,
+        coordination steps, eight %globaltimer stamps in ns; finalize [CTAs, 6])."""
         n = c_ll()
         call("glued_batch_phase_stamps", self._h, None, 0, ctypes.byref(n))
         buf = (ctypes.c_ulonglong * max(1, n.value))()
         call("glued_batch_phase_stamps", self._h, buf, n.value, ctypes.byref(n))
         v = np.array(buf[:n.value], dtype=np.uint64)
         grid = int(self.phase_times_last["grid"]) if hasattr(self, "phase_times_last") else 0
-        runs = v[:8 * grid].reshape(grid, 8)
-        return runs, v[8 * grid:].reshape(-1, 6)
+        runs = v[:10 * grid].reshape(grid, 10)
+        return runs, v[10 * grid:].reshape(-1, 6)
 
     @property
     def tuning(self):

@@ -324,7 +324,7 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool 
 // gathers are issued when the first step starts), then evaluates its slice.
 template <int RA, int BOX, int NH, bool HI>
 __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm, HillStage& hs) {
-    unsigned long long* st = B.stamps ? B.stamps + 7 * (size_t)blockIdx.x : nullptr;
+    unsigned long long* st = B.stamps ? B.stamps + 9 * (size_t)blockIdx.x : nullptr;
     if (st && threadIdx.x == 0) {
         unsigned sm;
         asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
@@ -339,16 +339,24 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     if (st && threadIdx.x == 0) st[1] = globalTimer();
     const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
     if (s0 < s1) {
+        // profiling stamps 7 and 8: the first step's data has landed / the first step is done
         if (hills)
             coordRun<RA, BOX, NH, HI>(
                 B.R, s0, s1, sm, NoPieceHook(),
                 [&]() {
+                    if (st && threadIdx.x == 0) st[7] = globalTimer();
                     hillStageData(B, 0, hs);
                     cpAsyncCommit();
                 },
-                [&]() { hillCVs(B, 0, hs); });   // read after the barriers of the hill slice
+                [&]() {
+                    hillCVs(B, 0, hs);   // read after the barriers of the hill slice
+                    if (st && threadIdx.x == 0) st[8] = globalTimer();
+                });
         else
-            coordRun<RA, BOX, NH, HI>(B.R, s0, s1, sm, NoPieceHook());
+            coordRun<RA, BOX, NH, HI>(
+                B.R, s0, s1, sm, NoPieceHook(),
+                [&]() { if (st && threadIdx.x == 0) st[7] = globalTimer(); },
+                [&]() { if (st && threadIdx.x == 0) st[8] = globalTimer(); });
     }
     if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
     // the finalize (a programmatic dependent launch) may be scheduled once every
@@ -1074,7 +1082,7 @@ static double pct(std::vector<double>& v, double p) {
 // the layout of out[24] is given with glued_batch_phase_times.
 void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
-    constexpr int RS = 7, FS = 6;   // stamps per runs / finalize CTA
+    constexpr int RS = 9, FS = 6;   // stamps per runs / finalize CTA
     const int fg = I.W * I.parts;
     DBuf st;
     st.alloc(sizeof(unsigned long long) * (RS * (size_t)I.grid + FS * (size_t)fg));
@@ -1124,6 +1132,8 @@ void Batch::phaseTimes(double* out) {
             I.lastStamps.push_back(r[6]);
             I.lastStamps.push_back((unsigned long long)(begin[g + 1] - begin[g]));
             for (int k = 0; k < 6; k++) I.lastStamps.push_back(r[k]);
+            I.lastStamps.push_back(r[7]);
+            I.lastStamps.push_back(r[8]);
         }
         for (int g = 0; g < fg; g++)
             for (int k = 0; k < FS; k++) I.lastStamps.push_back(h[RS * (size_t)I.grid + FS * (size_t)g + k]);
@@ -1134,9 +1144,13 @@ void Batch::phaseTimes(double* out) {
         f0 = std::min(f0, h[RS * (size_t)I.grid + FS * (size_t)g]);
         f1 = std::max(f1, h[RS * (size_t)I.grid + FS * (size_t)g + 5]);
     }
-    std::vector<double> stage, coord, end, hw, he, hr, fdur, fph[5];
+    std::vector<double> stage, coord, end, hw, he, hr, fdur, fph[5], ready, firstStep;
     for (int g = 0; g < I.grid; g++) {
         const unsigned long long* r = h.data() + RS * (size_t)g;
+        if (r[7] && r[8]) {
+            ready.push_back((r[7] - r[0]) * 1e-3);
+            firstStep.push_back((r[8] - r[7]) * 1e-3);
+        }
         stage.push_back((r[1] - r[0]) * 1e-3);
         coord.push_back((r[2] - t0) * 1e-3);
         hw.push_back((r[3] - r[2]) * 1e-3);
@@ -1158,6 +1172,7 @@ void Batch::phaseTimes(double* out) {
     for (int q = 0; q < 5; q++) out[16 + q] = pct(fph[q], 50);
     out[21] = pct(hw, 50); out[22] = pct(he, 50); out[23] = pct(hr, 50);
     out[24] = kr * 1e3; out[25] = kf * 1e3;
+    out[26] = pct(ready, 50); out[27] = pct(firstStep, 50);
 }
 
 long long Batch::phaseStamps(unsigned long long* out, long long cap) {

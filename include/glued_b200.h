@@ -292,7 +292,7 @@ int glued_batch_launch_count(glued_batch* b, long long* count);
 /* Profiling: runs one regular step (forces are accumulated as by execute), as
  * the step graph launches it, between two CUDA events, every CTA time-stamped,
  * then a second step with each launch between CUDA events (forces accumulated
- * again). out[26], times in microseconds: {the step (events); last finalize CTA end
+ * again). out[28], times in microseconds: {the step (events); last finalize CTA end
  * after the first runs CTA started; staging prologue of a runs CTA (median,
  * max); end of a CTA's coordination steps after the first runs CTA started
  * (min, median, max); end of a runs CTA incl. its hill slice (median, max);
@@ -302,12 +302,14 @@ int glued_batch_launch_count(glued_batch* b, long long* count);
  * walker record, CN and distance/angle/dihedral CVs, dU/dCV and energies,
  * coordination scatter, distance/angle/dihedral rows; median durations of the
  * runs CTAs' hill phases: wait for the staged data, hill-table evaluation,
- * lane reduction and store; second step: runs kernel, finalize kernel (events)}.
- * No reference counterpart.                                                    */
+ * lane reduction and store; second step: runs kernel, finalize kernel (events);
+ * first coordination step's data landed after a runs CTA started, first step's
+ * duration (medians)}. No reference counterpart.                               */
 int glued_batch_phase_times(glued_batch* b, double* out);
 /* Raw records of the last glued_batch_phase_times call: per runs CTA {SM id,
  * coordination steps, %globaltimer at entry, staging issued, coordination done,
- * hill data ready, hill evaluation done, exit}, then per finalize CTA six
+ * hill data ready, hill evaluation done, exit, first step's data landed, first
+ * step done}, then per finalize CTA six
  * %globaltimer stamps. *n = number of values; min(cap, *n) are copied to out
  * (out may be NULL when cap is 0). No reference counterpart.                   */
 int glued_batch_phase_stamps(glued_batch* b, unsigned long long* out, long long cap, long long* n);
