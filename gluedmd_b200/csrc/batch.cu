@@ -337,7 +337,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
         cpAsyncCommit();
     }
     if (st && threadIdx.x == 0) st[1] = globalTimer();
-    const int s0 = B.R.begin[blockIdx.x], s1 = B.R.begin[blockIdx.x + 1];
+    const int s0 = coordRange(B.R.numSteps, gridDim.x, blockIdx.x), s1 = coordRange(B.R.numSteps, gridDim.x, blockIdx.x + 1);
     if (s0 < s1) {
         // profiling stamps 7 and 8: the first step's data has landed / the first step is done
         if (hills)
@@ -625,7 +625,7 @@ struct Batch::Impl {
     std::vector<CoordItem> items;
     std::vector<int> coordAtoms;
     std::vector<CoordStep> steps;
-    DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, beginD, boxesD, sysPosqD, acc, cnPiece;
+    DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, gBD, gAD, stepPosqD, boxesD, sysPosqD, acc, cnPiece;
     DBuf hillCvPosD, hillCvTypeD, rowAtomD;
     std::vector<BSimple> simpleH;
     DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
@@ -656,20 +656,33 @@ struct Batch::Impl {
     // device copies are rewritten in place (a captured graph keeps their
     // addresses) unless they must grow.
     void balance() {
-        std::vector<int> begin = balanceRanges((int)steps.size(), grid, {});
+        std::vector<int> begin = balanceRanges((int)steps.size(), grid);
         const int pieces = buildCoordPieces(steps, begin, items);
         auto put = [&](DBuf& d, const void* src, size_t bytes) {
             if (d.bytes < bytes) { d.alloc(bytes); destroyGraph(); }
             if (bytes) cudaCheck(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice), "ranges");
         };
-        put(beginD, begin.data(), sizeof(int) * begin.size());
         put(stepsD, steps.data(), sizeof(CoordStep) * steps.size());
         put(itemsD, items.data(), sizeof(CoordItem) * items.size());
         if (cnPiece.bytes < sizeof(double) * std::max(1, pieces)) {
             cnPiece.alloc(sizeof(double) * std::max(1, pieces));
             destroyGraph();
         }
-        dev.R.begin = beginD.as<int>();
+        // per-step gather tables (slot = user atom index in a walker's posq)
+        const size_t n = std::max<size_t>(1, steps.size());
+        if (gBD.bytes < sizeof(int) * COORD_CH * n) { gBD.alloc(sizeof(int) * COORD_CH * n); destroyGraph(); }
+        if (gAD.bytes < sizeof(int) * COORD_TA * n) { gAD.alloc(sizeof(int) * COORD_TA * n); destroyGraph(); }
+        std::vector<const float4*> stepPosq(n, nullptr);
+        for (size_t k = 0; k < steps.size(); k++) stepPosq[k] = walkersH[steps[k].sys].posq;
+        put(stepPosqD, stepPosq.data(), sizeof(const float4*) * n);
+        launchStepGathers(0, stepsD.as<CoordStep>(), (int)steps.size(), grid, atomsD.as<int>(), gBD.as<int>(),
+                          gAD.as<int>());
+        cudaCheck(cudaGetLastError(), "gather tables");
+        cudaCheck(cudaDeviceSynchronize(), "gather tables");
+        dev.R.numSteps = (int)steps.size();
+        dev.R.gB = gBD.as<int>();
+        dev.R.gA = gAD.as<int>();
+        dev.R.stepPosq = stepPosqD.as<const float4*>();
         dev.R.steps = stepsD.as<CoordStep>();
         dev.R.items = itemsD.as<CoordItem>();
         dev.items = itemsD.as<CoordItem>();
@@ -1125,7 +1138,7 @@ void Batch::phaseTimes(double* out) {
     cudaCheck(cudaMemcpy(h.data(), st.p, st.bytes, cudaMemcpyDeviceToHost), "stamps");
     // raw records: runs CTA {SM, steps, 6 times}, finalize CTA {6 times}
     {
-        std::vector<int> begin = balanceRanges((int)I.steps.size(), I.grid, {});
+        std::vector<int> begin = balanceRanges((int)I.steps.size(), I.grid);
         I.lastStamps.clear();
         for (int g = 0; g < I.grid; g++) {
             const unsigned long long* r = h.data() + RS * (size_t)g;

@@ -388,21 +388,27 @@ void Context::buildPlan(const GluedForce& f) {
         const int beside = (simpleBeside_ ? simpleCtas : 0) + (groupBeside_ ? G_.numItems : 0);
         if (beside > 0) coordGrid_ = sms - beside;
         coordGrid_ = std::max(1, std::min(coordGrid_, (int)coordStepsH_.size()));
-        std::vector<int> begin = balanceRanges((int)coordStepsH_.size(), coordGrid_, {});
+        std::vector<int> begin = balanceRanges((int)coordStepsH_.size(), coordGrid_);
         const int pieces = buildCoordPieces(coordStepsH_, begin, coord);
         coordItemsH_ = coord;
         coordItems_.upload(coord);
         coordAtoms_.upload(coordAtoms);
         coordSlots_.alloc(sizeof(int) * std::max(1, coordAtomsN_));
         coordSteps_.upload(coordStepsH_);
-        coordBegin_.upload(begin);
+        const size_t nSteps = coordStepsH_.size();
+        coordGB_.alloc(sizeof(int) * COORD_CH * std::max<size_t>(1, nSteps));
+        coordGA_.alloc(sizeof(int) * COORD_TA * std::max<size_t>(1, nSteps));
+        coordStepPosq_.alloc(sizeof(const float4*) * std::max<size_t>(1, nSteps));
         coordSysPosq_.alloc(sizeof(const float4*));
         coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
         coordCnPiece_.alloc(sizeof(double) * std::max(1, pieces));
         cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
         R_.items = coordItems_.as<CoordItem>();
         R_.steps = coordSteps_.as<CoordStep>();
-        R_.begin = coordBegin_.as<int>();
+        R_.numSteps = (int)nSteps;
+        R_.gB = coordGB_.as<int>();
+        R_.gA = coordGA_.as<int>();
+        R_.stepPosq = coordStepPosq_.as<const float4*>();
         R_.slots = coordSlots_.as<int>();
         R_.sysPosq = coordSysPosq_.as<const float4*>();
         R_.sysBox = box_.as<BoxDev>();
@@ -637,8 +643,12 @@ void Context::bind(cudaStream_t s, const void* posq, const int* atomIndex, long 
     padded_ = padded;
     bound_ = true;
     invalidateGraphs();
-    if (coordItemsN_ > 0)
+    if (coordItemsN_ > 0) {
         cudaCheck(cudaMemcpy(coordSysPosq_.p, &posq_, sizeof(posq_), cudaMemcpyHostToDevice), "coordination posq");
+        std::vector<const float4*> stepPosq(std::max<size_t>(1, coordStepsH_.size()), posq_);
+        cudaCheck(cudaMemcpy(coordStepPosq_.p, stepPosq.data(), sizeof(const float4*) * stepPosq.size(),
+                             cudaMemcpyHostToDevice), "coordination step posq");
+    }
     atomsReordered();
 }
 
@@ -646,6 +656,9 @@ void Context::atomsReordered() {
     requireBound();
     launchInvertIndex(stream_, atomIndex_, u2g_.as<int>(), numParticles_);
     launchComposeSlots(stream_, coordAtoms_.as<int>(), u2g_.as<int>(), coordSlots_.as<int>(), coordAtomsN_);
+    if (coordItemsN_ > 0)
+        launchStepGathers(stream_, coordSteps_.as<CoordStep>(), (int)coordStepsH_.size(), coordGrid_,
+                          coordSlots_.as<int>(), coordGB_.as<int>(), coordGA_.as<int>());
     launchComposeSlots(stream_, gAtoms_.as<int>(), u2g_.as<int>(), gSlots_.as<int>(), gAtomsN_);
     launchComposeSimpleSlots(stream_, simple_.as<SimpleItem>(), u2g_.as<int>(), numSimple_);
     cudaCheck(cudaGetLastError(), "invert index");

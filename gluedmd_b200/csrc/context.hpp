@@ -116,7 +116,7 @@ private:
     DBuf jAtom_, jx_, jy_, jz_, jCv_;
     DBuf simple_, groupItems_, gAtoms_, gSlots_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
     int gAtomsN_ = 0, groupCached_ = 1;
-    DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordBegin_, coordAcc_, coordCnPiece_;
+    DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordGB_, coordGA_, coordStepPosq_, coordAcc_, coordCnPiece_;
     DBuf coordSysPosq_;
     DBuf biasDev_, mergeFlag_, uprobPartial_, sumPart_;
     bool kernelSums_ = false;

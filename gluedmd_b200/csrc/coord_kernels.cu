@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
     pdlEnter();
     extern __shared__ __align__(16) unsigned char dsm[];
     CoordRunSmem<RA>& sm = *reinterpret_cast<CoordRunSmem<RA>*>(dsm);
-    const int s0 = R.begin[blockIdx.x], s1 = R.begin[blockIdx.x + 1];
+    const int s0 = coordRange(R.numSteps, gridDim.x, blockIdx.x), s1 = coordRange(R.numSteps, gridDim.x, blockIdx.x + 1);
     if (s0 < s1) coordRun<RA, BOX, NH, HI>(R, s0, s1, sm, NoPieceHook());
 }
 
@@ -92,6 +92,32 @@ __global__ void k_compose_slots(const int* __restrict__ atoms, const int* __rest
 
 void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* slots, int n) {
     if (n > 0) k_compose_slots<<<(n + 255) / 256, 256, 0, s>>>(atoms, u2g, slots, n);
+}
+
+// Per-step gather tables of the coordination runs (CoordRunDev::gB, gA) from the
+// step list and the atoms' posq rows (slots), one thread per (step, lane of the
+// chunk / tile); rebuilt whenever the rows change. A step gathers its tile's A
+// atoms when it starts a tile run: the tile's first chunk, or the first step of
+// a CTA's range in a grid of `grid` CTAs.
+static_assert(COORD_TA == COORD_CH, "one thread per B chunk lane and A tile lane");
+__global__ void k_step_gathers(const CoordStep* __restrict__ steps, int numSteps, int grid,
+                               const int* __restrict__ slots, int* __restrict__ gB, int* __restrict__ gA) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)numSteps * COORD_CH) return;
+    const int s = (int)(i / COORD_CH), t = (int)(i % COORD_CH);
+    const CoordStep d = steps[s];
+    const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
+    gB[i] = t < nBv ? slots[d.bStart + t] : -1;
+    // smallest CTA whose range could start at s
+    const long long b = ((long long)s * grid + numSteps - 1) / numSteps;
+    const bool rangeStart = b < grid && coordRange(numSteps, grid, (int)b) == s;
+    gA[i] = ((fl & COORD_F_FIRST) || rangeStart) ? (t < nAv ? slots[d.aStart + t] : -2) : -1;
+}
+
+void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
+                       int* gA) {
+    const long long n = (long long)numSteps * COORD_CH;
+    if (n > 0) k_step_gathers<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(steps, numSteps, grid, slots, gB, gA);
 }
 
 void runKernelSetup(const void* fn, size_t dynSmem) {

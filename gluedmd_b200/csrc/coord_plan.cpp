@@ -39,28 +39,10 @@ int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep
     return rows;
 }
 
-std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost) {
-    std::vector<int> begin(grid + 1, 0);
-    if (grid < 1) return begin;
-    auto share = [&](double T, int b) {
-        double c = b < (int)preCost.size() ? preCost[b] : 0.0;
-        return std::max(0.0, T - c);
-    };
-    // level T with sum_b max(0, T - cost_b) == numSteps (bisection)
-    double lo = 0.0, hi = (double)numSteps + 1.0;
-    for (double c : preCost) hi = std::max(hi, c + (double)numSteps + 1.0);
-    for (int it = 0; it < 100; it++) {
-        double mid = 0.5 * (lo + hi), tot = 0.0;
-        for (int b = 0; b < grid; b++) tot += share(mid, b);
-        if (tot < numSteps) lo = mid; else hi = mid;
-    }
-    double cum = 0.0;
-    for (int b = 0; b < grid; b++) {
-        cum += share(hi, b);
-        begin[b + 1] = std::min(numSteps, (int)std::llround(cum));
-    }
-    begin[grid] = numSteps;
-    for (int b = 1; b <= grid; b++) begin[b] = std::max(begin[b], begin[b - 1]);
+std::vector<int> balanceRanges(int numSteps, int grid) {
+    // the split the kernels compute themselves (coordRange): equal counts +-1
+    std::vector<int> begin(std::max(grid, 0) + 1, 0);
+    for (int b = 0; b <= grid; b++) begin[b] = grid > 0 ? coordRange(numSteps, grid, b) : 0;
     return begin;
 }
 

@@ -56,12 +56,22 @@ constexpr double IFXD = 1.0 / 4294967296.0;
 constexpr int F_FIRST = COORD_F_FIRST, F_LAST = COORD_F_LAST;
 }  // namespace crun
 
+// Pair constants of one item in scaled units (coordinates divided by r0).
+struct RunConst {
+    float lo, hi;       // valid pairs: lo <= x^2 < hi
+    float n, m;         // general exponents (kind 0)
+    int ni, mi;         // integer exponents (kind -1)
+    float ir0;
+    BoxDev box;         // scaled: a, b, c divided by r0; inv multiplied by r0
+};
+
 template <int RA>
 struct CoordRunSmem {
     float4 pos[2][crun::CH];
     float4 apos[2][crun::NW * RA];
     float g[2][crun::NW][crun::CH * 3];
     CoordStep st[crun::WIN];
+    RunConst kst[crun::WIN];   // constants of the window's steps that start a tile run
     double red[2][crun::NW];
 };
 
@@ -83,15 +93,6 @@ __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_g
 __device__ __forceinline__ void redAddI64(unsigned long long* p, long long v) {
     redAddGlobal(p, (unsigned long long)v);
 }
-
-// Pair constants of one item in scaled units (coordinates divided by r0).
-struct RunConst {
-    float lo, hi;       // valid pairs: lo <= x^2 < hi
-    float n, m;         // general exponents (kind 0)
-    int ni, mi;         // integer exponents (kind -1)
-    float ir0;
-    BoxDev box;         // scaled: a, b, c divided by r0; inv multiplied by r0
-};
 
 __device__ __forceinline__ RunConst runConst(const CoordItem& it, const BoxDev& b) {
     RunConst k;
@@ -332,40 +333,47 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
     RunConst K;
     double cn = 0.0;
     int pieceSteps = 0;
+    static_assert(TA == COORD_TA, "gather tables are laid out for 128-atom A tiles");
     for (int w0 = s0; w0 < s1; w0 += WIN) {
         const int w1 = min(s1, w0 + WIN);
         const int nw = w1 - w0;
         __syncthreads();  // previous window fully consumed
+        // gather indices of step w0 + ls from the per-step tables (no other load
+        // first): B (threads < CH) and A (threads < TA; -1: no A gather)
+        auto loadIdx = [&](int ls, int& ib, int& ia, const float4*& pq) {
+            const size_t s = (size_t)(w0 + ls);
+            ib = tid < CH ? __ldg(R.gB + s * CH + tid) : -1;
+            ia = tid < TA ? __ldg(R.gA + s * TA + tid) : -1;
+            pq = R.stepPosq[s];
+        };
+        auto issue = [&](int ls, int ib, int ia, const float4* pq) {
+            const int b = (w0 + ls - s0) & 1;
+            if (tid < CH) cpAsync16(&sm.pos[b][tid], pq + (ib >= 0 ? ib : 0), ib >= 0);
+            if (tid < TA && ia != -1) cpAsync16(&sm.apos[b][tid], pq + (ia >= 0 ? ia : 0), ia >= 0);
+            cpAsyncCommit();
+        };
+        // the window's first two steps: gathers first, then the step records
+        // (both independent), then the constants of the steps that start a tile
+        // run, while the gathers land
+        {
+            int ib0, ia0, ib1 = -1, ia1 = -1;
+            const float4 *pq0, *pq1 = nullptr;
+            loadIdx(0, ib0, ia0, pq0);
+            if (nw > 1) loadIdx(1, ib1, ia1, pq1);
+            issue(0, ib0, ia0, pq0);
+            if (nw > 1) issue(1, ib1, ia1, pq1);
+        }
         {
             const int4* src = reinterpret_cast<const int4*>(R.steps + w0);
             int4* dst = reinterpret_cast<int4*>(sm.st);
             for (int i = tid; i < nw * 2; i += blockDim.x) dst[i] = __ldg(src + i);
         }
         __syncthreads();
-        // gather indices of a step: B (threads < CH) and A (threads < TA, first steps only)
-        auto loadIdx = [&](int ls, int& ib, int& ia, const float4*& pq) {
-            const CoordStep& d = sm.st[ls];
-            const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
-            const bool first = (w0 + ls == s0) || (fl & F_FIRST);
-            ib = (tid < CH && tid < nBv) ? __ldg(R.slots + d.bStart + tid) : -1;
-            ia = (first && tid < TA && tid < nAv) ? __ldg(R.slots + d.aStart + tid) : -1;
-            pq = R.sysPosq[d.sys];
-        };
-        auto issue = [&](int ls, int ib, int ia, const float4* pq) {
-            const CoordStep& d = sm.st[ls];
-            const int b = (w0 + ls - s0) & 1;
-            const int fl = d.packed >> 16;
-            const bool first = (w0 + ls == s0) || (fl & F_FIRST);
-            if (tid < CH) cpAsync16(&sm.pos[b][tid], pq + (ib >= 0 ? ib : 0), ib >= 0);
-            if (first && tid < TA) cpAsync16(&sm.apos[b][tid], pq + (ia >= 0 ? ia : 0), ia >= 0);
-            cpAsyncCommit();
-        };
-        int ib0, ia0, ib1 = -1, ia1 = -1;
-        const float4 *pq0, *pq1 = nullptr;
-        loadIdx(0, ib0, ia0, pq0);
-        if (nw > 1) loadIdx(1, ib1, ia1, pq1);
-        issue(0, ib0, ia0, pq0);
-        if (nw > 1) issue(1, ib1, ia1, pq1);
+        for (int i = tid; i < nw; i += blockDim.x) {
+            const CoordStep& d = sm.st[i];
+            if (w0 + i == s0 || i == 0 || ((d.packed >> 16) & F_FIRST))
+                sm.kst[i] = runConst(R.items[d.item], R.sysBox[d.sys]);
+        }
         cpAsyncWaitAll();
         __syncthreads();
         if (w0 == s0) start();
@@ -380,8 +388,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             const float4* pq2 = nullptr;
             if (ls + 2 < nw) loadIdx(ls + 2, ib2, ia2, pq2);
             if (first) {
-                const CoordItem it = R.items[d.item];
-                K = runConst(it, R.sysBox[d.sys]);
+                K = sm.kst[ls];
 #pragma unroll
                 for (int i = 0; i < RH; i++) {
                     const float4 p = sm.apos[b][ty + NW * (2 * i)], q = sm.apos[b][ty + NW * (2 * i + 1)];

@@ -107,6 +107,7 @@ struct CoordDev {
 // Coordination as static per-CTA runs of (A tile, B chunk) steps (coord_run.cuh).
 constexpr int COORD_NW = 16;    // warps per CTA
 constexpr int COORD_CH = 128;   // B atoms per chunk
+constexpr int COORD_TA = 128;   // A atoms per tile (16 warps x 8)
 constexpr int COORD_F_FIRST = 1, COORD_F_LAST = 2;
 
 // One (tile, chunk) step. 32 bytes.
@@ -124,13 +125,27 @@ struct __align__(16) CoordStep {
 struct CoordRunDev {
     const CoordItem* items;
     const CoordStep* steps;
-    const int* begin;          // [grid + 1]: CTA b runs steps [begin[b], begin[b+1])
+    int numSteps;              // CTA b of a grid of G runs steps [b N / G, (b + 1) N / G) (coordRange)
     const int* slots;          // per coordination atom: its row in posq
+    // per-step gather tables, so that a step's gathers need no other load first:
+    // gB[s][CH] = posq rows of the chunk's B atoms (-1 past the chunk: zero-fill);
+    // gA[s][TA] = posq rows of the tile's A atoms when step s starts a tile run
+    // (a tile's first chunk, or the first step of a CTA's range), -2 past the
+    // tile (zero-fill), all -1 otherwise (no A gather)
+    const int* gB;
+    const int* gA;
+    const float4* const* stepPosq;  // positions of the system of step s
     const float4* const* sysPosq;  // positions of system CoordStep::sys
     const BoxDev* sysBox;      // box of system CoordStep::sys
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
     double* cnPiece;           // CN partial of every run piece, item-contiguous (CoordItem::pieceBegin/End)
 };
+
+// Equal static ranges of the coordination steps: CTA b of a grid of G runs
+// steps [coordRange(N, G, b), coordRange(N, G, b + 1)).
+__host__ __device__ inline int coordRange(int numSteps, int grid, int b) {
+    return (int)(((long long)b * numSteps) / grid);
+}
 
 // Bias records, evaluated in the reference's bias-type order.
 struct BiasDev {

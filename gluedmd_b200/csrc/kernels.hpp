@@ -27,16 +27,19 @@ void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, l
 void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, int totalRows, int boxKind, int kind,
                  bool hi, const JacDev& J, double* cvv, int parts = 3);
 void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* slots, int n);
+void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
+                       int* gA);
 int coordRunOccupancy(int kind, int boxKind, bool hi);
 // Once per (kernel, device, size): maximum shared-memory carveout and the
 // dynamic shared-memory limit of a persistent runs kernel.
 void runKernelSetup(const void* fn, size_t dynSmem);
 // Host planning: steps tile-major (fills row0 / tilesA of the items, returns the
-// accumulator row count); per-CTA ranges of numSteps over grid CTAs with preCost[b]
-// steps' worth of other work on CTA b; whether the upper pair bound can bind.
+// accumulator row count); per-CTA ranges of numSteps over grid CTAs; whether the
+// upper pair bound can bind.
 // itemsPerSys: items of one system (sysPosq / sysBox entry), item-major.
 int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps, int itemsPerSys);
-std::vector<int> balanceRanges(int numSteps, int grid, const std::vector<double>& preCost);
+// CTA b of the persistent grid runs steps [begin[b], begin[b + 1]) (coordRange)
+std::vector<int> balanceRanges(int numSteps, int grid);
 // Run pieces of the static ranges (maximal sub-runs of one tile on one CTA): the
 // piece slots of their last steps, item-contiguous in step order, and every
 // item's slot range. Returns the number of pieces.
