@@ -159,16 +159,16 @@ class Batch:
         return dict(self.phase_times_last)
 
     def phase_stamps(self):
-        """Raw records of the last phase_times call: (runs [grid, 10] = SM id,
-        coordination steps, eight %globaltimer stamps in ns; finalize [CTAs, 6])."""
+        """Raw records of the last phase_times call: (runs [grid, 11] = SM id,
+        coordination steps, nine %globaltimer stamps in ns; finalize [CTAs, 6])."""
         n = c_ll()
         call("glued_batch_phase_stamps", self._h, None, 0, ctypes.byref(n))
         buf = (ctypes.c_ulonglong * max(1, n.value))()
         call("glued_batch_phase_stamps", self._h, buf, n.value, ctypes.byref(n))
         v = np.array(buf[:n.value], dtype=np.uint64)
         grid = int(self.phase_times_last["grid"]) if hasattr(self, "phase_times_last") else 0
-        runs = v[:10 * grid].reshape(grid, 10)
-        return runs, v[10 * grid:].reshape(-1, 6)
+        runs = v[:11 * grid].reshape(grid, 11)
+        return runs, v[11 * grid:].reshape(-1, 6)
 
     @property
     def tuning(self):

@@ -324,7 +324,7 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool 
 // gathers are issued when the first step starts), then evaluates its slice.
 template <int RA, int BOX, int NH, bool HI>
 __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm, HillStage& hs) {
-    unsigned long long* st = B.stamps ? B.stamps + 9 * (size_t)blockIdx.x : nullptr;
+    unsigned long long* st = B.stamps ? B.stamps + 10 * (size_t)blockIdx.x : nullptr;
     if (st && threadIdx.x == 0) {
         unsigned sm;
         asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
@@ -339,7 +339,8 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     if (st && threadIdx.x == 0) st[1] = globalTimer();
     const int s0 = coordRange(B.R.numSteps, gridDim.x, blockIdx.x), s1 = coordRange(B.R.numSteps, gridDim.x, blockIdx.x + 1);
     if (s0 < s1) {
-        // profiling stamps 7 and 8: the first step's data has landed / the first step is done
+        // profiling stamps 7, 9 and 8: the first step's data has landed / the first
+        // step is done / the hill CVs evaluated after it are done
         if (hills)
             coordRun<RA, BOX, NH, HI>(
                 B.R, s0, s1, sm, NoPieceHook(),
@@ -349,6 +350,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
                     cpAsyncCommit();
                 },
                 [&]() {
+                    if (st && threadIdx.x == 0) st[9] = globalTimer();
                     hillCVs(B, 0, hs);   // read after the barriers of the hill slice
                     if (st && threadIdx.x == 0) st[8] = globalTimer();
                 });
@@ -356,7 +358,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
             coordRun<RA, BOX, NH, HI>(
                 B.R, s0, s1, sm, NoPieceHook(),
                 [&]() { if (st && threadIdx.x == 0) st[7] = globalTimer(); },
-                [&]() { if (st && threadIdx.x == 0) st[8] = globalTimer(); });
+                [&]() { if (st && threadIdx.x == 0) st[8] = st[9] = globalTimer(); });
     }
     if (st) { __syncthreads(); if (threadIdx.x == 0) st[2] = globalTimer(); }
     // the finalize (a programmatic dependent launch) may be scheduled once every
@@ -1095,7 +1097,7 @@ static double pct(std::vector<double>& v, double p) {
 // the layout of out[24] is given with glued_batch_phase_times.
 void Batch::phaseTimes(double* out) {
     Impl& I = *impl_;
-    constexpr int RS = 9, FS = 6;   // stamps per runs / finalize CTA
+    constexpr int RS = 10, FS = 6;   // stamps per runs / finalize CTA
     const int fg = I.W * I.parts;
     DBuf st;
     st.alloc(sizeof(unsigned long long) * (RS * (size_t)I.grid + FS * (size_t)fg));
@@ -1147,6 +1149,7 @@ void Batch::phaseTimes(double* out) {
             for (int k = 0; k < 6; k++) I.lastStamps.push_back(r[k]);
             I.lastStamps.push_back(r[7]);
             I.lastStamps.push_back(r[8]);
+            I.lastStamps.push_back(r[9]);
         }
         for (int g = 0; g < fg; g++)
             for (int k = 0; k < FS; k++) I.lastStamps.push_back(h[RS * (size_t)I.grid + FS * (size_t)g + k]);

@@ -309,7 +309,7 @@ int glued_batch_phase_times(glued_batch* b, double* out);
 /* Raw records of the last glued_batch_phase_times call: per runs CTA {SM id,
  * coordination steps, %globaltimer at entry, staging issued, coordination done,
  * hill data ready, hill evaluation done, exit, first step's data landed, first
- * step done}, then per finalize CTA six
+ * step and its hill-CV evaluation done, first step done}, then per finalize CTA six
  * %globaltimer stamps. *n = number of values; min(cap, *n) are copied to out
  * (out may be NULL when cap is 0). No reference counterpart.                   */
 int glued_batch_phase_stamps(glued_batch* b, unsigned long long* out, long long cap, long long* n);
