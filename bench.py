@@ -32,7 +32,7 @@ FLOP_PAIR = 45.0      # coordination pair, FMA = 2 flops (per-pair count of the 
 FLOP_HILL = 14.0      # one hill Gaussian + gradient (plus one exp)
 # DRAM bytes (read + write) of one launch, from the ncu captures summarised under
 # profiles/ (cold caches, one launch of the full workload)
-TRAFFIC_C4_RUNS = 7.853e6
+TRAFFIC_C4_RUNS = 8.581e6
 TRAFFIC_C2_COORD = 0.680e6
 
 
