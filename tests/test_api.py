@@ -101,14 +101,13 @@ def test_xml_rejects_bad_input():
     assert f.usesPeriodicBoundaryConditions() and f.getNumCollectiveVariables() == 1
 
 
-# The reference tree's location comes from the oracle's build recipe
-# (GLUED_REFERENCE, else the recipe's default); the test is skipped without it.
-from build_ref import DEFAULT_REF  # noqa: E402
-
-REF_GLUED = os.path.join(DEFAULT_REF, "python", "glued.py")
+# The reference tree's location comes from GLUED_REFERENCE only; the test is
+# skipped when it is unset.
+REF_GLUED = os.path.join(os.environ.get("GLUED_REFERENCE", ""), "python", "glued.py")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_GLUED), reason="reference tree not present")
+@pytest.mark.skipif(not (os.environ.get("GLUED_REFERENCE") and os.path.exists(REF_GLUED)),
+                    reason="GLUED_REFERENCE not set to a reference tree")
 def test_reference_glued_py_runs_unchanged_on_this_gluedplugin():
     """GLUED's own python/glued.py (imported from the reference tree, not copied)
     builds forces through this library's gluedplugin; its encoded parameter
