@@ -170,8 +170,8 @@ def time_steps(torch, step_fn, steps, warmup, flush):
 def run_single(args, torch, cfg):
     from gluedmd_b200 import workloads as W, _native
     import ctypes
-    w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"), "c2": W.config2,
-             "c3": W.config3}[cfg]()
+    w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"), "c1h": lambda: W.config1("hills"),
+         "c2": W.config2, "c3": W.config3}[cfg]()
     ctx, f = build_single(w, torch, "cuda")
     nc = ctx.glued_context_for(f)
     # correctness of this exact workload against the FP64 oracle (untimed)
@@ -605,12 +605,81 @@ def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
                        "MetaD as the reference's 256x256 grid holding the same 50,000 hills)")
 
 
+SUM_VARIANTS = {"fp64": (0, 0), "fp32": (1, 0), "fp32c": (2, 1)}
+
+
+def precision_sweep(args, torch):
+    """Step time (CUDA events, L2 flushed before every step) and error against the
+    FP64 oracle of each sum-precision variant of one workload; one JSON line each.
+    c1h / c3: kernel sums in FP64, FP32, FP32 two-sum (+ blocked coordination);
+    c2cut: the C2 cutoff coordination on all-pairs tiles and on the cell list, in
+    C2's 5.9 nm box and in a 12 nm box at the same density;
+    c2: no-fit RMSD or Kabsch RMSD (FP64 eigensolve), per-tile-run or blocked
+    coordination sums; c4: the batch in plain FP32 and in two-sum FP32."""
+    from gluedmd_b200 import workloads as W
+    P = _checker()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = []
+
+    def single(w, kernel_sums, coord, label):
+        ctx, f = build_single(w, torch, "cuda")
+        nc = ctx.glued_context_for(f)
+        nc.set_sum_precision(kernel_sums, coord)
+        e, F = ctx.computeForces()
+        err = P.check_single(w, e, F, np.array(f.getLastCVValues(ctx)))
+        err.pop("ref")
+
+        def step(i):
+            nc.update_state(i)
+            nc.execute(True, False)
+
+        ms = time_steps(torch, step, args.steps, args.warmup, flush)
+        out.append({"sweep": args.config, "variant": label, "workload": w.name, "us_per_step": ms * 1e3 / args.steps,
+                    "max_rel_force_err": err["force"], "energy_rel_err": err["energy"], "cv_rel_err": err["cv"],
+                    "kernel_sums": kernel_sums, "coordination_blocked": coord})
+
+    if args.config in ("c3", "c1h"):
+        w = W.config3() if args.config == "c3" else W.config1("hills")
+        for name, (k, c) in SUM_VARIANTS.items():
+            single(w, k, c, name)
+    elif args.config == "c2":
+        for fit in (False, True):
+            w = W.config2(fit=fit)
+            for blocked in (0, 1):
+                single(w, 0, blocked, ("kabsch" if fit else "nofit") + ("+blocked" if blocked else "+per-run"))
+    elif args.config == "c2cut":
+        for box in (5.9, 12.0):
+            for method in (0, 1):
+                single(W.config2_cutoff(method, box=box), 0, 0, ("tiles+mask" if method == 0 else "cells") +
+                       f" box {box:g} nm")
+    elif args.config == "c4":
+        from gluedmd_b200.batch import Batch, WalkerPool, force_for
+        ws, hill = c4_inputs()
+        pool = WalkerPool([w["pos"] for w in ws], [w["box"] for w in ws])
+        b = Batch([force_for(w["cvs"], c4_biases(w, hill)) for w in ws], pool.walkers)
+        b.set_hills(hill["centers"], hill["heights"])
+        tune = b.autotune()
+        for mode, name in ((1, "fp32"), (2, "fp32c")):
+            b.set_sum_precision(mode)
+            par = parity_c4(b, pool, ws, hill)
+            ms = time_steps(torch, lambda i: (b.update_state(i), b.execute()), args.steps, args.warmup, flush)
+            out.append({"sweep": "c4", "variant": name, "workload": C4_WORKLOAD, "us_per_step": ms * 1e3 / args.steps,
+                        "max_rel_force_err": par["max_rel_force_err"], "energy_rel_err": par["energy_rel_err"],
+                        "cv_rel_err": par["cv_rel_err"], "tuning": tune, "status": b.status()})
+    else:
+        raise SystemExit("--precision-sweep: config must be c1h, c2, c2cut, c3 or c4")
+    for line in out:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--config", default="c4", choices=["c1", "c1pb", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c1pb", "c1h", "c2", "c2cut", "c3", "c4", "c5"])
+    ap.add_argument("--precision-sweep", action="store_true",
+                    help="time and check every sum-precision variant of --config (one JSON line each)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -649,8 +718,8 @@ def main():
                                                 "d2h_bytes_per_step": 0}}
         else:
             from gluedmd_b200 import workloads as W
-            w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"), "c2": W.config2,
-             "c3": W.config3}[args.config]()
+            w = {"c1": lambda: W.config1("grid"), "c1pb": lambda: W.config1("pbmetad"),
+                 "c1h": lambda: W.config1("hills"), "c2": W.config2, "c3": W.config3}[args.config]()
             cb = cpu_baseline_single(args.config, w, budget_s=max(5.0, 0.5 * args.steps))
             line = {"impl": "reference", "metric": "CV+bias+force us/step", "value": cb["value"], "unit": "us/step",
                     "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
@@ -671,6 +740,10 @@ def main():
     from gluedmd_b200 import _native
     import ctypes
     pk, src = peaks()
+
+    if args.precision_sweep:
+        precision_sweep(args, torch)
+        return
 
     if args.config == "c4" and args.profile:
         ws, hill = c4_inputs(args.walkers, args.hills)

@@ -78,6 +78,9 @@ _SIGS = {
     "glued_context_set_multiwalker_ptrs": [c_void_p, c_int, P(c_ll), c_int],
     "glued_context_device_arrays": [c_void_p] + [P(c_void_p)] * 7 + [P(c_int), P(c_int)],
     "glued_context_opes_last_decision": [c_void_p, c_int, P(c_int)],
+    "glued_context_set_sum_precision": [c_void_p, c_int, c_int],
+    "glued_context_coordination_pairs": [c_void_p, c_int, P(c_int), c_ll, P(c_ll)],
+    "glued_context_get_sum_precision": [c_void_p, P(c_int), P(c_int)],
     "glued_context_profile_phases": [c_void_p, c_int, P(c_double), P(c_int)],
     "glued_context_launch_count": [c_void_p, P(c_ll)],
     "glued_measure_fp32_peak": [P(c_double)],
@@ -92,6 +95,9 @@ _SIGS = {
     "glued_batch_set_tuning": [c_void_p, P(c_int)],
     "glued_batch_get_tuning": [c_void_p, P(c_int)],
     "glued_batch_autotune": [c_void_p, P(c_int)],
+    "glued_batch_autotune_ex": [c_void_p, c_int, P(c_int), P(c_int)],
+    "glued_batch_set_sum_precision": [c_void_p, c_int],
+    "glued_batch_get_sum_precision": [c_void_p, P(c_int)],
     "glued_batch_execute": [c_void_p],
     "glued_batch_update_state": [c_void_p, c_int],
     "glued_batch_get_energies": [c_void_p, P(c_double)],

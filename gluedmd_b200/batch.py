@@ -174,16 +174,29 @@ class Batch:
     def tuning(self):
         t = (c_int * 4)()
         call("glued_batch_get_tuning", self._h, t)
-        return dict(ra=t[0], parts=t[1], plain=t[2])
+        return dict(ra=t[0], parts=t[1], plain=t[2], ch=t[3])
 
-    def set_tuning(self, ra=8, parts=0, plain=0):
-        t = (c_int * 4)(ra, parts, plain, 0)
+    def set_tuning(self, ra=8, parts=0, plain=0, ch=128):
+        t = (c_int * 4)(ra, parts, plain, ch)
         call("glued_batch_set_tuning", self._h, t)
 
-    def autotune(self):
+    def set_sum_precision(self, mode):
+        """1: plain FP32 sums; 2: two-sum compensated hill sums, blocked coordination."""
+        call("glued_batch_set_sum_precision", self._h, int(mode))
+
+    def sum_precision(self):
+        m = c_int()
+        call("glued_batch_get_sum_precision", self._h, ctypes.byref(m))
+        return m.value
+
+    def autotune(self, use_cache=True):
+        """glued_batch_autotune_ex: the fastest tiling (cached per batch signature
+        for the process unless use_cache is False); self.tune_cached tells which."""
         t = (c_int * 4)()
-        call("glued_batch_autotune", self._h, t)
-        return dict(ra=t[0], parts=t[1], plain=t[2])
+        cached = c_int()
+        call("glued_batch_autotune_ex", self._h, 1 if use_cache else 0, t, ctypes.byref(cached))
+        self.tune_cached = bool(cached.value)
+        return dict(ra=t[0], parts=t[1], plain=t[2], ch=t[3])
 
 
 def force_for(cvs, biases, pbc=True):

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 
 #include "batch.hpp"
@@ -209,9 +210,17 @@ __device__ void hillCVs(const BatchDev& B, int wb, HillStage& hs) {
 // The hill pairs p = lane, lane + 32, ... (< np) of the staged chunk against the
 // JW walkers of this warp, two hills per packed instruction; acc[j][c]: packed
 // partial sums of g, g dx, g dy for walker slot j.
-template <bool P0, bool P1>
+// Packed two-sum: s + c gains b with the rounding error of the addition kept in c.
+__device__ __forceinline__ void twoSum2(unsigned long long& s, unsigned long long& c, unsigned long long b) {
+    const unsigned long long t = f2::add(s, b), bb = f2::sub(t, s);
+    c = f2::add(c, f2::add(f2::sub(s, f2::sub(t, bb)), f2::sub(b, bb)));
+    s = t;
+}
+
+template <bool P0, bool P1, bool COMP>
 __device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, int np, const float (&s0)[JW],
-                                         const float (&s1)[JW], unsigned long long (&acc)[JW][3]) {
+                                         const float (&s1)[JW], unsigned long long (&acc)[JW][3],
+                                         unsigned long long (&cmp)[JW][3]) {
     constexpr float R = 12582912.0f;   // 1.5 * 2^23: adding and removing it rounds to an integer
     const int lane = threadIdx.x & 31;
     const unsigned long long R2 = f2::pk(R, R);
@@ -238,15 +247,44 @@ __device__ __forceinline__ void hillEval(const HillStage& hs, const BHill& hb, i
             ga = ea <= hb.cut ? ga : 0.0f;
             gb = eb <= hb.cut ? gb : 0.0f;
             const unsigned long long g = f2::mul(hh, f2::pk(ga, gb));
-            acc[j][0] = f2::add(acc[j][0], g);
-            acc[j][1] = f2::fma(g, dx, acc[j][1]);
-            acc[j][2] = f2::fma(g, dy, acc[j][2]);
+            if (COMP) {
+                twoSum2(acc[j][0], cmp[j][0], g);
+                twoSum2(acc[j][1], cmp[j][1], f2::mul(g, dx));
+                twoSum2(acc[j][2], cmp[j][2], f2::mul(g, dy));
+            } else {
+                acc[j][0] = f2::add(acc[j][0], g);
+                acc[j][1] = f2::fma(g, dx, acc[j][1]);
+                acc[j][2] = f2::fma(g, dy, acc[j][2]);
+            }
         }
     }
 }
 
+// warpTransposeSum32 with a two-sum at every addition: e[] holds the slots'
+// compensation terms, which travel (and add up) with them; *err = the result's.
+__device__ __forceinline__ float warpTransposeSum32C(float (&v)[32], float (&e)[32], float& err) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < o; i++) {
+            const float sv = up ? v[i] : v[i + o], kv = up ? v[i + o] : v[i];
+            const float se = up ? e[i] : e[i + o], ke = up ? e[i + o] : e[i];
+            const float rv = __shfl_xor_sync(0xffffffffu, sv, o), re = __shfl_xor_sync(0xffffffffu, se, o);
+            const float t = __fadd_rn(kv, rv), bb = __fsub_rn(t, kv);
+            e[i] = __fadd_rn(__fadd_rn(ke, re), __fadd_rn(__fsub_rn(kv, __fsub_rn(t, bb)), __fsub_rn(rv, bb)));
+            v[i] = t;
+        }
+    }
+    err = e[0];
+    return v[0];
+}
+
 // This CTA's hill slice for every walker. `gathered`: the data of walker block
-// 0 was issued during the coordination steps.
+// 0 was issued during the coordination steps. COMP: two-sum compensated sums
+// (per lane, through the lane tree; the walker's value is hi + lo in FP64).
+template <bool COMP>
 __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool cvsDone, unsigned long long* st) {
     const BHill& hb = B.hill;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -279,9 +317,12 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool 
             const int wl = min(warp + COORD_NW * j, nw - 1);
             s0[j] = hs.sS[wl * 2]; s1[j] = hs.sS[wl * 2 + 1];
         }
-        unsigned long long pacc[JW][3];
+        unsigned long long pacc[JW][3], pcmp[JW][3];   // pcmp: compensation terms (COMP only)
 #pragma unroll
-        for (int j = 0; j < JW; j++) pacc[j][0] = pacc[j][1] = pacc[j][2] = 0ull;
+        for (int j = 0; j < JW; j++) {
+            pacc[j][0] = pacc[j][1] = pacc[j][2] = 0ull;
+            if (COMP) pcmp[j][0] = pcmp[j][1] = pcmp[j][2] = 0ull;
+        }
         for (int c0 = g0; c0 < g1; c0 += HS / 4) {
             if (c0 != g0) {
                 __syncthreads();
@@ -292,29 +333,51 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool 
             }
             const int np = 2 * min(g1 - c0, HS / 4);   // hill pairs staged
             const bool p0 = hb.pS[0] > 0.0f, p1 = hb.pS[1] > 0.0f;
-            if (p0 && p1) hillEval<true, true>(hs, hb, np, s0, s1, pacc);
-            else if (p0) hillEval<true, false>(hs, hb, np, s0, s1, pacc);
-            else if (p1) hillEval<false, true>(hs, hb, np, s0, s1, pacc);
-            else hillEval<false, false>(hs, hb, np, s0, s1, pacc);
+            if (p0 && p1) hillEval<true, true, COMP>(hs, hb, np, s0, s1, pacc, pcmp);
+            else if (p0) hillEval<true, false, COMP>(hs, hb, np, s0, s1, pacc, pcmp);
+            else if (p1) hillEval<false, true, COMP>(hs, hb, np, s0, s1, pacc, pcmp);
+            else hillEval<false, false, COMP>(hs, hb, np, s0, s1, pacc, pcmp);
         }
         if (st && wb == 0 && threadIdx.x == 0) st[4] = globalTimer();
-        float acc[32];
+        // lane 3 j + c: component c of walker slot j
+        double v;
+        if constexpr (COMP) {
+            float acc[32], cme[32];
 #pragma unroll
-        for (int j = 0; j < JW; j++)
+            for (int j = 0; j < JW; j++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                float a, b;
-                f2::upk(pacc[j][c], a, b);
-                acc[3 * j + c] = a + b;
-            }
+                for (int c = 0; c < 3; c++) {
+                    float a, b, ca, cb;
+                    f2::upk(pacc[j][c], a, b);
+                    f2::upk(pcmp[j][c], ca, cb);
+                    const float t = __fadd_rn(a, b), bb = __fsub_rn(t, a);
+                    acc[3 * j + c] = t;
+                    cme[3 * j + c] = __fadd_rn(__fadd_rn(ca, cb), __fadd_rn(__fsub_rn(a, __fsub_rn(t, bb)),
+                                                                             __fsub_rn(b, bb)));
+                }
 #pragma unroll
-        for (int k = 3 * JW; k < 32; k++) acc[k] = 0.0f;
-        const float v = warpTransposeSum32(acc);   // lane 3 j + c: component c of walker slot j
+            for (int k = 3 * JW; k < 32; k++) acc[k] = cme[k] = 0.0f;
+            float lo;
+            const float hi = warpTransposeSum32C(acc, cme, lo);
+            v = (double)hi + (double)lo;
+        } else {
+            float acc[32];
+#pragma unroll
+            for (int j = 0; j < JW; j++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    float a, b;
+                    f2::upk(pacc[j][c], a, b);
+                    acc[3 * j + c] = a + b;
+                }
+#pragma unroll
+            for (int k = 3 * JW; k < 32; k++) acc[k] = 0.0f;
+            v = (double)warpTransposeSum32(acc);
+        }
         const int j = lane / 3, c = lane - 3 * j;
         const int wl = warp + COORD_NW * j;
         if (lane < 3 * JW && wl < nw)
-            B.hillPart[3 * ((size_t)blockIdx.x * B.W + w0 + wl) + c] =
-                c == 0 ? (double)v : (double)v * (c == 1 ? hb.gsc[0] : hb.gsc[1]);
+            B.hillPart[3 * ((size_t)blockIdx.x * B.W + w0 + wl) + c] = c == 0 ? v : v * (c == 1 ? hb.gsc[0] : hb.gsc[1]);
     }
 }
 
@@ -322,8 +385,8 @@ __device__ void hillSlice(const BatchDev& B, HillStage& hs, bool gathered, bool 
 // Persistent CTAs (grid = SMs x resident CTAs): CTA b copies its hill tables,
 // runs its static range of coordination steps (equal step counts; the hill
 // gathers are issued when the first step starts), then evaluates its slice.
-template <int RA, int BOX, int NH, bool HI>
-__device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm, HillStage& hs) {
+template <int RA, int RB, int BOX, int NH, bool HI, bool COMP>
+__device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA, RB>& sm, HillStage& hs) {
     unsigned long long* st = B.stamps ? B.stamps + 10 * (size_t)blockIdx.x : nullptr;
     if (st && threadIdx.x == 0) {
         unsigned sm;
@@ -342,7 +405,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
         // profiling stamps 7, 9 and 8: the first step's data has landed / the first
         // step is done / the hill CVs evaluated after it are done
         if (hills)
-            coordRun<RA, BOX, NH, HI>(
+            coordRun<RA, RB, BOX, NH, HI, COMP>(
                 B.R, s0, s1, sm, NoPieceHook(),
                 [&]() {
                     if (st && threadIdx.x == 0) st[7] = globalTimer();
@@ -355,7 +418,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
                     if (st && threadIdx.x == 0) st[8] = globalTimer();
                 });
         else
-            coordRun<RA, BOX, NH, HI>(
+            coordRun<RA, RB, BOX, NH, HI, COMP>(
                 B.R, s0, s1, sm, NoPieceHook(),
                 [&]() { if (st && threadIdx.x == 0) st[7] = globalTimer(); },
                 [&]() { if (st && threadIdx.x == 0) st[8] = st[9] = globalTimer(); });
@@ -364,7 +427,7 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
     // the finalize (a programmatic dependent launch) may be scheduled once every
     // CTA is here; it waits for this grid's completion before reading its output
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    if (hills) hillSlice(B, hs, s0 < s1, s0 < s1, st);
+    if (hills) hillSlice<COMP>(B, hs, s0 < s1, s0 < s1, st);
     if (st) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -376,14 +439,14 @@ __device__ __forceinline__ void runsBody(const BatchDev& B, CoordRunSmem<RA>& sm
 
 // Dynamic shared memory: the coordination buffers, then (with a hill bias) the
 // hill staging area.
-template <int RA>
-constexpr size_t hillStageOffset() { return (sizeof(CoordRunSmem<RA>) + 255) / 256 * 256; }
+template <int RA, int RB>
+constexpr size_t hillStageOffset() { return (sizeof(CoordRunSmem<RA, RB>) + 255) / 256 * 256; }
 
-template <int RA, int BOX, int NH, bool HI>
+template <int RA, int RB, int BOX, int NH, bool HI, bool COMP>
 __global__ void __launch_bounds__(RUNS_THREADS, 1) k_batch_runs(BatchDev B) {
     extern __shared__ __align__(256) unsigned char dsm[];
-    runsBody<RA, BOX, NH, HI>(B, *reinterpret_cast<CoordRunSmem<RA>*>(dsm),
-                              *reinterpret_cast<HillStage*>(dsm + hillStageOffset<RA>()));
+    runsBody<RA, RB, BOX, NH, HI, COMP>(B, *reinterpret_cast<CoordRunSmem<RA, RB>*>(dsm),
+                                        *reinterpret_cast<HillStage*>(dsm + hillStageOffset<RA, RB>()));
 }
 
 // ------------------------------------------------------------- finalize
@@ -583,15 +646,46 @@ __global__ void __launch_bounds__(FT) k_batch_finalize(BatchDev B) {
 
 typedef void (*RunsFn)(BatchDev);
 
-template <int NH>
+template <int NH, bool COMP>
 RunsFn runsKernelB(int box, bool hi) {
-    if (box == 0) return k_batch_runs<8, 0, NH, true>;
-    if (box == 1) return hi ? k_batch_runs<8, 1, NH, true> : k_batch_runs<8, 1, NH, false>;
-    return hi ? k_batch_runs<8, 2, NH, true> : k_batch_runs<8, 2, NH, false>;
+    if (box == 0) return k_batch_runs<8, 4, 0, NH, true, COMP>;
+    if (box == 1) return hi ? k_batch_runs<8, 4, 1, NH, true, COMP> : k_batch_runs<8, 4, 1, NH, false, COMP>;
+    return hi ? k_batch_runs<8, 4, 2, NH, true, COMP> : k_batch_runs<8, 4, 2, NH, false, COMP>;
 }
 
-RunsFn runsKernel(int box, int kind, bool hi) {
-    return kind == 3 ? runsKernelB<3>(box, hi) : kind == -1 ? runsKernelB<-1>(box, true) : runsKernelB<0>(box, true);
+template <bool COMP>
+RunsFn runsKernelK(int box, int kind, bool hi) {
+    return kind == 3    ? runsKernelB<3, COMP>(box, hi)
+           : kind == -1 ? runsKernelB<-1, COMP>(box, true)
+                        : runsKernelB<0, COMP>(box, true);
+}
+
+// Other tile shapes (RA A atoms per warp, RB B atoms per lane) for the
+// autotuner: the n = 6, m = 12 switch in rectangular or no boxes, plain sums.
+template <int RA, int RB>
+RunsFn runsKernelShape(int box, bool hi) {
+    if (box == 0) return k_batch_runs<RA, RB, 0, 3, true, false>;
+    return hi ? k_batch_runs<RA, RB, 1, 3, true, false> : k_batch_runs<RA, RB, 1, 3, false, false>;
+}
+
+bool shapeAvailable(int box, int kind, bool comp, int ra, int ch) {
+    if (ra == 8 && ch == 128) return true;
+    return kind == 3 && !comp && box != 2 && (ra == 4 || ra == 8) && (ch == 128 || ch == 256);
+}
+
+// comp: two-sum compensated hill sums and blocked coordination A sums.
+RunsFn runsKernel(int box, int kind, bool hi, bool comp, int ra, int ch) {
+    if (ra == 4 && ch == 128) return runsKernelShape<4, 4>(box, hi);
+    if (ra == 8 && ch == 256) return runsKernelShape<8, 8>(box, hi);
+    if (ra == 4 && ch == 256) return runsKernelShape<4, 8>(box, hi);
+    return comp ? runsKernelK<true>(box, kind, hi) : runsKernelK<false>(box, kind, hi);
+}
+
+size_t runsSmemOffset(int ra, int ch) {
+    if (ra == 4 && ch == 128) return hillStageOffset<4, 4>();
+    if (ra == 8 && ch == 256) return hillStageOffset<8, 8>();
+    if (ra == 4 && ch == 256) return hillStageOffset<4, 8>();
+    return hillStageOffset<8, 4>();
 }
 
 __global__ void k_batch_deposit(BatchDev B) {
@@ -634,6 +728,23 @@ struct Batch::Impl {
     DBuf hMirror, hCenters, hHeights, hCount;
     BHill hill{};
     BatchTuning tune;
+    int sumMode = SUM_FP32;   // SUM_FP32: plain FP32 sums; SUM_FP32C: two-sum hills, blocked coordination
+    bool cachedTune = false;  // the last autotune returned a cached choice
+    // autotuner cache key: walker count, coordination group sizes, hill count
+    // (power-of-two bucket), box kind, switch kind, sum precision
+    int hostHillCount() const {
+        int n = 0;
+        cudaCheck(cudaMemcpy(&n, hill.count, sizeof(int), cudaMemcpyDeviceToHost), "hills");
+        return n;
+    }
+    std::string signature() const {
+        std::string k = std::to_string(W) + "|" + std::to_string(nC);
+        for (int c = 0; c < nC; c++) k += "|" + std::to_string(items[c].nA) + "x" + std::to_string(items[c].nB);
+        int hb = 0;
+        for (int n = hill.present ? hostHillCount() : 0; n > 0; n >>= 1) hb++;
+        return k + "|h" + std::to_string(hb) + "|b" + std::to_string(boxKind) + "|k" + std::to_string(kind) + "|s" +
+               std::to_string(sumMode);
+    }
     BatchDev dev{};
     int grid = 0;        // coordination runs: SMs x resident CTAs
     int rows = 0;        // coordination rows of one walker
@@ -652,7 +763,7 @@ struct Batch::Impl {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
     }
 
-    RunsFn runs() const { return runsKernel(boxKind, kind, hi); }
+    RunsFn runs() const { return runsKernel(boxKind, kind, hi, sumMode == SUM_FP32C, tune.ra, tune.ch); }
 
     // Per-CTA step ranges (equal step counts) and the run pieces to match. The
     // device copies are rewritten in place (a captured graph keeps their
@@ -672,13 +783,14 @@ struct Batch::Impl {
         }
         // per-step gather tables (slot = user atom index in a walker's posq)
         const size_t n = std::max<size_t>(1, steps.size());
-        if (gBD.bytes < sizeof(int) * COORD_CH * n) { gBD.alloc(sizeof(int) * COORD_CH * n); destroyGraph(); }
-        if (gAD.bytes < sizeof(int) * COORD_TA * n) { gAD.alloc(sizeof(int) * COORD_TA * n); destroyGraph(); }
+        const int ta = COORD_NW * tune.ra, ch = tune.ch;
+        if (gBD.bytes < sizeof(int) * ch * n) { gBD.alloc(sizeof(int) * ch * n); destroyGraph(); }
+        if (gAD.bytes < sizeof(int) * ta * n) { gAD.alloc(sizeof(int) * ta * n); destroyGraph(); }
         std::vector<const float4*> stepPosq(n, nullptr);
         for (size_t k = 0; k < steps.size(); k++) stepPosq[k] = walkersH[steps[k].sys].posq;
         put(stepPosqD, stepPosq.data(), sizeof(const float4*) * n);
         launchStepGathers(0, stepsD.as<CoordStep>(), (int)steps.size(), grid, atomsD.as<int>(), gBD.as<int>(),
-                          gAD.as<int>());
+                          gAD.as<int>(), ta, ch);
         cudaCheck(cudaGetLastError(), "gather tables");
         cudaCheck(cudaDeviceSynchronize(), "gather tables");
         dev.R.numSteps = (int)steps.size();
@@ -695,7 +807,7 @@ struct Batch::Impl {
 
     void plan() {
         // coordination steps over all walkers' items (walker-major)
-        buildCoordSteps(items, 8, steps, std::max(nC, 1));
+        buildCoordSteps(items, tune.ra, tune.ch, steps, std::max(nC, 1));
         rows = 0;
         for (int c = 0; c < nC; c++) rows += items[c].nA + items[c].nB;
         std::vector<const float4*> posqOf(W);
@@ -779,7 +891,7 @@ struct Batch::Impl {
 
     // dynamic shared memory of the runs kernel: coordination buffers, then the
     // hill staging area
-    size_t dynSmem() const { return hillStageOffset<8>() + (hill.present ? sizeof(HillStage) : 0); }
+    size_t dynSmem() const { return runsSmemOffset(tune.ra, tune.ch) + (hill.present ? sizeof(HillStage) : 0); }
 
     void launchRuns(cudaStream_t s) {
         void* args[] = {&dev};
@@ -993,7 +1105,11 @@ void Batch::setStream(cudaStream_t s) {
 }
 
 void Batch::setTuning(const BatchTuning& t) {
-    if (t.ra != 8) throw Error(GLUED_E_INVALID, "batch tuning: ra must be 8");
+    if ((t.ra != 4 && t.ra != 8) || (t.ch != 128 && t.ch != 256))
+        throw Error(GLUED_E_INVALID, "batch tuning: ra must be 4 or 8 and the B chunk 128 or 256");
+    if (!shapeAvailable(impl_->boxKind, impl_->kind, impl_->sumMode == SUM_FP32C, t.ra, t.ch))
+        throw Error(GLUED_E_INVALID, "batch tuning: tile shapes other than ra 8 / chunk 128 need the n = 6, m = 12 "
+                                     "switch, a rectangular or no box and plain FP32 sums");
     if (t.parts < 0 || t.parts > 4096) throw Error(GLUED_E_INVALID, "batch tuning: finalize parts must be 0..4096");
     if (t.plain != 0 && t.plain != 1) throw Error(GLUED_E_INVALID, "batch tuning: finalize launch mode must be 0 or 1");
     cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
@@ -1002,6 +1118,28 @@ void Batch::setTuning(const BatchTuning& t) {
 }
 
 BatchTuning Batch::tuning() const { return impl_->tune; }
+bool Batch::lastTuneCached() const { return impl_->cachedTune; }
+
+void Batch::setSumPrecision(int mode) {
+    if (mode != SUM_FP32 && mode != SUM_FP32C)
+        throw Error(GLUED_E_INVALID, "batch sum precision: mode must be 1 (FP32) or 2 (FP32 two-sum)");
+    cudaCheck(cudaStreamSynchronize(impl_->stream), "sync");
+    if (mode != impl_->sumMode) {
+        impl_->sumMode = mode;
+        impl_->destroyGraph();
+        BatchTuning& t = impl_->tune;
+        if (!shapeAvailable(impl_->boxKind, impl_->kind, mode == SUM_FP32C, t.ra, t.ch)) {
+            // compensated sums exist in the default tile shape only
+            t.ra = 8;
+            t.ch = 128;
+            impl_->plan();
+        }
+        // the other instantiation of the runs kernel: its shared-memory limit
+        runKernelSetup((const void*)impl_->runs(), impl_->dynSmem());
+    }
+}
+
+int Batch::sumPrecision() const { return impl_->sumMode; }
 
 void Batch::execute() {
     Impl& I = *impl_;
@@ -1034,9 +1172,35 @@ void Batch::execute() {
 // combination is kept. Every timed step starts with L2 flushed (a 192 MB memset
 // between steps), as in an MD loop where the engine's own kernels run between
 // force evaluations; the flush buffer is freed before returning.
-BatchTuning Batch::autotune() {
+// Choices of the autotuner, per batch signature (signature()), for the process.
+static std::map<std::string, BatchTuning>& tuneCache() {
+    static std::map<std::string, BatchTuning> m;
+    return m;
+}
+static std::mutex& tuneCacheMutex() {
+    static std::mutex m;
+    return m;
+}
+
+BatchTuning Batch::autotune(bool useCache) {
     Impl& I = *impl_;
     cudaCheck(cudaStreamSynchronize(I.stream), "sync");
+    if (useCache) {
+        BatchTuning hit;
+        bool found = false;
+        {
+            std::lock_guard<std::mutex> lock(tuneCacheMutex());
+            auto it = tuneCache().find(I.signature());
+            if (it != tuneCache().end()) { hit = it->second; found = true; }
+        }
+        if (found) {
+            I.tune = hit;
+            I.plan();
+            I.cachedTune = true;
+            return hit;
+        }
+    }
+    I.cachedTune = false;
     size_t maxPad = 0;
     for (auto& w : I.walkersH) maxPad = std::max(maxPad, (size_t)w.padded);
     I.scratchForce.alloc(sizeof(long long) * 3 * maxPad);
@@ -1051,10 +1215,18 @@ BatchTuning Batch::autotune() {
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
     const int base = I.minParts();
-    for (int plain : {0, 1})
-        for (int mul : {1, 2, 4}) {
-            BatchTuning t;
-            t.ra = 8; t.parts = base * mul; t.plain = plain;
+    std::vector<BatchTuning> cands;
+    for (int ra : {8, 4})
+        for (int ch : {128, 256}) {
+            if (!shapeAvailable(I.boxKind, I.kind, I.sumMode == SUM_FP32C, ra, ch)) continue;
+            for (int plain : {0, 1})
+                for (int mul : {1, 2, 4}) {
+                    BatchTuning t;
+                    t.ra = ra; t.ch = ch; t.parts = base * mul; t.plain = plain;
+                    cands.push_back(t);
+                }
+        }
+    for (const BatchTuning& t : cands) {
             I.tune = t;
             I.plan();
             for (int r = 0; r < 2; r++) I.launch(I.stream);
@@ -1080,6 +1252,10 @@ BatchTuning Batch::autotune() {
     I.tune = best;
     I.plan();
     I.lastMs = bestMs;
+    {
+        std::lock_guard<std::mutex> lock(tuneCacheMutex());
+        tuneCache()[I.signature()] = best;
+    }
     return best;
 }
 

@@ -159,8 +159,19 @@ __device__ __noinline__ void evalPbmetad(const BiasDev& b, const double* cvv, do
 
 // Kernel sums of the OPES and hill-sum MetaD biases (CommonGluedKernels.cpp:2642-2700
 // for OPES), spread over KSUM_CTAS CTAs per bias: each CTA sums a contiguous
-// range of kernels (per thread, then a fixed block tree) into 9 FP64 partials
-// {dV/ds_0..7 terms, value}; k_biases sums the partials in CTA order.
+// range of kernels into 9 FP64 partials {dV/ds_0..7 terms, value}; k_biases sums
+// the partials in CTA order.
+//
+// MODE (the context's sum precision): SUM_FP64 evaluates and sums every kernel
+// in FP64 (per thread, then a fixed block tree). SUM_FP32 / SUM_FP32C evaluate
+// the Gaussians and accumulate in FP32, plain or with a two-sum compensation
+// term per accumulator (also through the warp tree); the exponent that decides
+// whether a hill counts (> 8 truncated, a jump of h e^-8) is still formed in
+// FP64, so that decision is the FP64 path's. OPES heights exp(logW) are taken
+// relative to the largest logW of the warp, M_w: FP32 holds exp(logW - M_w) <= 1,
+// and the warp's sums are scaled by exp(M_w) in FP64 when they become partials
+// (the log-sum-exp normalisation in FP64). Kernels whose FP64 height would not
+// be finite (logW >= log 1e308) are skipped in every mode.
 //
 // The kernel tables (count, centres, sigmas, log-weights; hill centres and
 // heights) are written only by the deposit kernels of updateState, which have
@@ -168,6 +179,20 @@ __device__ __noinline__ void evalPbmetad(const BiasDev& b, const double* cvv, do
 // its own wait, or is a plain launch); so the record, the count and each
 // thread's first OPES kernel are loaded before the wait, and only the CV values
 // of the kernel before are read after it.
+__device__ __forceinline__ void twoSumAcc(float& s, float& c, float b) {
+    const float t = __fadd_rn(s, b);
+    const float bb = __fsub_rn(t, s);
+    c = __fadd_rn(c, __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(b, bb)));
+    s = t;
+}
+
+template <int MODE>
+__device__ __forceinline__ void accF(float& s, float& c, float b) {
+    if (MODE == SUM_FP32C) twoSumAcc(s, c, b);
+    else s = __fadd_rn(s, b);
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__ biases,
                                                       const double* __restrict__ cvv, double* __restrict__ part) {
     __shared__ double red[32 * 9];
@@ -182,6 +207,7 @@ __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__
     const int K = type == BIAS_OPES ? *b.numKernels : *b.hCount;
     const int k0 = (int)((long long)K * blockIdx.x / gridDim.x);
     const int k1 = (int)((long long)K * (blockIdx.x + 1) / gridDim.x);
+    constexpr double LW_MAX = 709.1962086421661;   // log(1e308)
     double pc[8], ps[8], plw = 0.0;
     const int kf = k0 + tid;
     if (type == BIAS_OPES && kf < k1) {
@@ -191,44 +217,125 @@ __global__ void __launch_bounds__(256) k_kernel_sums(const BiasDev* __restrict__
     pdlEnter();
     double s[8];
     for (int d = 0; d < D; d++) s[d] = cvv[b.cvIdx[d]];
-    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (type == BIAS_OPES) {
-        const double kfloor = exp(-0.5 * b.cutoff2);
-        for (int k = kf; k < k1; k += nt) {
-            const bool first = k == kf;
-            double n2 = 0, dc[8], is2[8];
-            for (int d = 0; d < D; d++) {
-                dc[d] = s[d] - (first ? pc[d] : b.centers[k * D + d]);
-                double sg = first ? ps[d] : b.sigmas[k * D + d];
-                is2[d] = 1.0 / (sg * sg);
-                n2 += dc[d] * dc[d] * is2[d];
+    if constexpr (MODE == SUM_FP64) {
+        double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (type == BIAS_OPES) {
+            const double kfloor = exp(-0.5 * b.cutoff2);
+            for (int k = kf; k < k1; k += nt) {
+                const bool first = k == kf;
+                double n2 = 0, dc[8], is2[8];
+                for (int d = 0; d < D; d++) {
+                    dc[d] = s[d] - (first ? pc[d] : b.centers[k * D + d]);
+                    double sg = first ? ps[d] : b.sigmas[k * D + d];
+                    is2[d] = 1.0 / (sg * sg);
+                    n2 += dc[d] * dc[d] * is2[d];
+                }
+                if (!(n2 < b.cutoff2)) continue;
+                double G = exp(-0.5 * n2), kern = G - kfloor;
+                if (kern <= 0.0) continue;
+                double h = exp(first ? plw : b.logW[k]);
+                if (!(h > 0.0 && h < 1e308)) continue;
+                acc[8] += h * kern;
+                for (int d = 0; d < D; d++) acc[d] += h * G * (-dc[d] * is2[d]);
             }
-            if (!(n2 < b.cutoff2)) continue;
-            double G = exp(-0.5 * n2), kern = G - kfloor;
-            if (kern <= 0.0) continue;
-            double h = exp(first ? plw : b.logW[k]);
-            if (!(h > 0.0 && h < 1e308)) continue;
-            acc[8] += h * kern;
-            for (int d = 0; d < D; d++) acc[d] += h * G * (-dc[d] * is2[d]);
+        } else {
+            // direct hill sum, exponent > 8 truncated like the grid deposit
+            for (int k = k0 + tid; k < k1; k += nt) {
+                double ex = 0, dc[8];
+                for (int d = 0; d < D; d++) {
+                    double x = s[d] - b.hCenters[k * D + d];
+                    if (b.period[d] > 0) x -= round(x / b.period[d]) * b.period[d];
+                    dc[d] = x;
+                    ex += x * x / (2.0 * b.sigma[d] * b.sigma[d]);
+                }
+                if (ex > 8.0) continue;
+                double g = b.hHeights[k] * exp(-ex);
+                acc[8] += g;
+                for (int d = 0; d < D; d++) acc[d] += -g * dc[d] / (b.sigma[d] * b.sigma[d]);
+            }
         }
+        blockSum<9>(acc, red);
+        if (tid < 9) part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 9 + tid] = acc[tid];
     } else {
-        // direct hill sum, exponent > 8 truncated like the grid deposit
-        for (int k = k0 + tid; k < k1; k += nt) {
-            double ex = 0, dc[8];
-            for (int d = 0; d < D; d++) {
-                double x = s[d] - b.hCenters[k * D + d];
-                if (b.period[d] > 0) x -= round(x / b.period[d]) * b.period[d];
-                dc[d] = x;
-                ex += x * x / (2.0 * b.sigma[d] * b.sigma[d]);
+        float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, cmp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int lane = tid & 31, warp = tid >> 5;
+        double M = 0.0;   // OPES: the warp's largest logW (-inf: no kernel in the warp)
+        if (type == BIAS_OPES) {
+            double m = -INFINITY;
+            for (int k = kf; k < k1; k += nt) {
+                const double lw = k == kf ? plw : b.logW[k];
+                if (lw < LW_MAX && lw > m) m = lw;
             }
-            if (ex > 8.0) continue;
-            double g = b.hHeights[k] * exp(-ex);
-            acc[8] += g;
-            for (int d = 0; d < D; d++) acc[d] += -g * dc[d] / (b.sigma[d] * b.sigma[d]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            M = m;
+            const float kfloor = __expf(-0.5f * (float)b.cutoff2);
+            const float cut2 = (float)b.cutoff2;
+            for (int k = kf; k < k1; k += nt) {
+                const bool first = k == kf;
+                const double lw = first ? plw : b.logW[k];
+                if (!(lw < LW_MAX)) continue;
+                float n2 = 0.0f, dc[8], is2[8];
+                for (int d = 0; d < D; d++) {
+                    dc[d] = (float)(s[d] - (first ? pc[d] : b.centers[k * D + d]));
+                    const float isg = __frcp_rn((float)(first ? ps[d] : b.sigmas[k * D + d]));
+                    const float u = dc[d] * isg;
+                    is2[d] = isg * isg;
+                    n2 = fmaf(u, u, n2);
+                }
+                if (!(n2 < cut2)) continue;
+                const float G = __expf(-0.5f * n2), kern = G - kfloor;
+                if (kern <= 0.0f) continue;
+                const float h = __expf((float)(lw - M));
+                accF<MODE>(acc[8], cmp[8], h * kern);
+                const float hG = h * G;
+                for (int d = 0; d < D; d++) accF<MODE>(acc[d], cmp[d], hG * (-dc[d] * is2[d]));
+            }
+        } else {
+            for (int k = k0 + tid; k < k1; k += nt) {
+                double ex = 0;
+                float dc[8];
+                for (int d = 0; d < D; d++) {
+                    double x = s[d] - b.hCenters[k * D + d];
+                    if (b.period[d] > 0) x -= round(x / b.period[d]) * b.period[d];
+                    dc[d] = (float)x;
+                    ex += x * x / (2.0 * b.sigma[d] * b.sigma[d]);
+                }
+                if (ex > 8.0) continue;
+                const float g = (float)b.hHeights[k] * __expf(-(float)ex);
+                accF<MODE>(acc[8], cmp[8], g);
+                for (int d = 0; d < D; d++) accF<MODE>(acc[d], cmp[d], -g * dc[d] * b.isg2f[d]);
+            }
+        }
+        // warp tree (the compensation terms travel with their sums), then the
+        // warps' partials in FP64, scaled by exp(M_w), summed in warp order
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float hs = __shfl_xor_sync(0xffffffffu, acc[i], o);
+                if (MODE == SUM_FP32C) {
+                    const float hc = __shfl_xor_sync(0xffffffffu, cmp[i], o);
+                    cmp[i] = __fadd_rn(cmp[i], hc);
+                    twoSumAcc(acc[i], cmp[i], hs);
+                } else {
+                    acc[i] = __fadd_rn(acc[i], hs);
+                }
+            }
+        }
+        if (lane == 0) {
+            const double scale = type == BIAS_OPES ? (M > -INFINITY ? exp(M) : 0.0) : 1.0;
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+                red[warp * 9 + i] = ((double)acc[i] + (MODE == SUM_FP32C ? (double)cmp[i] : 0.0)) * scale;
+        }
+        __syncthreads();
+        if (tid < 9) {
+            double t = 0.0;
+            for (int w = 0; w < (nt >> 5); w++) t += red[w * 9 + tid];
+            part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 9 + tid] = t;
         }
     }
-    blockSum<9>(acc, red);
-    if (tid < 9) part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 9 + tid] = acc[tid];
 }
 
 __device__ __forceinline__ bool singleLaneBias(int t) {
@@ -458,8 +565,15 @@ __global__ void k_hills_deposit(const BiasDev* __restrict__ bp, const double* __
 
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums,
-                  bool singleLane) {
-    if (kernelSums && !testGrad && nb > 0) launchPdl(k_kernel_sums, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
+                  bool singleLane, int sumMode) {
+    if (kernelSums && !testGrad && nb > 0) {
+        if (sumMode == SUM_FP32)
+            launchPdl(k_kernel_sums<SUM_FP32>, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
+        else if (sumMode == SUM_FP32C)
+            launchPdl(k_kernel_sums<SUM_FP32C>, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
+        else
+            launchPdl(k_kernel_sums<SUM_FP64>, dim3(KSUM_CTAS, nb), dim3(256), 0, s, biases, cvv, sumPart);
+    }
     // sG (rounded to an even count, so what follows is 16-byte aligned), the
     // per-bias contributions, then the staged records when they fit in 48 KB
     static_assert(sizeof(BiasDev) % 8 == 0, "bias records are copied as 8-byte words");

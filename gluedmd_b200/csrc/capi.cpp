@@ -2,6 +2,7 @@
 // exceptions into a status code and keeps the message for glued_last_error().
 #include "../../include/glued_b200.h"
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -336,6 +337,24 @@ int glued_coordination_noalloc(void* stream, const void* posq, const int* group_
 int glued_context_opes_last_decision(glued_context* c, int idx, int* decision) {
     return guard([&] { need(c, "context"); need(decision, "out"); *decision = c->c->opesLastDecision(idx); });
 }
+int glued_context_coordination_pairs(glued_context* c, int cv_index, int* out, long long cap, long long* n) {
+    return guard([&] {
+        need(c, "context"); need(n, "out");
+        std::vector<int> v = c->c->cellPairs(cv_index);
+        *n = (long long)(v.size() / 2);
+        if (out && cap > 0) std::memcpy(out, v.data(), sizeof(int) * 2 * (size_t)std::min<long long>(cap, *n));
+    });
+}
+int glued_context_set_sum_precision(glued_context* c, int kernel_sums, int coordination) {
+    return guard([&] { need(c, "context"); c->c->setSumPrecision(kernel_sums, coordination); });
+}
+int glued_context_get_sum_precision(glued_context* c, int* kernel_sums, int* coordination) {
+    return guard([&] {
+        need(c, "context"); need(kernel_sums, "out"); need(coordination, "out");
+        *kernel_sums = c->c->sumMode();
+        *coordination = c->c->coordBlocked() ? 1 : 0;
+    });
+}
 
 // ------------------------------------------------------------------ batch
 int glued_batch_create(const glued_force* const* forces, int num_walkers, const glued_walker_desc* walkers,
@@ -360,7 +379,7 @@ int glued_batch_set_tuning(glued_batch* b, const int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t;
-        t.ra = tune[0]; t.parts = tune[1]; t.plain = tune[2];
+        t.ra = tune[0]; t.parts = tune[1]; t.plain = tune[2]; t.ch = tune[3] == 0 ? 128 : tune[3];
         b->b->setTuning(t);
     });
 }
@@ -368,14 +387,22 @@ int glued_batch_get_tuning(glued_batch* b, int tune[4]) {
     return guard([&] {
         need(b, "batch"); need(tune, "tune");
         glued::BatchTuning t = b->b->tuning();
-        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = 0;
+        tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = t.ch;
     });
 }
-int glued_batch_autotune(glued_batch* b, int tune[4]) {
+int glued_batch_set_sum_precision(glued_batch* b, int mode) {
+    return guard([&] { need(b, "batch"); b->b->setSumPrecision(mode); });
+}
+int glued_batch_get_sum_precision(glued_batch* b, int* mode) {
+    return guard([&] { need(b, "batch"); need(mode, "out"); *mode = b->b->sumPrecision(); });
+}
+int glued_batch_autotune(glued_batch* b, int tune[4]) { return glued_batch_autotune_ex(b, 1, tune, nullptr); }
+int glued_batch_autotune_ex(glued_batch* b, int use_cache, int tune[4], int* cached) {
     return guard([&] {
         need(b, "batch");
-        glued::BatchTuning t = b->b->autotune();
-        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = 0; }
+        glued::BatchTuning t = b->b->autotune(use_cache != 0);
+        if (tune) { tune[0] = t.ra; tune[1] = t.parts; tune[2] = t.plain; tune[3] = t.ch; }
+        if (cached) *cached = b->b->lastTuneCached() ? 1 : 0;
     });
 }
 int glued_batch_execute(glued_batch* b) {

@@ -3,6 +3,7 @@
 #include "context.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -111,6 +112,7 @@ Context::Context(const GluedForce& f, int numParticles, const double* masses)
     periodic_ = f.usesPBC;
     std::memset(lastBox_, 0, sizeof lastBox_);
     cudaCheck(cudaMallocHost(&boxPinned_, sizeof(BoxDev)), "cudaMallocHost");
+    cudaCheck(cudaMallocHost(&cellBoxPinned_, sizeof(CellBox)), "cudaMallocHost");
     cudaCheck(cudaMallocHost(&energiesPinned_, sizeof(double) * 64), "cudaMallocHost");
     cudaCheck(cudaStreamCreateWithFlags(&capStream_, cudaStreamNonBlocking), "cudaStreamCreate");
     box_.alloc(sizeof(BoxDev));
@@ -133,7 +135,18 @@ Context::~Context() {
     invalidateGraphs();
     if (capStream_) cudaStreamDestroy(capStream_);
     if (boxPinned_) cudaFreeHost(boxPinned_);
+    if (cellBoxPinned_) cudaFreeHost(cellBoxPinned_);
     if (energiesPinned_) cudaFreeHost(energiesPinned_);
+}
+
+void Context::setSumPrecision(int kernelSums, int coordBlocked) {
+    if (kernelSums != SUM_FP64 && kernelSums != SUM_FP32 && kernelSums != SUM_FP32C)
+        throw Error(GLUED_E_INVALID, "sum precision: kernel sums must be 0 (FP64), 1 (FP32) or 2 (FP32 two-sum)");
+    if (coordBlocked != 0 && coordBlocked != 1)
+        throw Error(GLUED_E_INVALID, "sum precision: coordination mode must be 0 (per tile run) or 1 (blocked)");
+    if (kernelSums != sumMode_ || (coordBlocked != 0) != coordBlocked_) invalidateGraphs();
+    sumMode_ = kernelSums;
+    coordBlocked_ = coordBlocked != 0;
 }
 
 void Context::invalidateGraphs() {
@@ -170,6 +183,11 @@ void Context::buildPlan(const GluedForce& f) {
                 case CV_GYRATION: needA(1); break;
                 case CV_COORDINATION: case CV_COORDINATION_CUTOFF:
                     needA(2); needP(c.type == CV_COORDINATION ? 3 : 4);
+                    if (c.type == CV_COORDINATION_CUTOFF && c.params.size() > 4 && c.params[4] != 0.0 &&
+                        c.params[4] != 1.0)
+                        err("coordination cutoff: pair search params[4] must be 0 (cell list) or 1 (all pairs)");
+                    if (c.type == CV_COORDINATION_CUTOFF && !(c.params[3] > 0.0))
+                        err("coordination cutoff: rc must be > 0");
                     if (c.atoms[0] < 1 || c.atoms[0] >= (int)c.atoms.size())
                         err("coordination group-A size atoms[0]=" + std::to_string(c.atoms[0]) + " invalid");
                     break;
@@ -228,6 +246,7 @@ void Context::buildPlan(const GluedForce& f) {
     std::vector<int2> cmPairs;
     std::vector<float4> cmParams;
     std::vector<CoordItem> coord;
+    std::vector<double> coordRc;   // cutoff of every coordination item (0: none), FP64
     std::vector<int> coordAtoms;
     // per-kind atom cursors into the shared group arrays (the reference keeps one
     // array per kind; the row offset of an atom inside its kind is what matters)
@@ -254,6 +273,10 @@ void Context::buildPlan(const GluedForce& f) {
             it.r0 = (float)c.params[0]; it.n = (float)c.params[1]; it.m = (float)c.params[2];
             double rc = (t == CV_COORDINATION_CUTOFF) ? c.params[3] : 0.0;
             it.rc2 = (float)(rc * rc);
+            // cutoff items: all-pairs tiles with the cutoff mask, or the cell list when
+            // params[4] = 1 (faster once the box spans many cutoffs)
+            it.cells = (t == CV_COORDINATION_CUTOFF && c.params.size() > 4 && c.params[4] == 1.0) ? 1 : 0;
+            coordRc.push_back(rc);
             it.kind = coordKind(it.n, it.m);
             for (int k = 0; k < it.nA + it.nB; k++) { jAtom[jac0 + k] = c.atoms[1 + k]; jCv[jac0 + k] = cv; }
             coord.push_back(it);
@@ -371,7 +394,7 @@ void Context::buildPlan(const GluedForce& f) {
             if (it.kind != coordKind_) coordKind_ = (coordKind_ == 0 || it.kind == 0) ? 0 : -1;
         if (coordKind_ != 3)
             for (auto& it : coord) it.kind = coordKind_;
-        coordRows_ = buildCoordSteps(coord, 8, coordStepsH_, 1 << 30);
+        coordRows_ = buildCoordSteps(coord, 8, COORD_CH, coordStepsH_, 1 << 30);
         coordItemsN_ = (int)coord.size();
         coordAtomsN_ = (int)coordAtoms.size();
         int dev = 0, sms = 0;
@@ -403,6 +426,51 @@ void Context::buildPlan(const GluedForce& f) {
         coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
         coordCnPiece_.alloc(sizeof(double) * std::max(1, pieces));
         cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
+        // cell-list items: scratch carved from one allocation, 256-byte aligned pieces
+        cellItemsH_.clear();
+        cellTotalA_ = 0;
+        size_t bytes = 0;
+        auto carve = [&](size_t n) { size_t o = bytes; bytes += (n + 255) / 256 * 256; return o; };
+        std::vector<std::array<size_t, 4>> offs;
+        // every cutoff item gets cell-list state (its pair list); those evaluated on
+        // the cell list come first (cellEvalN_ of them)
+        std::vector<size_t> order;
+        for (size_t i = 0; i < coord.size(); i++)
+            if (coord[i].cells) order.push_back(i);
+        cellEvalN_ = (int)order.size();
+        cellEvalA_ = 0;
+        for (size_t i = 0; i < coord.size(); i++)
+            if (!coord[i].cells && coordRc[i] > 0.0) order.push_back(i);
+        for (size_t i : order) {
+            const CoordItem& it = coord[i];
+            offs.push_back({carve(sizeof(int) * (CELL_MAX + 1)), carve(sizeof(int) * std::max(1, it.nB)),
+                            carve(sizeof(float4) * std::max(1, it.nB)), carve(sizeof(int) * 4)});
+            CellItemDev ci{};
+            ci.item = (int)i; ci.a0 = it.a0; ci.nA = it.nA; ci.b0 = it.b0; ci.nB = it.nB;
+            ci.row0 = it.row0; ci.pieceBegin = it.pieceBegin;
+            ci.r0 = it.r0; ci.n = it.n; ci.m = it.m;
+            ci.rc = coordRc[i];
+            ci.rc2 = coordRc[i] * coordRc[i];
+            cellItemsH_.push_back(ci);
+            cellTotalA_ += it.nA;
+            if (it.cells) cellEvalA_ += it.nA;
+        }
+        cellItemsN_ = (int)cellItemsH_.size();
+        if (cellItemsN_ > 0) {
+            cellScratch_.alloc(bytes);
+            char* base = static_cast<char*>(cellScratch_.p);
+            for (int k = 0; k < cellItemsN_; k++) {
+                cellItemsH_[k].cellStart = reinterpret_cast<int*>(base + offs[k][0]);
+                cellItemsH_[k].sortedB = reinterpret_cast<int*>(base + offs[k][1]);
+                cellItemsH_[k].sortedPos = reinterpret_cast<float4*>(base + offs[k][2]);
+                cellItemsH_[k].grid = reinterpret_cast<int*>(base + offs[k][3]);
+            }
+            cellItems_.upload(cellItemsH_);
+            CellBox cb{};
+            cb.kind = 0;
+            cellBox_.alloc(sizeof(CellBox));
+            cudaCheck(cudaMemcpy(cellBox_.p, &cb, sizeof(CellBox), cudaMemcpyHostToDevice), "cell box");
+        }
         R_.items = coordItems_.as<CoordItem>();
         R_.steps = coordSteps_.as<CoordStep>();
         R_.numSteps = (int)nSteps;
@@ -460,7 +528,10 @@ void Context::setupBiases(const GluedForce& f) {
             // CommonBiasKernels.cpp:206-257
             needP(3 + 3 * D); needI(1 + 2 * D);
             d.h0 = p[0];
-            for (int k = 0; k < D; k++) d.sigma[k] = p[1 + k];
+            for (int k = 0; k < D; k++) {
+                d.sigma[k] = p[1 + k];
+                d.isg2f[k] = (float)(1.0 / (p[1 + k] * p[1 + k]));
+            }
             double gamma = p[1 + D], kT = p[2 + D];
             d.gamma = gamma; d.kT = kT;
             d.pace = ip[0];
@@ -539,7 +610,10 @@ void Context::setupBiases(const GluedForce& f) {
         } else if (d.type == BIAS_METAD_HILLS) {
             needP(3 + 3 * D); needI(2 + D);
             d.h0 = p[0];
-            for (int k = 0; k < D; k++) d.sigma[k] = p[1 + k];
+            for (int k = 0; k < D; k++) {
+                d.sigma[k] = p[1 + k];
+                d.isg2f[k] = (float)(1.0 / (p[1 + k] * p[1 + k]));
+            }
             double gamma = p[1 + D], kT = p[2 + D];
             d.gamma = gamma; d.kT = kT;
             d.pace = ip[0];
@@ -693,6 +767,20 @@ void Context::setBox(const double box[9]) {
     } else {
         cudaCheck(cudaMemcpy(box_.p, &b, sizeof(BoxDev), cudaMemcpyHostToDevice), "box");
     }
+    if (cellItemsN_ > 0) {
+        // FP64 box of the cell-list decisions (the oracle's: 1 / diagonal in FP64)
+        CellBox cb{};
+        for (int i = 0; i < 3; i++) { cb.a[i] = box[i]; cb.b[i] = box[3 + i]; cb.c[i] = box[6 + i]; }
+        cb.inv[0] = 1.0 / box[0]; cb.inv[1] = 1.0 / box[4]; cb.inv[2] = 1.0 / box[8];
+        cb.kind = b.kind;
+        if (bound_) {
+            *cellBoxPinned_ = cb;
+            cudaCheck(cudaMemcpyAsync(cellBox_.p, cellBoxPinned_, sizeof(CellBox), cudaMemcpyHostToDevice, stream_),
+                      "cell box");
+        } else {
+            cudaCheck(cudaMemcpy(cellBox_.p, &cb, sizeof(CellBox), cudaMemcpyHostToDevice), "cell box");
+        }
+    }
 }
 
 // ---------------------------------------------------------------- execute
@@ -710,22 +798,76 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
         // coordination pairs, the CV kernels that fit beside them, then the finalize
         if (!simpleBeside_) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, false);
         if (!groupBeside_) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, false);
-        launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 1);
+        launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 1,
+                    coordBlocked_);
         if (simpleBeside_) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, true);
         if (groupBeside_) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, true);
-        launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 2);
+        enqueueCells(s);
+        launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 2,
+                    coordBlocked_);
     } else {
         if (want(0)) launchSimpleCVs(s, posq_, u2g, simple_.as<SimpleItem>(), numSimple_, box, cvv, J_, false);
         if (want(1)) launchGroupCVs(s, posq_, u2g, G_, box, cvv, J_, groupCached_, groupClustered_, false);
-        if (want(2) || want(3))
-            launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv,
-                        onlyPhase < 0 ? 3 : (onlyPhase == 2 ? 1 : 2));
+        if (want(2))
+            launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 1,
+                        coordBlocked_);
+        if (want(2)) enqueueCells(s);
+        if (want(3))
+            launchCoord(s, R_, coordItemsN_, coordGrid_, coordRows_, boxHost_.kind, coordKind_, coordHi_, J_, cvv, 2,
+                        coordBlocked_);
     }
     if (want(4))
         launchBiases(s, biasDev_.as<BiasDev>(), (int)biases_.size(), cvv, numCVs_,
                      testGrad_.p ? testGrad_.as<double>() : nullptr, dudcv_.as<double>(), energies_.as<double>(),
-                     sumPart_.as<double>(), kernelSums_, singleLane_);
+                     sumPart_.as<double>(), kernelSums_, singleLane_, sumMode_);
     if (includeForces && want(5)) launchScatter(s, J_, u2g, dudcv_.as<double>(), force_buf_, padded_);
+}
+
+void Context::enqueueCells(cudaStream_t s) {
+    launchCellCoord(s, cellItems_.as<CellItemDev>(), cellEvalN_, cellEvalA_, coordKind_, coordSlots_.as<int>(),
+                    static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), coordAcc_.as<unsigned long long>(),
+                    coordCnPiece_.as<double>());
+}
+
+std::vector<int> Context::cellPairs(int cvIndex) {
+    requireBound();
+    int k = -1;
+    for (int i = 0; i < cellItemsN_; i++)
+        if (coordItemsH_[cellItemsH_[i].item].cv == cvIndex) k = i;
+    if (k < 0) throw Error(GLUED_E_INVALID, "cell pairs: CV " + std::to_string(cvIndex) +
+                                                " is not a cutoff coordination");
+    const int nA = cellItemsH_[k].nA;
+    int a0 = 0;
+    for (int i = 0; i < k; i++) a0 += cellItemsH_[i].nA;
+    // one count / offset per warp: CELL_SPLIT warps per A atom
+    const int nw = CELL_SPLIT * cellTotalA_;
+    DBuf cnt, off, pairs;
+    cnt.alloc(sizeof(int) * std::max(1, nw));
+    off.alloc(sizeof(long long) * std::max(1, nw));
+    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, coordKind_,
+                       coordSlots_.as<int>(), static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), cnt.as<int>(),
+                       nullptr, nullptr, 1);
+    std::vector<int> c(nw);
+    cudaCheck(cudaMemcpyAsync(c.data(), cnt.p, sizeof(int) * c.size(), cudaMemcpyDeviceToHost, stream_), "pairs");
+    cudaCheck(cudaStreamSynchronize(stream_), "pairs");
+    std::vector<long long> o(nw + 1, 0);
+    for (int i = 0; i < nw; i++) o[i + 1] = o[i] + c[i];
+    cudaCheck(cudaMemcpy(off.p, o.data(), sizeof(long long) * nw, cudaMemcpyHostToDevice), "pairs");
+    pairs.alloc(sizeof(int) * 2 * std::max<long long>(1, o[nw]));
+    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, coordKind_,
+                       coordSlots_.as<int>(), static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), nullptr,
+                       off.as<long long>(), pairs.as<int>(), 2);
+    const long long p0 = o[CELL_SPLIT * a0], p1 = o[CELL_SPLIT * (a0 + nA)];
+    std::vector<int> out(2 * (p1 - p0));
+    if (p1 > p0)
+        cudaCheck(cudaMemcpyAsync(out.data(), pairs.as<int>() + 2 * p0, sizeof(int) * out.size(),
+                                  cudaMemcpyDeviceToHost, stream_), "pairs");
+    cudaCheck(cudaStreamSynchronize(stream_), "pairs");
+    std::vector<std::pair<int, int>> v(p1 - p0);
+    for (size_t i = 0; i < v.size(); i++) v[i] = {out[2 * i], out[2 * i + 1]};
+    std::sort(v.begin(), v.end());
+    for (size_t i = 0; i < v.size(); i++) { out[2 * i] = v[i].first; out[2 * i + 1] = v[i].second; }
+    return out;
 }
 
 int Context::kernelsPerExecute(bool includeForces) const {
@@ -733,7 +875,7 @@ int Context::kernelsPerExecute(bool includeForces) const {
     if (kernelSums_ && !testGrad_.p && !biases_.empty()) k++;
     if (numSimple_ > 0) k++;
     if (G_.numItems > 0) k++;
-    if (coordItemsN_ > 0) k += 2;
+    if (coordItemsN_ > 0) k += (coordStepsH_.empty() ? 1 : 2) + (cellEvalN_ > 0 ? 2 : 0);
     if (includeForces && numRows_ > 0) k++;
     return k;
 }

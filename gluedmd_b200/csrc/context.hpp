@@ -77,6 +77,14 @@ public:
     int opesLastDecision(int opesIndex);
     std::vector<double> profilePhases(int reps);
     long long launchCount() const { return launches_; }
+    // Sum precision: kernelSums = SumMode of the OPES / hill kernel sums;
+    // coordBlocked = coordination A-side partials flushed every crun::BLK_STEPS steps.
+    void setSumPrecision(int kernelSums, int coordBlocked);
+    // Pair list of a cutoff coordination CV on the cell-list path (cvIndex = its
+    // CV value index): (a, b) group indices, sorted (synchronizing).
+    std::vector<int> cellPairs(int cvIndex);
+    int sumMode() const { return sumMode_; }
+    bool coordBlocked() const { return coordBlocked_; }
 
     int numCVs() const { return numCVs_; }
     int numRows() const { return numRows_; }
@@ -88,6 +96,7 @@ private:
     void buildPlan(const GluedForce& f);
     void setupBiases(const GluedForce& f);
     void enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase = -1);
+    void enqueueCells(cudaStream_t s);
     int kernelsPerExecute(bool includeForces) const;
     void invalidateGraphs();
     void syncUploadBias(HostBias& hb);
@@ -132,6 +141,14 @@ private:
     CoordRunDev R_{};
     int coordItemsN_ = 0, coordRows_ = 0, coordGrid_ = 0, coordKind_ = 3, coordAtomsN_ = 0;
     bool coordHi_ = true;
+    // cutoff coordination items on the cell-list path (coord_cells.cu)
+    DBuf cellItems_, cellBox_, cellScratch_;
+    std::vector<CellItemDev> cellItemsH_;
+    int cellItemsN_ = 0, cellTotalA_ = 0;   // every cutoff item
+    int cellEvalN_ = 0, cellEvalA_ = 0;     // the first cellEvalN_: evaluated on the cell list
+    CellBox* cellBoxPinned_ = nullptr;
+    int sumMode_ = SUM_FP64;        // OPES / hill kernel sums (SumMode)
+    bool coordBlocked_ = false;     // coordination A sums flushed every crun::BLK_STEPS steps
     int nUprobPartial_ = 296;
 
     std::vector<HostBias> biases_;       // addBias order

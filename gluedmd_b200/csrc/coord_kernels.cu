@@ -37,13 +37,13 @@ namespace glued {
 // One CTA of COORD_NW warps per SM: its warps meet at a barrier every step, so
 // none of them runs ahead; buffers in dynamic shared memory (above the 48 KB
 // static limit).
-template <int RA, int BOX, int NH, bool HI>
+template <int RA, int BOX, int NH, bool HI, bool BLK>
 __global__ void __launch_bounds__(COORD_NW * 32, 1) k_coord_run(CoordRunDev R) {
     pdlEnter();
     extern __shared__ __align__(16) unsigned char dsm[];
-    CoordRunSmem<RA>& sm = *reinterpret_cast<CoordRunSmem<RA>*>(dsm);
+    CoordRunSmem<RA, COORD_CH / 32>& sm = *reinterpret_cast<CoordRunSmem<RA, COORD_CH / 32>*>(dsm);
     const int s0 = coordRange(R.numSteps, gridDim.x, blockIdx.x), s1 = coordRange(R.numSteps, gridDim.x, blockIdx.x + 1);
-    if (s0 < s1) coordRun<RA, BOX, NH, HI>(R, s0, s1, sm, NoPieceHook());
+    if (s0 < s1) coordRun<RA, COORD_CH / 32, BOX, NH, HI, BLK>(R, s0, s1, sm, NoPieceHook());
 }
 
 // Fixed-point sums -> float Jacobian rows (one thread per row and component),
@@ -99,25 +99,29 @@ void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* s
 // chunk / tile); rebuilt whenever the rows change. A step gathers its tile's A
 // atoms when it starts a tile run: the tile's first chunk, or the first step of
 // a CTA's range in a grid of `grid` CTAs.
-static_assert(COORD_TA == COORD_CH, "one thread per B chunk lane and A tile lane");
 __global__ void k_step_gathers(const CoordStep* __restrict__ steps, int numSteps, int grid,
-                               const int* __restrict__ slots, int* __restrict__ gB, int* __restrict__ gA) {
+                               const int* __restrict__ slots, int* __restrict__ gB, int* __restrict__ gA, int ta,
+                               int ch) {
+    // one thread per (step, lane), lane < max(ta, ch)
+    const int w = ta > ch ? ta : ch;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)numSteps * COORD_CH) return;
-    const int s = (int)(i / COORD_CH), t = (int)(i % COORD_CH);
+    if (i >= (long long)numSteps * w) return;
+    const int s = (int)(i / w), t = (int)(i % w);
     const CoordStep d = steps[s];
-    const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
-    gB[i] = t < nBv ? slots[d.bStart + t] : -1;
-    // smallest CTA whose range could start at s
-    const long long b = ((long long)s * grid + numSteps - 1) / numSteps;
-    const bool rangeStart = b < grid && coordRange(numSteps, grid, (int)b) == s;
-    gA[i] = ((fl & COORD_F_FIRST) || rangeStart) ? (t < nAv ? slots[d.aStart + t] : -2) : -1;
+    const int nAv = stepNA(d.packed), nBv = stepNB(d.packed), fl = stepFlags(d.packed);
+    if (t < ch) gB[(size_t)s * ch + t] = t < nBv ? slots[d.bStart + t] : -1;
+    if (t < ta) {
+        // smallest CTA whose range could start at s
+        const long long b = ((long long)s * grid + numSteps - 1) / numSteps;
+        const bool rangeStart = b < grid && coordRange(numSteps, grid, (int)b) == s;
+        gA[(size_t)s * ta + t] = ((fl & COORD_F_FIRST) || rangeStart) ? (t < nAv ? slots[d.aStart + t] : -2) : -1;
+    }
 }
 
 void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
-                       int* gA) {
-    const long long n = (long long)numSteps * COORD_CH;
-    if (n > 0) k_step_gathers<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(steps, numSteps, grid, slots, gB, gA);
+                       int* gA, int ta, int ch) {
+    const long long n = (long long)numSteps * (ta > ch ? ta : ch);
+    if (n > 0) k_step_gathers<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(steps, numSteps, grid, slots, gB, gA, ta, ch);
 }
 
 void runKernelSetup(const void* fn, size_t dynSmem) {
@@ -132,33 +136,39 @@ void runKernelSetup(const void* fn, size_t dynSmem) {
     cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynSmem), "smem");
 }
 
-template <int RA, int BOX, int NH, bool HI>
+template <int RA, int BOX, int NH, bool HI, bool BLK>
 static void launchRun(cudaStream_t s, int grid, const CoordRunDev& R) {
-    const size_t dyn = sizeof(CoordRunSmem<RA>);
-    runKernelSetup((const void*)k_coord_run<RA, BOX, NH, HI>, dyn);
+    const size_t dyn = sizeof(CoordRunSmem<RA, COORD_CH / 32>);
+    runKernelSetup((const void*)k_coord_run<RA, BOX, NH, HI, BLK>, dyn);
     // plain launch: the persistent grid fills every SM, nothing to overlap
-    k_coord_run<RA, BOX, NH, HI><<<grid, COORD_NW * 32, dyn, s>>>(R);
+    k_coord_run<RA, BOX, NH, HI, BLK><<<grid, COORD_NW * 32, dyn, s>>>(R);
 }
 
-template <int BOX>
+template <int BOX, bool BLK>
 static void launchRunB(cudaStream_t s, int grid, int kind, bool hi, const CoordRunDev& R) {
     if (kind == 3) {
-        if (hi) launchRun<8, BOX, 3, true>(s, grid, R);
-        else launchRun<8, BOX, 3, false>(s, grid, R);
+        if (hi) launchRun<8, BOX, 3, true, BLK>(s, grid, R);
+        else launchRun<8, BOX, 3, false, BLK>(s, grid, R);
     } else if (kind == -1) {
-        launchRun<8, BOX, -1, true>(s, grid, R);
+        launchRun<8, BOX, -1, true, BLK>(s, grid, R);
     } else {
-        launchRun<8, BOX, 0, true>(s, grid, R);
+        launchRun<8, BOX, 0, true, BLK>(s, grid, R);
     }
 }
 
+template <bool BLK>
+static void launchRunK(cudaStream_t s, int grid, int boxKind, int kind, bool hi, const CoordRunDev& R) {
+    if (boxKind == 0) launchRunB<0, BLK>(s, grid, kind, true, R);
+    else if (boxKind == 1) launchRunB<1, BLK>(s, grid, kind, hi, R);
+    else launchRunB<2, BLK>(s, grid, kind, hi, R);
+}
+
 void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, int totalRows, int boxKind, int kind,
-                 bool hi, const JacDev& J, double* cvv, int parts) {
+                 bool hi, const JacDev& J, double* cvv, int parts, bool blocked) {
     if (numItems == 0) return;
-    if (parts & 1) {
-        if (boxKind == 0) launchRunB<0>(s, grid, kind, true, R);
-        else if (boxKind == 1) launchRunB<1>(s, grid, kind, hi, R);
-        else launchRunB<2>(s, grid, kind, hi, R);
+    if ((parts & 1) && R.numSteps > 0) {
+        if (blocked) launchRunK<true>(s, grid, boxKind, kind, hi, R);
+        else launchRunK<false>(s, grid, boxKind, kind, hi, R);
     }
     if (parts & 2) {
         const int n = std::max(3 * totalRows, numItems);
@@ -169,17 +179,17 @@ void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, i
 int coordRunOccupancy(int kind, int boxKind, bool hi) {
     const void* fn;
     if (kind == 3) {
-        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 3, true>
-             : boxKind == 1 ? (hi ? (const void*)k_coord_run<8, 1, 3, true> : (const void*)k_coord_run<8, 1, 3, false>)
-                            : (hi ? (const void*)k_coord_run<8, 2, 3, true> : (const void*)k_coord_run<8, 2, 3, false>);
+        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 3, true, false>
+             : boxKind == 1 ? (hi ? (const void*)k_coord_run<8, 1, 3, true, false> : (const void*)k_coord_run<8, 1, 3, false, false>)
+                            : (hi ? (const void*)k_coord_run<8, 2, 3, true, false> : (const void*)k_coord_run<8, 2, 3, false, false>);
     } else if (kind == -1) {
-        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, -1, true>
-             : boxKind == 1 ? (const void*)k_coord_run<8, 1, -1, true> : (const void*)k_coord_run<8, 2, -1, true>;
+        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, -1, true, false>
+             : boxKind == 1 ? (const void*)k_coord_run<8, 1, -1, true, false> : (const void*)k_coord_run<8, 2, -1, true, false>;
     } else {
-        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 0, true>
-             : boxKind == 1 ? (const void*)k_coord_run<8, 1, 0, true> : (const void*)k_coord_run<8, 2, 0, true>;
+        fn = boxKind == 0 ? (const void*)k_coord_run<8, 0, 0, true, false>
+             : boxKind == 1 ? (const void*)k_coord_run<8, 1, 0, true, false> : (const void*)k_coord_run<8, 2, 0, true, false>;
     }
-    const size_t dyn = sizeof(CoordRunSmem<8>);
+    const size_t dyn = sizeof(CoordRunSmem<8, COORD_CH / 32>);
     runKernelSetup(fn, dyn);
     int perSM = 0;
     cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, COORD_NW * 32, dyn), "occupancy");

@@ -8,27 +8,32 @@
 
 namespace glued {
 
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps, int itemsPerSys) {
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, int ch, std::vector<CoordStep>& steps, int itemsPerSys) {
     const int TA = COORD_NW * ra;
     steps.clear();
     int rows = 0;
     for (size_t i = 0; i < items.size(); i++) {
         CoordItem& it = items[i];
         it.row0 = rows;
+        if (it.cells) {
+            it.tilesA = 0;
+            rows += it.nA + it.nB;
+            continue;
+        }
         it.tilesA = std::max(1, (it.nA + TA - 1) / TA);
-        const int nCh = std::max(1, (it.nB + COORD_CH - 1) / COORD_CH);
+        const int nCh = std::max(1, (it.nB + ch - 1) / ch);
         for (int ta = 0; ta < it.tilesA; ta++) {
             const int nAv = std::min(TA, it.nA - ta * TA);
             for (int c = 0; c < nCh; c++) {
                 CoordStep s{};
                 s.item = (int)i;
                 s.aStart = it.a0 + ta * TA;
-                s.bStart = it.b0 + c * COORD_CH;
+                s.bStart = it.b0 + c * ch;
                 s.rowA = rows + ta * TA;
-                s.rowB = rows + it.nA + c * COORD_CH;
-                const int nBv = std::min(COORD_CH, it.nB - c * COORD_CH);
+                s.rowB = rows + it.nA + c * ch;
+                const int nBv = std::min(ch, it.nB - c * ch);
                 int fl = (c == 0 ? COORD_F_FIRST : 0) | (c == nCh - 1 ? COORD_F_LAST : 0);
-                s.packed = nAv | (nBv << 8) | (fl << 16);
+                s.packed = stepPack(nAv, nBv, fl);
                 s.pieceSlot = -1;
                 s.sys = (int)i / std::max(1, itemsPerSys);
                 steps.push_back(s);
@@ -50,7 +55,7 @@ int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begi
     std::vector<std::vector<int>> per(items.size());
     for (size_t b = 0; b + 1 < begin.size(); b++)
         for (int s = begin[b]; s < begin[b + 1]; s++) {
-            const int fl = steps[s].packed >> 16;
+            const int fl = stepFlags(steps[s].packed);
             steps[s].pieceSlot = -1;
             if (s == begin[b + 1] - 1 || (fl & COORD_F_LAST)) per[steps[s].item].push_back(s);
         }
@@ -58,6 +63,7 @@ int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begi
     for (size_t i = 0; i < items.size(); i++) {
         std::sort(per[i].begin(), per[i].end());
         items[i].pieceBegin = slot;
+        if (items[i].cells) slot += CELL_SPLIT * items[i].nA;   // partials of the A atoms' stencil slices
         for (int s : per[i]) steps[s].pieceSlot = slot++;
         items[i].pieceEnd = slot;
     }

@@ -1,8 +1,10 @@
 // Coordination pairs as static per-CTA runs of (item, A tile, B chunk) steps.
 //
 // Work decomposition. Every coordination item (one CV of one system) is cut into
-// A tiles of TA = NW*RA atoms (NW = 16 warps, RA = 8: 128 atoms) and B chunks of
-// CH = 128 atoms; one step is one (tile, chunk) block of TA x CH pairs. The host
+// A tiles of TA = NW*RA atoms (NW = 16 warps, RA A atoms per warp: 8 by default,
+// 128 atoms) and B chunks of CH = 32*RB atoms (RB B atoms per lane: 4 by
+// default, 128 atoms); one step is one (tile, chunk) block of TA x CH pairs. The
+// batched path instantiates other (RA, RB) shapes for its autotuner. The host
 // lists the steps tile-major (CoordStep) and gives every CTA of a persistent grid
 // of one 512-thread CTA per SM one contiguous range of them with the same number
 // of steps. One CTA per SM, its warps meeting at a barrier every step, keeps
@@ -28,7 +30,12 @@
 //
 // Accumulation. Per-pair gradients h*d (scaled units) are summed in FP32 over a
 // step: per lane over its A atoms for B, per warp over lanes for A (one butterfly
-// for all A atoms of the warp). Those sums are converted to 64-bit fixed point
+// for all A atoms of the warp). The A sums run in registers over the whole tile
+// run (its steps = the B group in chunks of CH) and are reduced once at its end;
+// with BLK (blocked sums) they are reduced and flushed every BLK_STEPS steps
+// instead, so that no FP32 partial holds more than 4 * BLK_STEPS pairs per lane
+// (a register-resident two-sum would need 48 more registers per thread, and the
+// kernel is at the 128 of one 512-thread CTA per SM). Those sums are converted to 64-bit fixed point
 // (value * 2^32) and added with integer atomics into acc[row][3] (integer
 // addition is exact and order-independent, so the sums are bitwise reproducible
 // and do not depend on the grid); the reader multiplies by the item's scale
@@ -46,10 +53,8 @@ namespace glued {
 
 namespace crun {
 constexpr int NW = COORD_NW;   // warps per CTA
-constexpr int RB = 4;          // B atoms per lane per step
-constexpr int CH = 32 * RB;    // B atoms per chunk
-static_assert(CH == COORD_CH, "chunk size");
 constexpr int WIN = 64;        // step descriptors per shared-memory window
+constexpr int BLK_STEPS = 8;   // steps per A partial with blocked sums
 constexpr float FX = 4294967296.0f;   // 2^32
 constexpr double FXD = 4294967296.0;
 constexpr double IFXD = 1.0 / 4294967296.0;
@@ -65,11 +70,12 @@ struct RunConst {
     BoxDev box;         // scaled: a, b, c divided by r0; inv multiplied by r0
 };
 
-template <int RA>
+// Shared memory of a run with A tiles of NW * RA atoms and B chunks of 32 * RB.
+template <int RA, int RB>
 struct CoordRunSmem {
-    float4 pos[2][crun::CH];
+    float4 pos[2][32 * RB];
     float4 apos[2][crun::NW * RA];
-    float g[2][crun::NW][crun::CH * 3];
+    float g[2][crun::NW][32 * RB * 3];
     CoordStep st[crun::WIN];
     RunConst kst[crun::WIN];   // constants of the window's steps that start a tile run
     double red[2][crun::NW];
@@ -236,7 +242,7 @@ __device__ __forceinline__ PackedConst packedConst(const RunConst& K) {
 // bounds as the scalar loop; B-gradient and CN sums are kept as two partials
 // (even / odd A atoms) and added at the end of the step. Writes the warp's B
 // partials to gw (negated sums) and adds the step's CN to cnc.
-template <int RA, int BOX, int NH, bool HI>
+template <int RA, int RB, int BOX, int NH, bool HI>
 __device__ __forceinline__ void pairsPacked(const unsigned long long (&apx)[RA / 2],
                                             const unsigned long long (&apy)[RA / 2],
                                             const unsigned long long (&apz)[RA / 2], unsigned long long (&gpx)[RA / 2],
@@ -250,7 +256,7 @@ __device__ __forceinline__ void pairsPacked(const unsigned long long (&apx)[RA /
     const float INF = __int_as_float(0x7f800000);
     unsigned long long cn2 = 0ull;
 #pragma unroll
-    for (int half = 0; half < crun::RB / 2; half++) {
+    for (int half = 0; half < RB / 2; half++) {
         unsigned long long nbx[2], nby[2], nbz[2], gbx[2], gby[2], gbz[2];
 #pragma unroll
         for (int jj = 0; jj < 2; jj++) {
@@ -320,12 +326,16 @@ struct NoStartHook {
 // complete after its end-of-step wait. AfterFirst() is called once by all
 // threads right after the first step's end-of-step barrier (everything Start()
 // issued has landed and is visible).
-template <int RA, int BOX, int NH, bool HI, class Hook, class Start = NoStartHook, class AfterFirst = NoStartHook>
-__device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>& sm, const Hook& hook,
+template <int RA, int RB, int BOX, int NH, bool HI, bool BLK, class Hook, class Start = NoStartHook,
+          class AfterFirst = NoStartHook>
+__device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA, RB>& sm, const Hook& hook,
                          const Start& start = Start(), const AfterFirst& afterFirst = AfterFirst()) {
     using namespace crun;
     static_assert(RA % 2 == 0 && 3 * RA <= 32, "A atoms per warp");
+    static_assert(RB % 2 == 0 && RB >= 2, "B atoms per lane");
     constexpr int TA = NW * RA;
+    constexpr int CH = 32 * RB;
+    static_assert(TA <= COORD_TA_MAX && CH <= COORD_CH_MAX, "step packing");
     constexpr int RH = RA / 2;
     const int tid = threadIdx.x, lane = tid & 31, ty = tid >> 5;
     // A atoms 2i, 2i+1 of the warp (scaled) and their gradient sums, packed
@@ -333,7 +343,6 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
     RunConst K;
     double cn = 0.0;
     int pieceSteps = 0;
-    static_assert(TA == COORD_TA, "gather tables are laid out for 128-atom A tiles");
     for (int w0 = s0; w0 < s1; w0 += WIN) {
         const int w1 = min(s1, w0 + WIN);
         const int nw = w1 - w0;
@@ -371,7 +380,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
         __syncthreads();
         for (int i = tid; i < nw; i += blockDim.x) {
             const CoordStep& d = sm.st[i];
-            if (w0 + i == s0 || i == 0 || ((d.packed >> 16) & F_FIRST))
+            if (w0 + i == s0 || i == 0 || (stepFlags(d.packed) & F_FIRST))
                 sm.kst[i] = runConst(R.items[d.item], R.sysBox[d.sys]);
         }
         cpAsyncWaitAll();
@@ -381,7 +390,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             const int s = w0 + ls;
             const int b = (s - s0) & 1;
             const CoordStep d = sm.st[ls];
-            const int nAv = d.packed & 0xff, nBv = (d.packed >> 8) & 0xff, fl = d.packed >> 16;
+            const int nAv = stepNA(d.packed), nBv = stepNB(d.packed), fl = stepFlags(d.packed);
             const bool first = (s == s0) || (fl & F_FIRST);
             const bool last = (s == s1 - 1) || (fl & F_LAST);
             int ib2 = -1, ia2 = -1;
@@ -407,7 +416,7 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
             bool packed = false;
             if constexpr (NH > 0 && BOX != 2) {
                 if (full) {
-                    pairsPacked<RA, BOX, NH, HI>(apx, apy, apz, gpx, gpy, gpz, sm.pos[b], K, gw, cnc);
+                    pairsPacked<RA, RB, BOX, NH, HI>(apx, apy, apz, gpx, gpy, gpz, sm.pos[b], K, gw, cnc);
                     packed = true;
                 }
             }
@@ -416,44 +425,50 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                 // kinds). B is scaled exactly as A, so that an atom present in
                 // both groups gives a difference of exactly zero (excluded by the
                 // lower bound); the products are rounded, never contracted.
-                float bx[RB], by[RB], bz[RB], gbx[RB], gby[RB], gbz[RB];
+                // B atoms in blocks of (at most) 4 per lane
+                constexpr int QB = RB < 4 ? RB : 4;
 #pragma unroll
-                for (int j = 0; j < RB; j++) {
-                    const float4 p = sm.pos[b][lane + 32 * j];
-                    bx[j] = __fmul_rn(p.x, K.ir0); by[j] = __fmul_rn(p.y, K.ir0); bz[j] = __fmul_rn(p.z, K.ir0);
-                    gbx[j] = gby[j] = gbz[j] = 0.0f;
-                }
+                for (int jb = 0; jb < RB; jb += QB) {
+                    float bx[QB], by[QB], bz[QB], gbx[QB], gby[QB], gbz[QB];
 #pragma unroll
-                for (int i = 0; i < RH; i++) {
-                    float ax[2], ay[2], az[2], gx[2], gy[2], gz[2];
-                    f2::upk(apx[i], ax[0], ax[1]); f2::upk(apy[i], ay[0], ay[1]); f2::upk(apz[i], az[0], az[1]);
-                    f2::upk(gpx[i], gx[0], gx[1]); f2::upk(gpy[i], gy[0], gy[1]); f2::upk(gpz[i], gz[0], gz[1]);
-#pragma unroll
-                    for (int e = 0; e < 2; e++) {
-                        const bool av = (ty + NW * (2 * i + e)) < nAv;
-#pragma unroll
-                        for (int j = 0; j < RB; j++) {
-                            const bool bv = (lane + 32 * j) < nBv;
-                            float dx = ax[e] - bx[j], dy = ay[e] - by[j], dz = az[e] - bz[j];
-                            imageS<BOX>(dx, dy, dz, K.box);
-                            const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                            float f, h;
-                            switchX2<NH>(x2, av && bv && x2 >= K.lo && x2 < K.hi, K, f, h);
-                            cnc += f;
-                            gx[e] = fmaf(h, dx, gx[e]); gy[e] = fmaf(h, dy, gy[e]); gz[e] = fmaf(h, dz, gz[e]);
-                            gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]); gbz[j] = fmaf(-h, dz, gbz[j]);
-                        }
+                    for (int j = 0; j < QB; j++) {
+                        const float4 p = sm.pos[b][lane + 32 * (jb + j)];
+                        bx[j] = __fmul_rn(p.x, K.ir0); by[j] = __fmul_rn(p.y, K.ir0); bz[j] = __fmul_rn(p.z, K.ir0);
+                        gbx[j] = gby[j] = gbz[j] = 0.0f;
                     }
-                    gpx[i] = f2::pk(gx[0], gx[1]); gpy[i] = f2::pk(gy[0], gy[1]); gpz[i] = f2::pk(gz[0], gz[1]);
-                }
 #pragma unroll
-                for (int j = 0; j < RB; j++) {
-                    const int o = (lane + 32 * j) * 3;
-                    gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
+                    for (int i = 0; i < RH; i++) {
+                        float ax[2], ay[2], az[2], gx[2], gy[2], gz[2];
+                        f2::upk(apx[i], ax[0], ax[1]); f2::upk(apy[i], ay[0], ay[1]); f2::upk(apz[i], az[0], az[1]);
+                        f2::upk(gpx[i], gx[0], gx[1]); f2::upk(gpy[i], gy[0], gy[1]); f2::upk(gpz[i], gz[0], gz[1]);
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const bool av = (ty + NW * (2 * i + e)) < nAv;
+#pragma unroll
+                            for (int j = 0; j < QB; j++) {
+                                const bool bv = (lane + 32 * (jb + j)) < nBv;
+                                float dx = ax[e] - bx[j], dy = ay[e] - by[j], dz = az[e] - bz[j];
+                                imageS<BOX>(dx, dy, dz, K.box);
+                                const float x2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                                float f, h;
+                                switchX2<NH>(x2, av && bv && x2 >= K.lo && x2 < K.hi, K, f, h);
+                                cnc += f;
+                                gx[e] = fmaf(h, dx, gx[e]); gy[e] = fmaf(h, dy, gy[e]); gz[e] = fmaf(h, dz, gz[e]);
+                                gbx[j] = fmaf(-h, dx, gbx[j]); gby[j] = fmaf(-h, dy, gby[j]);
+                                gbz[j] = fmaf(-h, dz, gbz[j]);
+                            }
+                        }
+                        gpx[i] = f2::pk(gx[0], gx[1]); gpy[i] = f2::pk(gy[0], gy[1]); gpz[i] = f2::pk(gz[0], gz[1]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < QB; j++) {
+                        const int o = (lane + 32 * (jb + j)) * 3;
+                        gw[o] = gbx[j]; gw[o + 1] = gby[j]; gw[o + 2] = gbz[j];
+                    }
                 }
             }
             cn += (double)cnc;
-            if (last) {
+            if (last || (BLK && pieceSteps % BLK_STEPS == 0)) {
                 // A sums over lanes: slot 3k + c = component c of A atom k, one
                 // butterfly for all slots; lane 3k + c adds its slot
                 float v[32];
@@ -469,6 +484,12 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA>&
                 const int k = lane / 3, c = lane - 3 * k;
                 const int i = ty + NW * k;
                 if (lane < 3 * RA && i < nAv) redAddI64(R.acc + 3 * (size_t)(d.rowA + i) + c, __float2ll_rn(t * FX));
+                if (BLK && !last) {
+#pragma unroll
+                    for (int q = 0; q < RH; q++) gpx[q] = gpy[q] = gpz[q] = 0ull;
+                }
+            }
+            if (last) {
                 const double cs = warpSum(cn);
                 if (lane == 0) sm.red[b][ty] = cs;
             }

@@ -117,22 +117,51 @@ __global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restr
 // ---------------------------------------------------------------- group CVs
 
 // Jacobi eigen-decomposition of a symmetric 4x4 in FP64 (quaternion RMSD).
-__device__ void jacobi4(double A[4][4], double V[4][4], double w[4]) {
-    for (int i = 0; i < 4; i++) for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
+// Cyclic Jacobi on a symmetric 4x4 (FP64). Every index is a compile-time
+// constant (unrolled p, q, k loops), so A and V stay in registers; with runtime
+// indices they lived in local memory and the eigensolve of one Kabsch CV took
+// tens of microseconds.
+__device__ __forceinline__ void jacobi4(double (&A)[4][4], double (&V)[4][4], double (&w)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 64; sweep++) {
         double off = 0;
-        for (int p = 0; p < 4; p++) for (int q = p + 1; q < 4; q++) off += A[p][q] * A[p][q];
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+            for (int q = p + 1; q < 4; q++) off += A[p][q] * A[p][q];
         if (off < 1e-30) break;
-        for (int p = 0; p < 4; p++) for (int q = p + 1; q < 4; q++) {
-            if (fabs(A[p][q]) < 1e-300) continue;
-            double th = (A[q][q] - A[p][p]) / (2 * A[p][q]);
-            double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
-            double c = 1 / sqrt(t * t + 1), s = t * c;
-            for (int k = 0; k < 4; k++) { double x = A[k][p], y = A[k][q]; A[k][p] = c * x - s * y; A[k][q] = s * x + c * y; }
-            for (int k = 0; k < 4; k++) { double x = A[p][k], y = A[q][k]; A[p][k] = c * x - s * y; A[q][k] = s * x + c * y; }
-            for (int k = 0; k < 4; k++) { double x = V[k][p], y = V[k][q]; V[k][p] = c * x - s * y; V[k][q] = s * x + c * y; }
-        }
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+            for (int q = p + 1; q < 4; q++) {
+                if (fabs(A[p][q]) < 1e-300) continue;
+                const double th = (A[q][q] - A[p][p]) / (2 * A[p][q]);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+                const double c = 1 / sqrt(t * t + 1), s = t * c;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double x = A[k][p], y = A[k][q];
+                    A[k][p] = c * x - s * y;
+                    A[k][q] = s * x + c * y;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double x = A[p][k], y = A[q][k];
+                    A[p][k] = c * x - s * y;
+                    A[q][k] = s * x + c * y;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double x = V[k][p], y = V[k][q];
+                    V[k][p] = c * x - s * y;
+                    V[k][q] = s * x + c * y;
+                }
+            }
     }
+#pragma unroll
     for (int i = 0; i < 4; i++) w[i] = A[i][i];
 }
 
@@ -389,15 +418,17 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
                 {R[0][1] - R[1][0], R[0][2] + R[2][0], R[1][2] + R[2][1], -R[0][0] - R[1][1] + R[2][2]}};
             double V[4][4], w[4];
             jacobi4(F, V, w);
-            int im = 0;
-            for (int i = 1; i < 4; i++) if (w[i] > w[im]) im = i;
+            // largest eigenvalue and its eigenvector, selected without a runtime index
+            double wm = w[0], q0 = V[0][0], q1 = V[1][0], q2 = V[2][0], q3 = V[3][0];
+#pragma unroll
+            for (int i = 1; i < 4; i++)
+                if (w[i] > wm) { wm = w[i]; q0 = V[0][i]; q1 = V[1][i]; q2 = V[2][i]; q3 = V[3][i]; }
             // q rotates x onto y (correlation x y^T); bc[0..8] is its transpose,
             // the rotation that takes the reference y onto x
-            double q0 = V[0][im], q1 = V[1][im], q2 = V[2][im], q3 = V[3][im];
             bc[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3; bc[1] = 2 * (q1 * q2 + q0 * q3); bc[2] = 2 * (q1 * q3 - q0 * q2);
             bc[3] = 2 * (q1 * q2 - q0 * q3); bc[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3; bc[5] = 2 * (q2 * q3 + q0 * q1);
             bc[6] = 2 * (q1 * q3 + q0 * q2); bc[7] = 2 * (q2 * q3 - q0 * q1); bc[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
-            double msd = fmax(0.0, (c[9] - 2 * w[im]) / na);
+            double msd = fmax(0.0, (c[9] - 2 * wm) / na);
             double rmsd = sqrt(msd);
             bc[9] = rmsd > 1e-10 ? 1.0 / (na * rmsd) : 0.0;
             cvv[it.cv] = rmsd;

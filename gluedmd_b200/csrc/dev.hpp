@@ -91,6 +91,8 @@ struct CoordItem {
     int cn0;        // offset of this item's per-CTA CN partials
     int row0;       // first fixed-point accumulator row (A rows, then B rows)
     int pieceBegin, pieceEnd;   // this item's run-piece CN partials in cnPiece
+    int cells;      // 1: cutoff item evaluated by the cell-list path (coord_cells.cu):
+                    // no tile steps; one CN partial per A atom in cnPiece
 };
 
 struct CoordDev {
@@ -104,11 +106,44 @@ struct CoordDev {
     int bSplit;            // B atoms per split (multiple of the B chunk)
 };
 
+// Cutoff coordination through a cell list (coord_cells.cu). The box in FP64 for
+// the cutoff decisions, which must equal the FP64 oracle's: a, b, c and the
+// reciprocal diagonal 1/a_x, 1/b_y, 1/c_z; kind as BoxDev (0 none, 1
+// rectangular, 2 triclinic).
+struct CellBox {
+    double a[3], b[3], c[3], inv[3];
+    int kind, pad;
+};
+
+constexpr int CELL_MAX_DIM = 8;                      // cells per box dimension at most
+constexpr int CELL_MAX = CELL_MAX_DIM * CELL_MAX_DIM * CELL_MAX_DIM;
+constexpr int CELL_SPLIT = 3;   // warps per A atom (one per z slice of the stencil); CN partials per A atom
+
+struct CellItemDev {
+    int item;               // coordination item (accumulator rows, CN partials)
+    int a0, nA, b0, nB;     // into the coordination atom slots
+    int row0, pieceBegin;   // first accumulator row (A rows, then B rows); first CN partial
+    float r0, n, m;
+    double rc2;             // rc * rc in FP64
+    double rc;
+    int* cellStart;         // [CELL_MAX + 1]: first sorted B atom of every cell
+    int* sortedB;           // [nB]: B atom (0 .. nB - 1) of every sorted position
+    float4* sortedPos;      // [nB]: its position
+    int* grid;              // [4]: cells per dimension of the last binning, and their product
+};
+
 // Coordination as static per-CTA runs of (A tile, B chunk) steps (coord_run.cuh).
 constexpr int COORD_NW = 16;    // warps per CTA
-constexpr int COORD_CH = 128;   // B atoms per chunk
-constexpr int COORD_TA = 128;   // A atoms per tile (16 warps x 8)
+constexpr int COORD_CH = 128;   // B atoms per chunk (default shape)
+constexpr int COORD_TA = 128;   // A atoms per tile (16 warps x 8; default shape)
+constexpr int COORD_TA_MAX = 128, COORD_CH_MAX = 256;   // largest shapes (step packing)
 constexpr int COORD_F_FIRST = 1, COORD_F_LAST = 2;
+
+// CoordStep::packed = valid A atoms (8 bits) | valid B atoms (9 bits) << 8 | flags << 17
+__host__ __device__ inline int stepPack(int nA, int nB, int flags) { return nA | (nB << 8) | (flags << 17); }
+__host__ __device__ inline int stepNA(int p) { return p & 0xff; }
+__host__ __device__ inline int stepNB(int p) { return (p >> 8) & 0x1ff; }
+__host__ __device__ inline int stepFlags(int p) { return p >> 17; }
 
 // One (tile, chunk) step. 32 bytes.
 struct __align__(16) CoordStep {
@@ -117,7 +152,7 @@ struct __align__(16) CoordStep {
     int bStart;          // index into slots of the chunk's first B atom
     int rowA;            // acc row of the tile's first A atom
     int rowB;            // acc row of the chunk's first B atom
-    int packed;          // nAv | nBv << 8 | flags << 16 (COORD_F_*)
+    int packed;          // stepPack(nAv, nBv, flags (COORD_F_*))
     int pieceSlot;       // cnPiece slot of the run piece this step ends (static ranges), else -1
     int sys;             // system of the item (index into sysPosq / sysBox)
 };
@@ -147,6 +182,11 @@ __host__ __device__ inline int coordRange(int numSteps, int grid, int b) {
     return (int)(((long long)b * numSteps) / grid);
 }
 
+// Precision of the OPES / hill kernel sums (k_kernel_sums): FP64 evaluation and
+// sums; FP32 Gaussians with plain FP32 sums; FP32 Gaussians with two-sum
+// compensated FP32 sums.
+enum SumMode { SUM_FP64 = 0, SUM_FP32 = 1, SUM_FP32C = 2 };
+
 // Bias records, evaluated in the reference's bias-type order.
 struct BiasDev {
     int type;
@@ -159,6 +199,7 @@ struct BiasDev {
     // MetaD grid / hills
     double h0, hif;         // initial height, 1/((gamma-1) kT) or 0
     double sigma[8];
+    float isg2f[8];         // hills: 1 / sigma^2 in FP32 (FP32 kernel-sum modes)
     double origin[8], invSp[8], period[8];
     int npts[8], strides[8], per[8];
     double* grid;

@@ -24,12 +24,25 @@ void launchTestForce(cudaStream_t s, const float4* posq, const int* atomIndex, l
 // kind: switch kind shared by every item of the launch (3: n = 6, m = 12;
 // -1: other integer exponents; 0: non-integer exponents); hi: compare the upper
 // pair bound (cutoff or x <= 1000) in the full-tile path.
+// blocked: the A-side FP32 partials are flushed to the fixed-point sums every
+// crun::BLK_STEPS steps of a tile run instead of once at its end.
 void launchCoord(cudaStream_t s, const CoordRunDev& R, int numItems, int grid, int totalRows, int boxKind, int kind,
-                 bool hi, const JacDev& J, double* cvv, int parts = 3);
+                 bool hi, const JacDev& J, double* cvv, int parts = 3, bool blocked = false);
 void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* slots, int n);
+// gB[s][ch], gA[s][ta] of a step list built with A tiles of ta and B chunks of ch atoms
 void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
-                       int* gA);
+                       int* gA, int ta = COORD_TA, int ch = COORD_CH);
 int coordRunOccupancy(int kind, int boxKind, bool hi);
+// Cutoff coordination items on the cell-list path (coord_cells.cu): bin the B
+// atoms, then pair terms into acc / cnPiece (before k_coord_finalize). kind as
+// launchCoord. launchCellPairList: pass 1 bins and counts the pairs of every warp
+// (CELL_SPLIT per A atom: pairCount[CELL_SPLIT * totalA]); pass 2 writes them
+// at pairOffset (int pairs (a, b)).
+void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
+                     const float4* posq, const CellBox* box, unsigned long long* acc, double* cnPiece);
+void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
+                        const float4* posq, const CellBox* box, int* pairCount, const long long* pairOffset,
+                        int* pairs, int pass);
 // Once per (kernel, device, size): maximum shared-memory carveout and the
 // dynamic shared-memory limit of a persistent runs kernel.
 void runKernelSetup(const void* fn, size_t dynSmem);
@@ -37,7 +50,7 @@ void runKernelSetup(const void* fn, size_t dynSmem);
 // accumulator row count); per-CTA ranges of numSteps over grid CTAs; whether the
 // upper pair bound can bind.
 // itemsPerSys: items of one system (sysPosq / sysBox entry), item-major.
-int buildCoordSteps(std::vector<CoordItem>& items, int ra, std::vector<CoordStep>& steps, int itemsPerSys);
+int buildCoordSteps(std::vector<CoordItem>& items, int ra, int ch, std::vector<CoordStep>& steps, int itemsPerSys);
 // CTA b of the persistent grid runs steps [begin[b], begin[b + 1]) (coordRange)
 std::vector<int> balanceRanges(int numSteps, int grid);
 // Run pieces of the static ranges (maximal sub-runs of one tile on one CTA): the
@@ -50,7 +63,7 @@ bool coordNeedsHi(const std::vector<CoordItem>& items, const double box[9], bool
 constexpr int KSUM_CTAS = 64;
 void launchBiases(cudaStream_t s, const BiasDev* biases, int nb, const double* cvv, int numCVs,
                   const double* testGrad, double* dUdCV, double* energies, double* sumPart, bool kernelSums,
-                  bool singleLane);
+                  bool singleLane, int sumMode = SUM_FP64);
 void launchScatter(cudaStream_t s, const JacDev& J, const int* u2g, const double* dUdCV, long long* force,
                    int padded);
 void launchMetadDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, const double* energies);

@@ -360,6 +360,28 @@ class NativeContext:
         call("glued_context_opes_last_decision", self._h, int(idx), ctypes.byref(d))
         return d.value
 
+    SUM_FP64, SUM_FP32, SUM_FP32_TWOSUM = 0, 1, 2
+
+    def set_sum_precision(self, kernel_sums=0, coordination=0):
+        """glued_context_set_sum_precision: kernel_sums 0 FP64 / 1 FP32 / 2 FP32
+        two-sum; coordination 0 per tile run / 1 blocked."""
+        call("glued_context_set_sum_precision", self._h, int(kernel_sums), int(coordination))
+
+    def sum_precision(self):
+        k, c = c_int(), c_int()
+        call("glued_context_get_sum_precision", self._h, ctypes.byref(k), ctypes.byref(c))
+        return k.value, c.value
+
+    def coordination_pairs(self, cv_index):
+        """glued_context_coordination_pairs: sorted (a, b) group indices, shape (n, 2)."""
+        import numpy as np
+        n = c_ll()
+        call("glued_context_coordination_pairs", self._h, int(cv_index), None, 0, ctypes.byref(n))
+        out = np.zeros(2 * max(1, n.value), dtype=np.int32)
+        call("glued_context_coordination_pairs", self._h, int(cv_index),
+             out.ctypes.data_as(ctypes.POINTER(c_int)), n.value, ctypes.byref(n))
+        return out[:2 * n.value].reshape(-1, 2)
+
     def profile_phases(self, reps=20):
         n = c_int(6)
         out = (c_double * 6)()

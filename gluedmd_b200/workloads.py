@@ -25,6 +25,7 @@ import numpy as np
 KT300 = 2.494338785
 CV_DISTANCE, CV_ANGLE, CV_DIHEDRAL, CV_COM_DISTANCE, CV_GYRATION = 1, 2, 3, 4, 5
 CV_COORDINATION, CV_RMSD, CV_PATH, CV_CONTACTMAP = 6, 7, 10, 13
+CV_COORDINATION_CUTOFF, CV_RMSD_KABSCH = 106, 107
 BIAS_HARMONIC, BIAS_METAD, BIAS_PBMETAD, BIAS_OPES, BIAS_EXTERNAL, BIAS_METAD_HILLS = 1, 3, 4, 5, 6, 103
 
 
@@ -239,8 +240,8 @@ def config1(form="grid", n_hills=2000, bins=256):
                     dict(centers=centers, heights=heights))
 
 
-def coordination_cn_fp64(pos, A, B, box_len, r0=0.35, n=6, m=12, chunk=256):
-    """Reference-semantics CN in FP64 (no cutoff), used to place the C2 grid."""
+def coordination_cn_fp64(pos, A, B, box_len, r0=0.35, n=6, m=12, chunk=256, rc=0.0):
+    """Reference-semantics CN in FP64 (no cutoff unless rc > 0), used to place the C2 grid."""
     cn = 0.0
     pa, pb = pos[A], pos[B]
     for s in range(0, len(A), chunk):
@@ -251,15 +252,30 @@ def coordination_cn_fp64(pos, A, B, box_len, r0=0.35, n=6, m=12, chunk=256):
         with np.errstate(divide="ignore", invalid="ignore"):
             f = (1 - x ** n) / (1 - x ** m)
         f = np.where(np.abs(x - 1) < 1e-4, n / m, f)
-        cn += f[(r * r >= 1e-20) & (x <= 1000)].sum()
+        keep = (r * r >= 1e-20) & (x <= 1000)
+        if rc > 0:
+            keep &= r * r < rc * rc
+        cn += f[keep].sum()
     return cn
 
 
-def config2(n_hills=20000, bins=256, with_bias=True):
+def _cn_axis(cn0, bins):
+    """Grid bounds on (CN, RMSD): CN over [0.9, 1.1] cn0 shifted so that cn0 sits
+    0.37 of a cell past a grid node (on a node, the interpolated bias has a kink
+    there and the FP32 CN's last bits would pick one side's gradient or the
+    other), RMSD over [0, 0.5]."""
+    sp = 0.2 * cn0 / bins
+    lo = cn0 * 0.9 - 0.37 * sp
+    return [lo, 0.0], [lo + 0.2 * cn0, 0.5]
+
+
+def config2(n_hills=20000, bins=256, with_bias=True, fit=False):
     """C2: 20,000 atoms at water density (5.9 nm cube, seed 3); coordination
     between the first 2,048 and next 8,192 atoms of a seeded permutation (r0 0.35,
     6/12, no cutoff); RMSD over 1,000 atoms vs pos + N(0, 0.1) (seed 4); 2-D MetaD
-    on (CN, RMSD), 256 x 256 non-periodic grid, 20,000 hills (seed 5)."""
+    on (CN, RMSD), 256 x 256 non-periodic grid, 20,000 hills (seed 5). fit: the
+    RMSD after optimal superposition (Kabsch, FP64 quaternion eigensolve) instead
+    of the reference's no-fit RMSD; workload "C2-kabsch"."""
     L = 5.9
     rng = np.random.default_rng(3)
     pos = rng.uniform(0.0, L, (20000, 3))
@@ -268,14 +284,13 @@ def config2(n_hills=20000, bins=256, with_bias=True):
     R = perm[2048 + 8192:2048 + 8192 + 1000]
     ref = pos[R] + np.random.default_rng(4).normal(0.0, 0.1, (1000, 3))
     cvs = [(CV_COORDINATION, [2048] + list(A) + list(B), [0.35, 6, 12]),
-           (CV_RMSD, list(R), list(ref.ravel()))]
+           (CV_RMSD_KABSCH if fit else CV_RMSD, list(R), list(ref.ravel()))]
     extra = dict(A=A, B=B, R=R)
     if not with_bias:
         return Workload("C2-cv", pos, _cube(L), cvs, [], np.ones(20000), True, b"", extra)
     cn0 = coordination_cn_fp64(pos, A, B, L)
     rmsd0 = float(np.sqrt(((pos[R] - ref) ** 2).sum(-1).mean()))
-    lo = [cn0 * 0.9, 0.0]
-    hi = [cn0 * 1.1, 0.5]
+    lo, hi = _cn_axis(cn0, bins)
     sigma = [0.02 * (hi[0] - lo[0]), 0.02 * (hi[1] - lo[1])]
     hr = np.random.default_rng(5)
     centers = np.stack([hr.uniform(lo[0], hi[0], n_hills), hr.uniform(lo[1], hi[1], n_hills)], 1)
@@ -284,7 +299,45 @@ def config2(n_hills=20000, bins=256, with_bias=True):
     params = [1.2] + sigma + [10.0, KT300] + lo + hi
     biases = [(BIAS_METAD, [0, 1], params, [500, bins, bins, 0, 0])]
     extra.update(cn0=cn0, rmsd0=rmsd0)
-    return Workload("C2", pos, _cube(L), cvs, biases, np.ones(20000), True, blob(metad=[(n_hills, g)]), extra)
+    return Workload("C2-kabsch" if fit else "C2", pos, _cube(L), cvs, biases, np.ones(20000), True,
+                    blob(metad=[(n_hills, g)]), extra)
+
+
+def config2_cutoff(method=0, rc=1.2, box=5.9):
+    """C2 with the coordination restricted to pairs closer than rc = 1.2 nm
+    (CV_COORDINATION_CUTOFF, no reference counterpart): 2,048 x 8,192 coordination
+    and the 1,000-atom RMSD of a seeded permutation of atoms at C2's density
+    (97.4 nm^-3) in a cube of side `box` (5.9 nm: C2's own atoms), 256 x 256
+    MetaD grid on (CN, RMSD) centred on this CN. method 0: all-pairs tiles with
+    a cutoff mask; 1: cell-list pair search. Positions are FP32-exact (as OpenMM's
+    posq holds them), so the FP64 oracle's cutoff decisions see the same
+    coordinates as the GPU."""
+    if box == 5.9:
+        w = config2()
+        pos, A, B, R = w.positions, w.extra["A"], w.extra["B"], w.extra["R"]
+        rmsd_cv = w.cvs[1]
+    else:
+        n = int(round(20000 * (box / 5.9) ** 3))
+        rng = np.random.default_rng(13)
+        pos = rng.uniform(0.0, box, (n, 3))
+        perm = rng.permutation(n)
+        A, B, R = perm[:2048], perm[2048:2048 + 8192], perm[2048 + 8192:2048 + 8192 + 1000]
+        ref = pos[R] + np.random.default_rng(4).normal(0.0, 0.1, (1000, 3))
+        rmsd_cv = (CV_RMSD, list(R), list(ref.ravel()))
+    pos = np.asarray(pos, np.float32).astype(np.float64)
+    cvs = [(CV_COORDINATION_CUTOFF, [len(A)] + list(A) + list(B), [0.35, 6, 12, rc, float(method)]), rmsd_cv]
+    cn0 = coordination_cn_fp64(pos, A, B, box, rc=rc)
+    lo, hi = _cn_axis(cn0, 256)
+    sigma = [0.02 * (hi[0] - lo[0]), 0.02 * (hi[1] - lo[1])]
+    hr = np.random.default_rng(5)
+    n_hills, bins = 20000, 256
+    centers = np.stack([hr.uniform(lo[0], hi[0], n_hills), hr.uniform(lo[1], hi[1], n_hills)], 1)
+    heights = wt_hill_heights(centers, sigma, [0.0, 0.0], 1.2, 10.0, KT300)
+    g = grid_from_hills_windowed(centers, heights, sigma, lo, hi, [bins, bins], [0, 0])
+    biases = [(BIAS_METAD, [0, 1], [1.2] + sigma + [10.0, KT300] + lo + hi, [500, bins, bins, 0, 0])]
+    extra = dict(A=A, B=B, R=R, cn0=cn0, rc=rc)
+    name = "C2-cutoff" + ("" if box == 5.9 else f"-{box:g}nm") + ("-tiles" if method == 0 else "-cells")
+    return Workload(name, pos, _cube(box), cvs, biases, np.ones(len(pos)), True, blob(metad=[(n_hills, g)]), extra)
 
 
 def _opes_pair_sum(centers, sigmas, logw, cutoff2, chunk=1024):

@@ -163,6 +163,25 @@ int glued_measure_fp32_peak(double* tflops);
 /* Test hook: index of the last OPES deposit decision of OPES bias opes_index
  * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
 int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);
+/* Sum precision (no reference counterpart; the reference sums in FP32/FP64 as
+ * its kernels are written). kernel_sums, for the OPES and hill-sum MetaD kernel
+ * sums: 0 = FP64 evaluation and sums (default), 1 = FP32 Gaussians and plain FP32
+ * sums, 2 = FP32 Gaussians and two-sum compensated FP32 sums; in modes 1 and 2
+ * OPES heights are exp(logW - M) with M the largest logW of a warp, rescaled by
+ * exp(M) in FP64, and the hill truncation exponent is formed in FP64.
+ * coordination: 0 = per-lane FP32 A-gradient sums over a whole tile run (default),
+ * 1 = blocked, flushed into the exact 64-bit fixed-point sums every 8 steps
+ * (<= 32 pairs per FP32 partial). Takes effect at the next execute.            */
+int glued_context_set_sum_precision(glued_context* c, int kernel_sums, int coordination);
+/* Pair list of a cutoff coordination CV (CV_COORDINATION_CUTOFF on the default
+ * cell-list path; params[4] = 1 selects all-pairs tiles instead and has no list)
+ * at the bound positions and box: pairs (a, b) of group-A index a and group-B
+ * index b with 1e-20 <= r^2 < rc^2 (r^2 in FP64 from the FP32 positions,
+ * minimum image floor(d / L + 1/2)), sorted; *n = number of pairs, min(cap, *n)
+ * pairs (2 ints each) copied to out (may be NULL when cap is 0). cv_index is
+ * the CV's value index. Synchronizing. No reference counterpart.              */
+int glued_context_coordination_pairs(glued_context* c, int cv_index, int* out, long long cap, long long* n);
+int glued_context_get_sum_precision(glued_context* c, int* kernel_sums, int* coordination);
 
 /* ------------------------------------------------------ differentiable bias
  * Contact map + path CV + hill bias E(CMAP, s) with a hand-written backward
@@ -259,16 +278,30 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
                        glued_batch** out);
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
-/* Tuning: tune[4] = {ra (8), finalize_parts (finalize CTAs per walker; 0 = the
- * fewest that cover the walker's coordination rows), finalize launch (0: a
- * programmatic dependent launch of the runs kernel, 1: a plain stream-ordered
- * launch), 0}. autotune times the candidates on the
+/* Tuning: tune[4] = {ra (A atoms per warp of a coordination tile: 4 or 8, tile =
+ * 16 ra atoms), finalize_parts (finalize CTAs per walker; 0 = the fewest that
+ * cover the walker's coordination rows), finalize launch (0: a programmatic
+ * dependent launch of the runs kernel, 1: a plain stream-ordered launch), B chunk
+ * (128 or 256 atoms; 0 = 128)}. Tile shapes other than ra 8 / chunk 128 exist for
+ * the n = 6, m = 12 switch in rectangular or no boxes with plain FP32 sums.
+ * autotune times every available shape x finalize parts x launch mode on the
  * live walkers, each timed step after an L2 flush (forces of the trial launches
  * go to a scratch buffer; a 192 MB flush buffer is allocated for the call and
- * freed), keeps the fastest and returns it in tune (synchronizing).            */
+ * freed), keeps the fastest and returns it in tune (synchronizing). The choice
+ * is cached for the process per (walker count, coordination group sizes, hill
+ * count to a power of two, box kind, switch kind, sum precision);
+ * glued_batch_autotune uses the cache, glued_batch_autotune_ex(use_cache = 0)
+ * times again (*cached = 1 when the returned choice came from the cache).      */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);
+int glued_batch_autotune_ex(glued_batch* b, int use_cache, int tune[4], int* cached);
+/* Sum precision of the batch: 1 = plain FP32 hill and coordination sums
+ * (default), 2 = two-sum compensated FP32 hill sums (per lane and through the
+ * lane tree, hi + lo in FP64 per runs CTA) and blocked coordination A sums
+ * (as glued_context_set_sum_precision coordination = 1).                       */
+int glued_batch_set_sum_precision(glued_batch* b, int mode);
+int glued_batch_get_sum_precision(glued_batch* b, int* mode);
 /* One step for all walkers: CVs, biases and force scatter (one graph of two
  * launches: the coordination/hill runs kernel, then the finalize kernel).
  * Forces are added to each walker's buffer.                                    */

@@ -596,3 +596,33 @@ def max_rel_force_err(f, fref):
     """||f - fref||_inf / ||fref||_inf over all atoms and components."""
     den = np.max(np.abs(fref))
     return float(np.max(np.abs(np.asarray(f) - fref)) / den) if den > 0 else float(np.max(np.abs(f)))
+
+
+def coordination_pair_list(pos, A, B, box9, rc, periodic=True, block=128):
+    """Pairs (a, b) (indices into the groups A and B) that a cutoff coordination
+    counts: 1e-20 <= r^2 < rc^2 with r^2 formed in FP64 as cv_coordination forms
+    it (glued_oracle.cpp, cv_coordination and Box::image: d = p_a - p_b, then
+    s = floor(d_z / c_z + 1/2), d -= s c; the same along b and a; r^2 = x^2 + y^2
+    + z^2 left to right, each operation rounded on its own; rc^2 = rc * rc).
+    numpy evaluates every elementwise operation with one rounding and no
+    contraction, which is the oracle's arithmetic. Sorted by (a, b)."""
+    pos = np.asarray(pos, np.float64)
+    bx = np.asarray(box9, np.float64).reshape(3, 3)
+    inv = np.array([1.0 / bx[0, 0], 1.0 / bx[1, 1], 1.0 / bx[2, 2]])
+    rc2 = float(rc) * float(rc)
+    pb = pos[np.asarray(B)]
+    out = []
+    A = np.asarray(A)
+    for s in range(0, len(A), block):
+        pa = pos[A[s:s + block]]
+        d = pa[:, None, :] - pb[None, :, :]
+        if periodic:
+            for axis, vec in ((2, bx[2]), (1, bx[1]), (0, bx[0])):
+                sh = np.floor(d[..., axis] * inv[axis] + 0.5)
+                for k in range(axis + 1):
+                    d[..., k] = d[..., k] - sh * vec[k]
+        r2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+        ia, ib = np.nonzero((r2 >= 1e-20) & (r2 < rc2))
+        out.append(np.stack([ia + s, ib], 1))
+    p = np.concatenate(out) if out else np.zeros((0, 2), np.int64)
+    return p[np.lexsort((p[:, 1], p[:, 0]))].astype(np.int32)

@@ -90,13 +90,44 @@ def test_batch_repeatable_and_autotuned():
     f2 = [w.forces() for w in walkers]
     for a, c in zip(f1, f2):
         assert np.array_equal(a, c)  # deterministic reductions: bitwise repeatable
-    t = b.autotune()
-    assert t["ra"] == 8 and t["parts"] >= 1
+    t = b.autotune(use_cache=False)
+    assert t["ra"] in (4, 8) and t["ch"] in (128, 256) and t["parts"] >= 1 and not b.tune_cached
     for wk in walkers:
         wk.force.zero_()
     b.execute()
     for i, w in enumerate(walkers):
         assert O.max_rel_force_err(w.forces(), f1[i]) < 2e-6
+    assert b.status() == 0
+    # a second batch of the same signature takes the cached choice without timing
+    b2, walkers2, _ = _setup(ws, hill, True)
+    assert b2.autotune() == t and b2.tune_cached
+
+
+@pytest.mark.parametrize("ra,ch", [(8, 128), (4, 128), (8, 256), (4, 256)])
+def test_batch_tile_shapes_agree(ra, ch):
+    """Every tile shape the autotuner may pick: forces and CVs of all walkers
+    within the FP64 oracle's gates (the walkers' groups are not multiples of the
+    tiles, so ragged steps are included), and within 1e-6 of the default shape.
+    The shapes group the FP32 pair terms differently before the 64-bit
+    fixed-point sums, so they agree to FP32 rounding, not bit for bit."""
+    ws, hill = _walkers(n_walkers=6, coord=(200, 700))   # full and ragged tiles in every shape
+    b, walkers, specs = _setup(ws, hill, True)
+    ref = []
+    for shape in ((8, 128), (ra, ch)):
+        b.set_tuning(ra=shape[0], ch=shape[1])
+        assert b.tuning["ra"] == shape[0] and b.tuning["ch"] == shape[1]
+        for wk in walkers:
+            wk.force.zero_()
+        b.execute()
+        ref.append(([w.forces() for w in walkers], b.cv_values(), b.energies()))
+    (f0, cv0, e0), (f1, cv1, e1) = ref
+    for i in range(len(walkers)):
+        assert O.max_rel_force_err(f1[i], f0[i]) < 1e-6, i
+    np.testing.assert_allclose(cv1, cv0, rtol=1e-7)
+    np.testing.assert_allclose(e1, e0, rtol=1e-6, atol=1e-9)
+    for i, w in enumerate(ws):
+        r = _oracle(w, specs[i], hill)
+        assert O.max_rel_force_err(f1[i], r["forces"]) < 1e-4, i
     assert b.status() == 0
 
 
