@@ -542,19 +542,21 @@ def run_c4(args, torch, ws, hill):
     flops = pairs * FLOP_PAIR + W_ * b.num_hills() * FLOP_HILL
     # per-kernel durations (CUDA events around each launch of one step, L2 flushed
     # before every step): the dominant kernel is the coordination-runs kernel
-    runs, fins = [], []
+    runs, fins, waits = [], [], []
     for i in range(20):
         flush.add_(1.0)
         pt = b.phase_times()
         runs.append(pt["runs_us"])
         fins.append(pt["finalize_us"])
+        waits.append(pt["hill_wait_us"])
     runs_us = sum(runs) / len(runs)
     fin_us = sum(fins) / len(fins)
+    hill_wait_us = float(np.median(waits))
     return dict(walkers=W_, step_ms=step_ms, value=W_ * 1e3 / step_ms, plain_ms=plain_ms,
                 plain_value=W_ * 1e3 / plain_ms, plain_launches=plain_launches, e2e_value=W_ * 1e3 / e2e_ms,
                 h2d=int(h2d), d2h=int(d2h), launches_per_step=launches / float(args.steps + args.warmup),
                 flops=flops, clocks=clk.summary(), tune=tune, status=status, hills=b.num_hills(),
-                graphed=True, runs_us=runs_us, finalize_us=fin_us, parity=parity)
+                graphed=True, runs_us=runs_us, finalize_us=fin_us, hill_wait_us=hill_wait_us, parity=parity)
 
 
 def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
@@ -613,7 +615,8 @@ def precision_sweep(args, torch):
     FP64 oracle of each sum-precision variant of one workload; one JSON line each.
     c1h / c3: kernel sums in FP64, FP32, FP32 two-sum (+ blocked coordination);
     c2cut: the C2 cutoff coordination on all-pairs tiles and on the cell list, in
-    C2's 5.9 nm box and in a 12 nm box at the same density;
+    C2's 5.9 nm box and in a 12 nm box at the same density; c4tiles: every tile shape
+    of the batch at the autotuned finalize setting;
     c2: no-fit RMSD or Kabsch RMSD (FP64 eigensolve), per-tile-run or blocked
     coordination sums; c4: the batch in plain FP32 and in two-sum FP32."""
     from gluedmd_b200 import workloads as W
@@ -652,6 +655,25 @@ def precision_sweep(args, torch):
             for method in (0, 1):
                 single(W.config2_cutoff(method, box=box), 0, 0, ("tiles+mask" if method == 0 else "cells") +
                        f" box {box:g} nm")
+    elif args.config == "c4tiles":
+        # the batch's tile shapes (A atoms per warp x B chunk) at the fewest finalize parts
+        from gluedmd_b200.batch import Batch, WalkerPool, force_for
+        ws, hill = c4_inputs()
+        pool = WalkerPool([w["pos"] for w in ws], [w["box"] for w in ws])
+        b = Batch([force_for(w["cvs"], c4_biases(w, hill)) for w in ws], pool.walkers)
+        b.set_hills(hill["centers"], hill["heights"])
+        picked = b.autotune(use_cache=False)
+        for ra, ch in ((8, 128), (4, 128), (8, 256), (4, 256)):
+            b.set_tuning(ra=ra, parts=picked["parts"], plain=picked["plain"], ch=ch)
+            par = parity_c4(b, pool, ws, hill)
+            ms = time_steps(torch, lambda i: (b.update_state(i), b.execute()), args.steps, args.warmup, flush)
+            runs = []
+            for _ in range(10):
+                flush.add_(1.0)
+                runs.append(b.phase_times()["runs_us"])
+            out.append({"sweep": "c4tiles", "variant": f"ra {ra} x chunk {ch}", "workload": C4_WORKLOAD,
+                        "us_per_step": ms * 1e3 / args.steps, "runs_us": float(np.median(runs)),
+                        "max_rel_force_err": par["max_rel_force_err"], "autotuned": picked})
     elif args.config == "c4":
         from gluedmd_b200.batch import Batch, WalkerPool, force_for
         ws, hill = c4_inputs()
@@ -667,7 +689,7 @@ def precision_sweep(args, torch):
                         "max_rel_force_err": par["max_rel_force_err"], "energy_rel_err": par["energy_rel_err"],
                         "cv_rel_err": par["cv_rel_err"], "tuning": tune, "status": b.status()})
     else:
-        raise SystemExit("--precision-sweep: config must be c1h, c2, c2cut, c3 or c4")
+        raise SystemExit("--precision-sweep: config must be c1h, c2, c2cut, c3, c4 or c4tiles")
     for line in out:
         print(json.dumps(line))
 
@@ -677,7 +699,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--config", default="c4", choices=["c1", "c1pb", "c1h", "c2", "c2cut", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c1pb", "c1h", "c2", "c2cut", "c3", "c4", "c4tiles", "c5"])
     ap.add_argument("--precision-sweep", action="store_true",
                     help="time and check every sum-precision variant of --config (one JSON line each)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -778,7 +800,8 @@ def main():
                     "peak_source": "FP32 FMA microkernel measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
                     "algorithmic": f"64 x 262144 pairs x {FLOP_PAIR:.0f} flop + 64 x {info['hills']} hills x {FLOP_HILL:.0f} flop",
                     "whole_step_frac": info["flops"] / (info["step_ms"] * 1e-3) / 1e12 / fp32.value,
-                    "finalize_us": info["finalize_us"]}
+                    "finalize_us": info["finalize_us"],
+                    "hill_data_wait_us": info["hill_wait_us"]}
             cb = cb1 = None
             if not args.no_cpu_baseline and world == 1:
                 cb = cpu_reference_c4(ws, hill, steps_budget_s=15.0)

@@ -84,6 +84,7 @@ _SIGS = {
     "glued_context_profile_phases": [c_void_p, c_int, P(c_double), P(c_int)],
     "glued_context_launch_count": [c_void_p, P(c_ll)],
     "glued_measure_fp32_peak": [P(c_double)],
+    "glued_measure_hill_staging": [c_int, c_int, c_int, P(c_double), P(c_int)],
     "glued_ad_forward": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int],
     "glued_ad_backward": [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                           c_void_p],

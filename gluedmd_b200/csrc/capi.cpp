@@ -304,6 +304,12 @@ int glued_context_profile_phases(glued_context* c, int reps, double* out, int* n
 int glued_context_launch_count(glued_context* c, long long* count) {
     return guard([&] { need(c, "context"); need(count, "out"); *count = c->c->launchCount(); });
 }
+int glued_measure_hill_staging(int num_hills, int ctas, int reps, double out[2], int* status) {
+    return guard([&] {
+        need(out, "out"); need(status, "status");
+        glued::measureHillStaging(num_hills, ctas, reps, &out[0], &out[1], status);
+    });
+}
 int glued_measure_fp32_peak(double* tflops) {
     return guard([&] { need(tflops, "out"); *tflops = glued::measureFp32Peak(); });
 }

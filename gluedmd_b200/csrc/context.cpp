@@ -431,7 +431,7 @@ void Context::buildPlan(const GluedForce& f) {
         cellTotalA_ = 0;
         size_t bytes = 0;
         auto carve = [&](size_t n) { size_t o = bytes; bytes += (n + 255) / 256 * 256; return o; };
-        std::vector<std::array<size_t, 4>> offs;
+        std::vector<std::array<size_t, 7>> offs;
         // every cutoff item gets cell-list state (its pair list); those evaluated on
         // the cell list come first (cellEvalN_ of them)
         std::vector<size_t> order;
@@ -439,12 +439,15 @@ void Context::buildPlan(const GluedForce& f) {
             if (coord[i].cells) order.push_back(i);
         cellEvalN_ = (int)order.size();
         cellEvalA_ = 0;
+        cellMaxB_ = cellEvalMaxB_ = 0;
         for (size_t i = 0; i < coord.size(); i++)
             if (!coord[i].cells && coordRc[i] > 0.0) order.push_back(i);
         for (size_t i : order) {
             const CoordItem& it = coord[i];
             offs.push_back({carve(sizeof(int) * (CELL_MAX + 1)), carve(sizeof(int) * std::max(1, it.nB)),
-                            carve(sizeof(float4) * std::max(1, it.nB)), carve(sizeof(int) * 4)});
+                            carve(sizeof(float4) * std::max(1, it.nB)), carve(sizeof(int) * 4),
+                            carve(sizeof(int) * std::max(1, it.nB)), carve(sizeof(float4) * std::max(1, it.nB)),
+                            carve(sizeof(int) * CELL_MAX)});
             CellItemDev ci{};
             ci.item = (int)i; ci.a0 = it.a0; ci.nA = it.nA; ci.b0 = it.b0; ci.nB = it.nB;
             ci.row0 = it.row0; ci.pieceBegin = it.pieceBegin;
@@ -453,7 +456,11 @@ void Context::buildPlan(const GluedForce& f) {
             ci.rc2 = coordRc[i] * coordRc[i];
             cellItemsH_.push_back(ci);
             cellTotalA_ += it.nA;
-            if (it.cells) cellEvalA_ += it.nA;
+            cellMaxB_ = std::max(cellMaxB_, it.nB);
+            if (it.cells) {
+                cellEvalA_ += it.nA;
+                cellEvalMaxB_ = std::max(cellEvalMaxB_, it.nB);
+            }
         }
         cellItemsN_ = (int)cellItemsH_.size();
         if (cellItemsN_ > 0) {
@@ -464,6 +471,9 @@ void Context::buildPlan(const GluedForce& f) {
                 cellItemsH_[k].sortedB = reinterpret_cast<int*>(base + offs[k][1]);
                 cellItemsH_[k].sortedPos = reinterpret_cast<float4*>(base + offs[k][2]);
                 cellItemsH_[k].grid = reinterpret_cast<int*>(base + offs[k][3]);
+                cellItemsH_[k].cellId = reinterpret_cast<int*>(base + offs[k][4]);
+                cellItemsH_[k].posB = reinterpret_cast<float4*>(base + offs[k][5]);
+                cellItemsH_[k].counts = reinterpret_cast<int*>(base + offs[k][6]);
             }
             cellItems_.upload(cellItemsH_);
             CellBox cb{};
@@ -824,7 +834,8 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
 }
 
 void Context::enqueueCells(cudaStream_t s) {
-    launchCellCoord(s, cellItems_.as<CellItemDev>(), cellEvalN_, cellEvalA_, coordKind_, coordSlots_.as<int>(),
+    launchCellCoord(s, cellItems_.as<CellItemDev>(), cellEvalN_, cellEvalA_, cellEvalMaxB_, coordKind_,
+                    coordSlots_.as<int>(),
                     static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), coordAcc_.as<unsigned long long>(),
                     coordCnPiece_.as<double>());
 }
@@ -844,7 +855,7 @@ std::vector<int> Context::cellPairs(int cvIndex) {
     DBuf cnt, off, pairs;
     cnt.alloc(sizeof(int) * std::max(1, nw));
     off.alloc(sizeof(long long) * std::max(1, nw));
-    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, coordKind_,
+    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, cellMaxB_, coordKind_,
                        coordSlots_.as<int>(), static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), cnt.as<int>(),
                        nullptr, nullptr, 1);
     std::vector<int> c(nw);
@@ -854,7 +865,7 @@ std::vector<int> Context::cellPairs(int cvIndex) {
     for (int i = 0; i < nw; i++) o[i + 1] = o[i] + c[i];
     cudaCheck(cudaMemcpy(off.p, o.data(), sizeof(long long) * nw, cudaMemcpyHostToDevice), "pairs");
     pairs.alloc(sizeof(int) * 2 * std::max<long long>(1, o[nw]));
-    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, coordKind_,
+    launchCellPairList(stream_, cellItems_.as<CellItemDev>(), cellItemsN_, cellTotalA_, cellMaxB_, coordKind_,
                        coordSlots_.as<int>(), static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), nullptr,
                        off.as<long long>(), pairs.as<int>(), 2);
     const long long p0 = o[CELL_SPLIT * a0], p1 = o[CELL_SPLIT * (a0 + nA)];

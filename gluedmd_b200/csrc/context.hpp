@@ -146,6 +146,7 @@ private:
     std::vector<CellItemDev> cellItemsH_;
     int cellItemsN_ = 0, cellTotalA_ = 0;   // every cutoff item
     int cellEvalN_ = 0, cellEvalA_ = 0;     // the first cellEvalN_: evaluated on the cell list
+    int cellMaxB_ = 0, cellEvalMaxB_ = 0;   // largest B group (all / evaluated items)
     CellBox* cellBoxPinned_ = nullptr;
     int sumMode_ = SUM_FP64;        // OPES / hill kernel sums (SumMode)
     bool coordBlocked_ = false;     // coordination A sums flushed every crun::BLK_STEPS steps

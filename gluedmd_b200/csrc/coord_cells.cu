@@ -16,20 +16,26 @@
 // closer than rc is then in neighbouring cells. Other boxes (triclinic, or no
 // periodicity) use one cell: every B atom is a candidate.
 //
-// k_cell_bin (one CTA per item) sorts the B atoms by cell with a stable
-// counting sort: counts, a scan, then chunks of 1024 atoms in index order, each
-// atom's slot = the cell's cursor + same-cell atoms of earlier warps in the chunk
-// + same-cell lanes before it in its warp (match_any). Within a cell the atoms
-// stay in index order, so the candidate order is fixed.
+// Binning, a counting sort of the B atoms by cell in three launches:
+// k_cell_count (one thread per B atom) writes every atom's cell and position and
+// counts the cells with integer atomics; k_cell_scan turns the counts into cell
+// starts and write cursors; k_cell_scatter places every atom at its cell's next
+// slot. The order within a cell follows the atomics, which is why every sum of
+// the pairs kernel is formed in 64-bit fixed point (exact, order-independent):
+// the results are bitwise reproducible all the same. The pairs kernel clears
+// the counts after its wait.
 //
 // k_cell_pairs (CELL_SPLIT warps per A atom, one z slice of the stencil each)
-// visits the slice's cells in a fixed order, lanes striding over each cell's
-// atoms. CN partial of the (A atom, slice): lane sums in FP64, fixed butterfly,
-// stored to its own cnPiece slot (the finalize adds the item's slots in order).
-// Gradients: A sums over lanes (FP32 butterfly) and every B term go to the
-// 64-bit fixed-point accumulator rows, as on the tile path, so k_coord_finalize
-// turns them into Jacobian rows unchanged. EMIT = 1 counts the pairs of every
-// warp, EMIT = 2 writes them (test and diagnostic use).
+// visits the slice's cells, lanes striding over each cell's atoms. Every pair
+// term (switch value, gradient components) is converted to 64-bit fixed point
+// (value * 2^32) and summed exactly: the CN partial of the (A atom, slice) goes
+// to its own cnPiece slot (the finalize adds the item's slots in order), the A
+// sums and every B term to the fixed-point accumulator rows, as on the tile
+// path, so k_coord_finalize turns them into Jacobian rows unchanged. EMIT = 1
+// counts the pairs of every warp, EMIT = 2 writes them (test and diagnostic
+// use; the host sorts the list).
+#include <algorithm>
+
 #include "coord_run.cuh"
 #include "kernels.hpp"
 #include "pdl.cuh"
@@ -84,95 +90,92 @@ __device__ __forceinline__ int cellOf(const float4& p, const CellBox& b, const i
 
 }  // namespace
 
-constexpr int BIN_THREADS = 1024;
-constexpr int BIN_PER = 8;   // atoms per thread held in registers between the two passes
+constexpr int COUNT_THREADS = 256;
 
-__global__ void __launch_bounds__(BIN_THREADS) k_cell_bin(const CellItemDev* __restrict__ items,
-                                                          const int* __restrict__ slots,
-                                                          const float4* __restrict__ posq,
-                                                          const CellBox* __restrict__ boxp) {
-    __shared__ int cnt[CELL_MAX], cursor[CELL_MAX];
-    __shared__ unsigned char wc[BIN_THREADS / 32][CELL_MAX];
+// Binning, first half (grid: B atoms x items): the cell of every B atom and its
+// position into cellId / posB, per-cell counts with integer atomics (one per
+// distinct cell of a warp), and the cell grid.
+__global__ void __launch_bounds__(COUNT_THREADS) k_cell_count(const CellItemDev* __restrict__ items,
+                                                              const int* __restrict__ slots,
+                                                              const float4* __restrict__ posq,
+                                                              const CellBox* __restrict__ boxp) {
     pdlEnter();
-    const CellItemDev& it = items[blockIdx.x];
+    const CellItemDev& it = items[blockIdx.y];
     const CellBox box = *boxp;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nB = it.nB;
     int nc[3];
     cellDims(box, it.rc, nc);
-    const int ncell = nc[0] * nc[1] * nc[2];
-    for (int c = tid; c < ncell; c += BIN_THREADS) cnt[c] = 0;
-    for (int i = tid; i < (BIN_THREADS / 32) * CELL_MAX; i += BIN_THREADS) (&wc[0][0])[i] = 0;
-    __syncthreads();
-    const int* bs = slots + it.b0;
-    constexpr int GROUP = BIN_PER * BIN_THREADS;
-    float4 P[BIN_PER];
-    int C[BIN_PER];
-    // positions and cells of one group of atoms, every load issued before any use
-    auto load = [&](int g0) {
-        int sl[BIN_PER];
-#pragma unroll
-        for (int k = 0; k < BIN_PER; k++) {
-            const int j = g0 + k * BIN_THREADS + tid;
-            sl[k] = j < nB ? bs[j] : -1;
-        }
-#pragma unroll
-        for (int k = 0; k < BIN_PER; k++) P[k] = sl[k] >= 0 ? posq[sl[k]] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int k = 0; k < BIN_PER; k++) C[k] = sl[k] >= 0 ? cellOf(P[k], box, nc) : -1;
-    };
-    for (int g0 = 0; g0 < nB; g0 += GROUP) {
-        load(g0);
-#pragma unroll
-        for (int k = 0; k < BIN_PER; k++)
-            if (C[k] >= 0) atomicAdd(&cnt[C[k]], 1);
+    const int j = blockIdx.x * COUNT_THREADS + threadIdx.x;
+    int c = -1;
+    if (j < it.nB) {
+        const float4 p = posq[slots[it.b0 + j]];
+        c = cellOf(p, box, nc);
+        it.cellId[j] = c;
+        it.posB[j] = p;
     }
-    __syncthreads();
-    if (tid == 0) {
-        int s = 0;
-        for (int c = 0; c < ncell; c++) {
-            it.cellStart[c] = s;
-            cursor[c] = s;
-            s += cnt[c];
-        }
-        it.cellStart[ncell] = s;
-        it.grid[0] = nc[0]; it.grid[1] = nc[1]; it.grid[2] = nc[2]; it.grid[3] = ncell;
+    const unsigned m = __match_any_sync(0xffffffffu, c);
+    if (c >= 0 && (m & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(it.counts + c, __popc(m));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        it.grid[0] = nc[0]; it.grid[1] = nc[1]; it.grid[2] = nc[2]; it.grid[3] = nc[0] * nc[1] * nc[2];
     }
-    __syncthreads();
-    // stable scatter, chunks of BIN_THREADS atoms in index order
-    const unsigned lt = (1u << lane) - 1u;
-    for (int g0 = 0; g0 < nB; g0 += GROUP) {
-        if (nB > GROUP) load(g0);   // one group: still in registers
+}
+
+// Binning, second step (one CTA per item): exclusive scan of the counts into
+// cellStart; the counts become the cells' write cursors.
+__global__ void __launch_bounds__(CELL_MAX) k_cell_scan(const CellItemDev* __restrict__ items) {
+    __shared__ int wsum[CELL_MAX / 32];
+    pdlEnter();
+    const CellItemDev& it = items[blockIdx.x];
+    const int ncell = it.grid[3];
+    const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
+    const int v = c < ncell ? it.counts[c] : 0;
+    int x = v;   // inclusive warp scan
 #pragma unroll
-        for (int k = 0; k < BIN_PER; k++) {
-            if (g0 + k * BIN_THREADS >= nB) break;   // uniform
-            const int c = C[k];
-            const unsigned m = __match_any_sync(0xffffffffu, c);
-            const bool leader = (m & lt) == 0;
-            if (c >= 0 && leader) wc[warp][c] = (unsigned char)__popc(m);
-            __syncthreads();
-            if (c >= 0) {
-                int cross = 0;
-                for (int w = 0; w < warp; w++) cross += wc[w][c];
-                const int slot = cursor[c] + cross + __popc(m & lt);
-                it.sortedB[slot] = g0 + k * BIN_THREADS + tid;
-                it.sortedPos[slot] = P[k];
-            }
-            __syncthreads();
-            if (c >= 0 && leader) {
-                atomicAdd(&cursor[c], __popc(m));
-                wc[warp][c] = 0;
-            }
-            __syncthreads();
-        }
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    const int start = before + x - v;
+    if (c < ncell) {
+        it.cellStart[c] = start;
+        it.counts[c] = start;
+    }
+    if (c == 0) it.cellStart[ncell] = it.nB;
+}
+
+// Binning, third step (one thread per B atom): each atom takes the next slot of
+// its cell (one atomic per distinct cell of a warp). The order within a cell
+// depends on the atomics' order; every sum the pairs kernel forms is in 64-bit
+// fixed point, so the results do not.
+__global__ void __launch_bounds__(COUNT_THREADS) k_cell_scatter(const CellItemDev* __restrict__ items) {
+    pdlEnter();
+    const CellItemDev& it = items[blockIdx.y];
+    const int j = blockIdx.x * COUNT_THREADS + threadIdx.x;
+    const int c = j < it.nB ? it.cellId[j] : -1;
+    const unsigned m = __match_any_sync(0xffffffffu, c);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (c >= 0 && lane == leader) base = atomicAdd(it.counts + c, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (c >= 0) {
+        const int slot = base + __popc(m & ((1u << lane) - 1u));
+        it.sortedB[slot] = j;
+        it.sortedPos[slot] = it.posB[j];
     }
 }
 
 // Warps (CELL_SPLIT w + z) of the grid take A atom w of the cell items
 // (item-major), z-slice z of its stencil (dz = z - 1; slices 1 and 2 are empty
-// when the box has one cell along z). Candidates pass a loose FP32 test first
-// (r^2 below rc^2 (1 + 1e-3) + 1e-6 L^2, far above the FP32 rounding of r^2);
-// the decision is then the FP64 one. EMIT: 0 evaluate; 1 pairCount[warp] = pairs
+// when the box has one cell along z). Every candidate's r^2 is formed in FP32
+// first; only those within a margin (1e-3 rc^2 + 1e-6 L^2, far above the FP32
+// rounding of r^2) of the cutoff or near the lower bound are decided in FP64,
+// the rest are inside or outside beyond any rounding, so the decisions are the
+// FP64 oracle's. Pair terms use the FP32 difference, or the FP64 one where it
+// was formed. EMIT: 0 evaluate; 1 pairCount[warp] = pairs
 // found; 2 write them as (a, b) at pairs[2 * (pairOffset[warp] + k)], in
 // candidate order.
 template <int NH, int EMIT>
@@ -189,6 +192,9 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
     int wi = 0;
     while (wi < numItems && a >= items[wi].nA) { a -= items[wi].nA; wi++; }
     pdlEnter();
+    if (blockIdx.x == 0)   // the binning of this step is complete: clear its counts for the next one
+        for (int i = 0; i < numItems; i++)
+            for (int k = threadIdx.x; k < CELL_MAX; k += blockDim.x) items[i].counts[k] = 0;
     if (wi >= numItems) return;   // warp-uniform
     const CellItemDev& it = items[wi];
     const CellBox box = *boxp;
@@ -207,9 +213,14 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
     const float fc0 = (float)box.c[0], fc1 = (float)box.c[1], fc2 = (float)box.c[2];
     const float fi0 = (float)box.inv[0], fi1 = (float)box.inv[1], fi2 = (float)box.inv[2];
     const double Lm = fmax(fmax(fabs(box.a[0]), fabs(box.b[1])), fabs(box.c[2]));
-    const float loose = (float)(rc2 * (1.0 + 1e-3) + 1e-6 * Lm * Lm);
-    double cn = 0.0;
-    float gx = 0.f, gy = 0.f, gz = 0.f;
+    // |FP32 r^2 - FP64 r^2| stays far below this margin (the FP32 rounding of a
+    // difference and its image is ~1e-7 L per component)
+    const double margin = rc2 * 1e-3 + 1e-6 * Lm * Lm;
+    const float sureIn = (float)(rc2 - margin), sureOut = (float)(rc2 + margin);
+    const float ir0f = 1.0f / it.r0;
+    // CN and A-gradient sums in 64-bit fixed point (value * 2^32): exact, so
+    // independent of the candidate order
+    long long cnq = 0, gqx = 0, gqy = 0, gqz = 0;
     int found = 0;
     long long out = EMIT == 2 ? pairOffset[gw] : 0;
     const bool sliceLive = nz >= 3 || zs == 0;
@@ -224,8 +235,7 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
                 for (int k0 = s; k0 < e; k0 += 32) {
                     const int k = k0 + lane;
                     bool in = false;
-                    D3 d = {0.0, 0.0, 0.0};
-                    double r2 = 0.0;
+                    float ex = 0.f, ey = 0.f, ez = 0.f, x2e = 0.f;   // the pair's scaled difference and x^2
                     if (k < e) {
                         const float4 pb = it.sortedPos[k];
                         float ux = pa.x - pb.x, uy = pa.y - pb.y, uz = pa.z - pb.z;
@@ -237,12 +247,22 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
                             const float s1 = floorf(fmaf(ux, fi0, 0.5f));
                             ux = fmaf(-s1, fa0, ux);
                         }
-                        if (fmaf(uz, uz, fmaf(uy, uy, ux * ux)) < loose) {
-                            d = {__dsub_rn(A.x, (double)pb.x), __dsub_rn(A.y, (double)pb.y),
-                                 __dsub_rn(A.z, (double)pb.z)};
+                        const float r2f = fmaf(uz, uz, fmaf(uy, uy, ux * ux));
+                        if (r2f < sureIn && r2f > 1e-10f) {
+                            // inside beyond any rounding: the FP64 decision is "in"
+                            in = true;
+                            ex = ux * ir0f; ey = uy * ir0f; ez = uz * ir0f;
+                            x2e = r2f * (ir0f * ir0f);
+                        } else if (r2f < sureOut) {
+                            // near the cutoff (or the lower bound): the decision in FP64
+                            D3 d = {__dsub_rn(A.x, (double)pb.x), __dsub_rn(A.y, (double)pb.y),
+                                    __dsub_rn(A.z, (double)pb.z)};
                             if (periodic) d = cellImage(d, box);
-                            r2 = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
+                            const double r2 =
+                                __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
                             in = !(r2 < 1e-20) && r2 < rc2;
+                            ex = (float)(d.x * ir0); ey = (float)(d.y * ir0); ez = (float)(d.z * ir0);
+                            x2e = (float)(r2 * ir02);
                         }
                     }
                     if (EMIT == 1) {
@@ -260,17 +280,18 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
                         continue;
                     }
                     if (in) {
-                        const float sx = (float)(d.x * ir0), sy = (float)(d.y * ir0), sz = (float)(d.z * ir0);
-                        const float x2 = (float)(r2 * ir02);
+                        const float sx = ex, sy = ey, sz = ez;
                         float f, h;
-                        switchX2<NH>(x2, true, K, f, h);
-                        cn += (double)f;
-                        const float hx = h * sx, hy = h * sy, hz = h * sz;
-                        gx += hx; gy += hy; gz += hz;
+                        switchX2<NH>(x2e, true, K, f, h);
+                        const long long qx = __float2ll_rn(h * sx * crun::FX);
+                        const long long qy = __float2ll_rn(h * sy * crun::FX);
+                        const long long qz = __float2ll_rn(h * sz * crun::FX);
+                        cnq += __float2ll_rn(f * crun::FX);
+                        gqx += qx; gqy += qy; gqz += qz;
                         unsigned long long* rb = acc + 3 * (size_t)(it.row0 + it.nA + it.sortedB[k]);
-                        redAddI64(rb, __float2ll_rn(-hx * crun::FX));
-                        redAddI64(rb + 1, __float2ll_rn(-hy * crun::FX));
-                        redAddI64(rb + 2, __float2ll_rn(-hz * crun::FX));
+                        redAddI64(rb, -qx);
+                        redAddI64(rb + 1, -qy);
+                        redAddI64(rb + 2, -qz);
                     }
                 }
             }
@@ -279,16 +300,22 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
         return;
     }
     if (EMIT == 2) return;
-    gx = warpSumF(gx); gy = warpSumF(gy); gz = warpSumF(gz);
-    cn = warpSum(cn);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gqx += __shfl_xor_sync(0xffffffffu, gqx, o);
+        gqy += __shfl_xor_sync(0xffffffffu, gqy, o);
+        gqz += __shfl_xor_sync(0xffffffffu, gqz, o);
+        cnq += __shfl_xor_sync(0xffffffffu, cnq, o);
+    }
     if (lane == 0) {
         if (sliceLive) {
             unsigned long long* ra = acc + 3 * (size_t)(it.row0 + a);
-            redAddI64(ra, __float2ll_rn(gx * crun::FX));
-            redAddI64(ra + 1, __float2ll_rn(gy * crun::FX));
-            redAddI64(ra + 2, __float2ll_rn(gz * crun::FX));
+            redAddI64(ra, gqx);
+            redAddI64(ra + 1, gqy);
+            redAddI64(ra + 2, gqz);
         }
-        cnPiece[it.pieceBegin + CELL_SPLIT * a + zs] = cn;   // every slot written, empty slices 0
+        // every slot written (empty slices 0); exact: |cnq| < 2^53
+        cnPiece[it.pieceBegin + CELL_SPLIT * a + zs] = (double)cnq * crun::IFXD;
     }
 }
 
@@ -308,19 +335,30 @@ static void launchPairs(cudaStream_t s, int kind, int totalA, const CellItemDev*
                   pairOffset, pairs);
 }
 
-void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
+// maxB: the largest B group of the items
+static void launchBin(cudaStream_t s, const CellItemDev* items, int numItems, int maxB, const int* slots,
+                      const float4* posq, const CellBox* box) {
+    const dim3 grid((unsigned)((std::max(1, maxB) + COUNT_THREADS - 1) / COUNT_THREADS), numItems);
+    launchPdl(k_cell_count, grid, dim3(COUNT_THREADS), 0, s, items, slots, posq, box);
+    launchPdl(k_cell_scan, dim3(numItems), dim3(CELL_MAX), 0, s, items);
+    launchPdl(k_cell_scatter, grid, dim3(COUNT_THREADS), 0, s, items);
+}
+
+void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
+                     const int* slots,
                      const float4* posq, const CellBox* box, unsigned long long* acc, double* cnPiece) {
     if (numItems == 0 || totalA == 0) return;
-    launchPdl(k_cell_bin, dim3(numItems), dim3(BIN_THREADS), 0, s, items, slots, posq, box);
+    launchBin(s, items, numItems, maxB, slots, posq, box);
     launchPairs<0>(s, kind, totalA, items, numItems, slots, posq, box, acc, cnPiece, nullptr, nullptr, nullptr);
 }
 
-void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
+void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
+                        const int* slots,
                         const float4* posq, const CellBox* box, int* pairCount, const long long* pairOffset,
                         int* pairs, int pass) {
     if (numItems == 0 || totalA == 0) return;
     if (pass == 1) {
-        launchPdl(k_cell_bin, dim3(numItems), dim3(BIN_THREADS), 0, s, items, slots, posq, box);
+        launchBin(s, items, numItems, maxB, slots, posq, box);
         launchPairs<1>(s, kind, totalA, items, numItems, slots, posq, box, nullptr, nullptr, pairCount, nullptr,
                        nullptr);
     } else {

@@ -23,6 +23,7 @@
 //           window (CommonGluedKernels.cpp:983-1003);
 //   0     : non-integer exponents: the reference formula (pow, Taylor branch).
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -70,14 +71,18 @@ __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* 
         out[it.jac0 + (row - base)] = (float)((double)v * crun::IFXD * coordAccScale(it));
     }
     if (blockIdx.x == 0) {
-        // one warp per item: lane l sums the item's pieces l, l + 32, ... (step
-        // order), then a fixed xor tree
-        const int lane = threadIdx.x & 31;
-        for (int i = threadIdx.x >> 5; i < numItems; i += blockDim.x >> 5) {
+        // CN of each item: thread t sums the item's pieces t, t + 256, ... (in
+        // order), then the fixed block tree (a cell-list item has 3 per A atom)
+        __shared__ double red[32];
+        for (int i = 0; i < numItems; i++) {
             double t = 0.0;
-            for (int k = R.items[i].pieceBegin + lane; k < R.items[i].pieceEnd; k += 32) t += R.cnPiece[k];
-            t = warpSum(t);
-            if (lane == 0) cvv[R.items[i].cv] = t;
+#pragma unroll 8
+            for (int k = R.items[i].pieceBegin + (int)threadIdx.x; k < R.items[i].pieceEnd; k += blockDim.x)
+                t += R.cnPiece[k];
+            double v[1] = {t};
+            blockSum<1>(v, red);
+            if (threadIdx.x == 0) cvv[R.items[i].cv] = v[0];
+            __syncthreads();
         }
     }
 }
@@ -124,16 +129,21 @@ void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int
     if (n > 0) k_step_gathers<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(steps, numSteps, grid, slots, gB, gA, ta, ch);
 }
 
+// The dynamic shared-memory limit is a per-function maximum: it only ever grows
+// (a smaller request after a larger one must not lower it under a batch that
+// still launches with the larger size).
 void runKernelSetup(const void* fn, size_t dynSmem) {
     static std::mutex mu;
-    static std::set<std::pair<std::pair<const void*, int>, size_t>> done;
+    static std::map<std::pair<const void*, int>, size_t> limit;
     int dev = 0;
     cudaCheck(cudaGetDevice(&dev), "device");
     std::lock_guard<std::mutex> lock(mu);
-    if (!done.insert({{fn, dev}, dynSmem}).second) return;
+    auto it = limit.find({fn, dev});
+    if (it != limit.end() && it->second >= dynSmem) return;
     cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    (int)cudaSharedmemCarveoutMaxShared), "carveout");
     cudaCheck(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynSmem), "smem");
+    limit[{fn, dev}] = dynSmem;
 }
 
 template <int RA, int BOX, int NH, bool HI, bool BLK>

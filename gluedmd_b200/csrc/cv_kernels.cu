@@ -117,22 +117,27 @@ __global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restr
 // ---------------------------------------------------------------- group CVs
 
 // Jacobi eigen-decomposition of a symmetric 4x4 in FP64 (quaternion RMSD).
-// Cyclic Jacobi on a symmetric 4x4 (FP64). Every index is a compile-time
-// constant (unrolled p, q, k loops), so A and V stay in registers; with runtime
-// indices they lived in local memory and the eigensolve of one Kabsch CV took
-// tens of microseconds.
+// Cyclic Jacobi on a symmetric 4x4 (FP64), until the off-diagonal part is below
+// 1e-12 of the matrix norm. Every index is a compile-time constant (unrolled p,
+// q, k loops), so A and V stay in registers.
 __device__ __forceinline__ void jacobi4(double (&A)[4][4], double (&V)[4][4], double (&w)[4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 64; sweep++) {
-        double off = 0;
+        double off = 0, dia = 0;
 #pragma unroll
-        for (int p = 0; p < 4; p++)
+        for (int p = 0; p < 4; p++) {
+            dia += A[p][p] * A[p][p];
 #pragma unroll
             for (int q = p + 1; q < 4; q++) off += A[p][q] * A[p][q];
-        if (off < 1e-30) break;
+        }
+        // converged relative to the matrix: off-diagonal entries below 1e-12 of
+        // the norm put the eigenvalues within ~1e-24 and the eigenvectors within
+        // ~1e-12 (relative) of exact; a bound at FP64 resolution itself may never
+        // be met, and then every sweep runs
+        if (off <= 1e-24 * dia || off < 1e-300) break;
 #pragma unroll
         for (int p = 0; p < 4; p++)
 #pragma unroll

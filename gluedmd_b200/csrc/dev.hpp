@@ -130,6 +130,9 @@ struct CellItemDev {
     int* sortedB;           // [nB]: B atom (0 .. nB - 1) of every sorted position
     float4* sortedPos;      // [nB]: its position
     int* grid;              // [4]: cells per dimension of the last binning, and their product
+    int* cellId;            // [nB]: cell of every B atom (binning scratch)
+    float4* posB;           // [nB]: its position (binning scratch)
+    int* counts;            // [CELL_MAX]: atoms per cell (zero between steps)
 };
 
 // Coordination as static per-CTA runs of (A tile, B chunk) steps (coord_run.cuh).

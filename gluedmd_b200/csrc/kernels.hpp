@@ -38,11 +38,12 @@ int coordRunOccupancy(int kind, int boxKind, bool hi);
 // launchCoord. launchCellPairList: pass 1 bins and counts the pairs of every warp
 // (CELL_SPLIT per A atom: pairCount[CELL_SPLIT * totalA]); pass 2 writes them
 // at pairOffset (int pairs (a, b)).
-void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
-                     const float4* posq, const CellBox* box, unsigned long long* acc, double* cnPiece);
-void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int kind, const int* slots,
-                        const float4* posq, const CellBox* box, int* pairCount, const long long* pairOffset,
-                        int* pairs, int pass);
+void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
+                     const int* slots, const float4* posq, const CellBox* box, unsigned long long* acc,
+                     double* cnPiece);
+void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
+                        const int* slots, const float4* posq, const CellBox* box, int* pairCount,
+                        const long long* pairOffset, int* pairs, int pass);
 // Once per (kernel, device, size): maximum shared-memory carveout and the
 // dynamic shared-memory limit of a persistent runs kernel.
 void runKernelSetup(const void* fn, size_t dynSmem);
@@ -73,6 +74,10 @@ void launchOpesDeposit(cudaStream_t s, const BiasDev* b, const double* cvv, cons
                        int* mergeFlag, double* partial, int nPartial);
 
 double measureFp32Peak();
+// Hill-slice staging alone (staging_probe.cu): mean microseconds per launch of
+// ctas CTAs staging equal slices of a numHills table with 16-byte cp.async and
+// with bulk copies; status bit 0: a bulk-copy wait gave up.
+void measureHillStaging(int numHills, int ctas, int reps, double* usCpAsync, double* usBulk, int* status);
 void adForward(int dtype, cudaStream_t st, const glued_ad_spec& S, double* out, double* part, int nPart);
 void adBackward(int dtype, cudaStream_t st, const glued_ad_spec& S, const double* out, const double* gE,
                 long long* acc, void* gPos, void* gR0, void* gFrames, void* gH);

@@ -160,6 +160,12 @@ int glued_context_launch_count(glued_context* c, long long* count);
 /* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 flops),
  * measured with a register-resident FMA-chain kernel (synchronizing).         */
 int glued_measure_fp32_peak(double* tflops);
+/* Hill-slice staging probe (synchronizing): ctas CTAs each copy an equal slice of
+ * the three float arrays of a num_hills table into shared memory, timed alone
+ * after an L2 flush, reps launches per form: out[0] = us per launch with 16-byte
+ * cp.async copies, out[1] = with one bulk copy (cp.async.bulk, mbarrier
+ * completion, no multicast) per array; *status bit 0: a bulk wait gave up.     */
+int glued_measure_hill_staging(int num_hills, int ctas, int reps, double out[2], int* status);
 /* Test hook: index of the last OPES deposit decision of OPES bias opes_index
  * (>= 0 merged into that kernel, -1 appended, -2 warm-up skip, -3 table full).  */
 int glued_context_opes_last_decision(glued_context* c, int opes_index, int* decision);

@@ -126,7 +126,7 @@ def test_batch_tile_shapes_agree(ra, ch):
     np.testing.assert_allclose(cv1, cv0, rtol=1e-7)
     np.testing.assert_allclose(e1, e0, rtol=1e-6, atol=1e-9)
     for i, w in enumerate(ws):
-        r = _oracle(w, specs[i], hill)
+        r = _oracle(w, specs[i], hill).execute(w["pos"], w["box"].ravel())
         assert O.max_rel_force_err(f1[i], r["forces"]) < 1e-4, i
     assert b.status() == 0
 
