@@ -117,57 +117,138 @@ __global__ void k_simple_cvs(const float4* __restrict__ posq, const int* __restr
 // ---------------------------------------------------------------- group CVs
 
 // Jacobi eigen-decomposition of a symmetric 4x4 in FP64 (quaternion RMSD).
-// Cyclic Jacobi on a symmetric 4x4 (FP64), until the off-diagonal part is below
-// 1e-12 of the matrix norm. Every index is a compile-time constant (unrolled p,
-// q, k loops), so A and V stay in registers.
-__device__ __forceinline__ void jacobi4(double (&A)[4][4], double (&V)[4][4], double (&w)[4]) {
+// Largest eigenvalue and a unit eigenvector of a symmetric, traceless 4x4 F
+// (the quaternion key matrix of optimal superposition), in FP64 on one thread:
+//   - lambda by Newton on the characteristic polynomial
+//     P(l) = l^4 - (tr F^2 / 2) l^2 - (tr F^3 / 3) l + det F, started at an upper
+//     bound `upper` of the spectrum, from which it descends monotonically to the
+//     largest root;
+//   - the eigenvector by two steps of inverse iteration with (F - mu I), mu
+//     just above lambda (Gaussian elimination with partial pivoting), which
+//     also serves a nearly double largest eigenvalue;
+//   - lambda again as the Rayleigh quotient of that vector.
+// A handful of divisions in all, against about 200 divisions and square roots
+// of a cyclic Jacobi solve, whose serial latency was ~10 us per Kabsch CV.
+__device__ __forceinline__ void maxEigen4(const double (&F)[4][4], double upper, double& lam, double (&v)[4]) {
+    double p2 = 0.0, p3 = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 64; sweep++) {
-        double off = 0, dia = 0;
+        for (int j = 0; j < 4; j++) {
+            double f2 = 0.0;
 #pragma unroll
-        for (int p = 0; p < 4; p++) {
-            dia += A[p][p] * A[p][p];
-#pragma unroll
-            for (int q = p + 1; q < 4; q++) off += A[p][q] * A[p][q];
+            for (int k = 0; k < 4; k++) f2 += F[i][k] * F[k][j];
+            p2 += F[i][j] * F[j][i];
+            p3 += F[i][j] * f2;   // (F F^2)_ii summed: tr F^3 (F symmetric)
         }
-        // converged relative to the matrix: off-diagonal entries below 1e-12 of
-        // the norm put the eigenvalues within ~1e-24 and the eigenvectors within
-        // ~1e-12 (relative) of exact; a bound at FP64 resolution itself may never
-        // be met, and then every sweep runs
-        if (off <= 1e-24 * dia || off < 1e-300) break;
+    // det F by elimination with partial pivoting on a copy
+    double M[4][4];
 #pragma unroll
-        for (int p = 0; p < 4; p++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int q = p + 1; q < 4; q++) {
-                if (fabs(A[p][q]) < 1e-300) continue;
-                const double th = (A[q][q] - A[p][p]) / (2 * A[p][q]);
-                const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
-                const double c = 1 / sqrt(t * t + 1), s = t * c;
+        for (int j = 0; j < 4; j++) M[i][j] = F[i][j];
+    double det = 1.0;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const double x = A[k][p], y = A[k][q];
-                    A[k][p] = c * x - s * y;
-                    A[k][q] = s * x + c * y;
-                }
+    for (int c = 0; c < 4; c++) {
+        int piv = c;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const double x = A[p][k], y = A[q][k];
-                    A[p][k] = c * x - s * y;
-                    A[q][k] = s * x + c * y;
-                }
+        for (int r = c + 1; r < 4; r++)
+            if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+        if (piv != c) {
+            det = -det;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const double x = V[k][p], y = V[k][q];
-                    V[k][p] = c * x - s * y;
-                    V[k][q] = s * x + c * y;
-                }
+            for (int j = 0; j < 4; j++) {
+                // swap rows c and piv with compile-time row indices only
+                double a = M[c][j], b = 0.0;
+#pragma unroll
+                for (int r = c + 1; r < 4; r++) b = (r == piv) ? M[r][j] : b;
+                M[c][j] = b;
+#pragma unroll
+                for (int r = c + 1; r < 4; r++)
+                    if (r == piv) M[r][j] = a;
             }
-    }
+        }
+        const double d = M[c][c];
+        det *= d;
+        if (d != 0.0) {
+            const double id = 1.0 / d;
 #pragma unroll
-    for (int i = 0; i < 4; i++) w[i] = A[i][i];
+            for (int r = c + 1; r < 4; r++) {
+                const double f = M[r][c] * id;
+#pragma unroll
+                for (int j = c; j < 4; j++) M[r][j] -= f * M[c][j];
+            }
+        }
+    }
+    const double c2 = -0.5 * p2, c1 = -p3 / 3.0, c0 = det;
+    double l = upper;
+    for (int it = 0; it < 100; it++) {
+        const double P = ((l * l + c2) * l + c1) * l + c0;
+        const double dP = (4.0 * l * l + 2.0 * c2) * l + c1;
+        if (!(dP > 0.0)) break;
+        const double step = P / dP;
+        l -= step;
+        if (fabs(step) <= 1e-15 * fabs(l) + 1e-300) break;
+    }
+    // inverse iteration with mu slightly above lambda
+    const double mu = l + 1e-12 * (fabs(l) + fabs(upper)) + 1e-300;
+    double x[4] = {1.0, 1.0, 1.0, 1.0};
+    for (int rep = 0; rep < 2; rep++) {
+        double A[4][5];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) A[i][j] = F[i][j] - (i == j ? mu : 0.0);
+            A[i][4] = x[i];
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int piv = c;
+#pragma unroll
+            for (int r = c + 1; r < 4; r++)
+                if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                double a = A[c][j], b = a;
+#pragma unroll
+                for (int r = c + 1; r < 4; r++) b = (r == piv) ? A[r][j] : b;
+                A[c][j] = b;
+#pragma unroll
+                for (int r = c + 1; r < 4; r++)
+                    if (r == piv) A[r][j] = a;
+            }
+            const double d = A[c][c] != 0.0 ? A[c][c] : 1e-300;
+            const double id = 1.0 / d;
+#pragma unroll
+            for (int r = c + 1; r < 4; r++) {
+                const double f = A[r][c] * id;
+#pragma unroll
+                for (int j = c; j < 5; j++) A[r][j] -= f * A[c][j];
+            }
+        }
+        double y[4];
+#pragma unroll
+        for (int c = 3; c >= 0; c--) {
+            double t = A[c][4];
+#pragma unroll
+            for (int j = c + 1; j < 4; j++) t -= A[c][j] * y[j];
+            y[c] = t / (A[c][c] != 0.0 ? A[c][c] : 1e-300);
+        }
+        const double n = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+        const double in = n > 0.0 ? 1.0 / n : 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[i] = y[i] * in;
+    }
+    double rq = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        double fx = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) fx += F[i][j] * x[j];
+        rq += x[i] * fx;
+        v[i] = x[i];
+    }
+    lam = rq;
 }
 
 // Positions of the group atoms [a0, a1) are gathered once into shared memory
@@ -395,7 +476,7 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
         if (tid == 0) cvv[it.cv] = q[0];
     } else if (it.type == CV_RMSD_KABSCH) {
         // Optimal superposition RMSD: FP64 centroids and correlation matrix, the
-        // quaternion 4x4 eigenproblem solved in FP64 by one thread.
+        // quaternion 4x4 eigenproblem solved in FP64 by one thread (maxEigen4).
         const int na = it.s1 - it.s0;
         double v[6] = {0, 0, 0, 0, 0, 0};
         for (int j = it.s0 + tid; j < it.s1; j += nt) {
@@ -421,13 +502,11 @@ __global__ void __launch_bounds__(GROUP_THREADS) k_group_cvs(const float4* __res
                 {R[1][2] - R[2][1], R[0][0] - R[1][1] - R[2][2], R[0][1] + R[1][0], R[0][2] + R[2][0]},
                 {R[2][0] - R[0][2], R[0][1] + R[1][0], -R[0][0] + R[1][1] - R[2][2], R[1][2] + R[2][1]},
                 {R[0][1] - R[1][0], R[0][2] + R[2][0], R[1][2] + R[2][1], -R[0][0] - R[1][1] + R[2][2]}};
-            double V[4][4], w[4];
-            jacobi4(F, V, w);
-            // largest eigenvalue and its eigenvector, selected without a runtime index
-            double wm = w[0], q0 = V[0][0], q1 = V[1][0], q2 = V[2][0], q3 = V[3][0];
-#pragma unroll
-            for (int i = 1; i < 4; i++)
-                if (w[i] > wm) { wm = w[i]; q0 = V[0][i]; q1 = V[1][i]; q2 = V[2][i]; q3 = V[3][i]; }
+            // largest eigenvalue (bounded above by (sum |x|^2 + sum |y|^2) / 2) and its
+            // eigenvector
+            double wm, q[4];
+            maxEigen4(F, 0.5 * c[9], wm, q);
+            const double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
             // q rotates x onto y (correlation x y^T); bc[0..8] is its transpose,
             // the rotation that takes the reference y onto x
             bc[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3; bc[1] = 2 * (q1 * q2 + q0 * q3); bc[2] = 2 * (q1 * q3 - q0 * q2);
