@@ -425,6 +425,7 @@ void Context::buildPlan(const GluedForce& f) {
         coordSysPosq_.alloc(sizeof(const float4*));
         coordAcc_.alloc(sizeof(unsigned long long) * 3 * std::max(1, coordRows_));
         coordCnPiece_.alloc(sizeof(double) * std::max(1, pieces));
+        coordCellCn_.alloc(sizeof(unsigned long long) * coord.size());
         cudaCheck(cudaMemset(coordAcc_.p, 0, coordAcc_.bytes), "coord acc");
         // cell-list items: scratch carved from one allocation, 256-byte aligned pieces
         cellItemsH_.clear();
@@ -450,7 +451,7 @@ void Context::buildPlan(const GluedForce& f) {
                             carve(sizeof(int) * CELL_MAX)});
             CellItemDev ci{};
             ci.item = (int)i; ci.a0 = it.a0; ci.nA = it.nA; ci.b0 = it.b0; ci.nB = it.nB;
-            ci.row0 = it.row0; ci.pieceBegin = it.pieceBegin;
+            ci.row0 = it.row0;
             ci.r0 = it.r0; ci.n = it.n; ci.m = it.m;
             ci.rc = coordRc[i];
             ci.rc2 = coordRc[i] * coordRc[i];
@@ -475,6 +476,8 @@ void Context::buildPlan(const GluedForce& f) {
                 cellItemsH_[k].posB = reinterpret_cast<float4*>(base + offs[k][5]);
                 cellItemsH_[k].counts = reinterpret_cast<int*>(base + offs[k][6]);
             }
+            for (int k = 0; k < cellItemsN_; k++)
+                cellItemsH_[k].cn = coordCellCn_.as<unsigned long long>() + cellItemsH_[k].item;
             cellItems_.upload(cellItemsH_);
             CellBox cb{};
             cb.kind = 0;
@@ -492,6 +495,7 @@ void Context::buildPlan(const GluedForce& f) {
         R_.sysBox = box_.as<BoxDev>();
         R_.acc = coordAcc_.as<unsigned long long>();
         R_.cnPiece = coordCnPiece_.as<double>();
+        R_.cellCn = coordCellCn_.as<unsigned long long>();
     }
 }
 
@@ -835,9 +839,8 @@ void Context::enqueueExecute(cudaStream_t s, bool includeForces, int onlyPhase) 
 
 void Context::enqueueCells(cudaStream_t s) {
     launchCellCoord(s, cellItems_.as<CellItemDev>(), cellEvalN_, cellEvalA_, cellEvalMaxB_, coordKind_,
-                    coordSlots_.as<int>(),
-                    static_cast<const float4*>(posq_), cellBox_.as<CellBox>(), coordAcc_.as<unsigned long long>(),
-                    coordCnPiece_.as<double>());
+                    coordSlots_.as<int>(), static_cast<const float4*>(posq_), cellBox_.as<CellBox>(),
+                    coordAcc_.as<unsigned long long>());
 }
 
 std::vector<int> Context::cellPairs(int cvIndex) {

@@ -126,7 +126,7 @@ private:
     DBuf simple_, groupItems_, gAtoms_, gSlots_, gMass_, gRef_, gEv_, cmPairs_, cmParams_;
     int gAtomsN_ = 0, groupCached_ = 1;
     DBuf coordItems_, coordAtoms_, coordSlots_, coordSteps_, coordGB_, coordGA_, coordStepPosq_, coordAcc_, coordCnPiece_;
-    DBuf coordSysPosq_;
+    DBuf coordSysPosq_, coordCellCn_;
     DBuf biasDev_, mergeFlag_, uprobPartial_, sumPart_;
     bool kernelSums_ = false;
     bool groupClustered_ = false;   // group CVs as one CTA cluster per CV

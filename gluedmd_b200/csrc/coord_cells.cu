@@ -28,10 +28,10 @@
 // k_cell_pairs (CELL_SPLIT warps per A atom, one z slice of the stencil each)
 // visits the slice's cells, lanes striding over each cell's atoms. Every pair
 // term (switch value, gradient components) is converted to 64-bit fixed point
-// (value * 2^32) and summed exactly: the CN partial of the (A atom, slice) goes
-// to its own cnPiece slot (the finalize adds the item's slots in order), the A
-// sums and every B term to the fixed-point accumulator rows, as on the tile
-// path, so k_coord_finalize turns them into Jacobian rows unchanged. EMIT = 1
+// (value * 2^32) and summed exactly: the CN per CTA into the item's one CN
+// accumulator (k_coord_finalize converts and clears it), the A sums and every B
+// term to the fixed-point accumulator rows, as on the tile path, so
+// k_coord_finalize turns them into Jacobian rows unchanged. EMIT = 1
 // counts the pairs of every warp, EMIT = 2 writes them (test and diagnostic
 // use; the host sorts the list).
 #include <algorithm>
@@ -182,7 +182,7 @@ template <int NH, int EMIT>
 __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restrict__ items, int numItems,
                                                     const int* __restrict__ slots, const float4* __restrict__ posq,
                                                     const CellBox* __restrict__ boxp, unsigned long long* __restrict__ acc,
-                                                    double* __restrict__ cnPiece, int* __restrict__ pairCount,
+                                                    int* __restrict__ pairCount,
                                                     const long long* __restrict__ pairOffset,
                                                     int* __restrict__ pairs) {
     const int lane = threadIdx.x & 31;
@@ -195,7 +195,9 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
     if (blockIdx.x == 0)   // the binning of this step is complete: clear its counts for the next one
         for (int i = 0; i < numItems; i++)
             for (int k = threadIdx.x; k < CELL_MAX; k += blockDim.x) items[i].counts[k] = 0;
-    if (wi >= numItems) return;   // warp-uniform
+    const bool live = wi < numItems;   // warp-uniform
+    if (!live && EMIT != 0) return;   // (the EMIT passes have no CTA barrier)
+    if (!live) { wi = 0; a = 0; }     // evaluates nothing, joins the CTA's CN reduction
     const CellItemDev& it = items[wi];
     const CellBox box = *boxp;
     const float4 pa = posq[slots[it.a0 + a]];
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
     long long cnq = 0, gqx = 0, gqy = 0, gqz = 0;
     int found = 0;
     long long out = EMIT == 2 ? pairOffset[gw] : 0;
-    const bool sliceLive = nz >= 3 || zs == 0;
+    const bool sliceLive = live && (nz >= 3 || zs == 0);
     const int dz = nz >= 3 ? zs - 1 : 0;
     const int oy = ny >= 3 ? -1 : 0, ey = ny >= 3 ? 1 : 0;
     const int ox = nx >= 3 ? -1 : 0, ex = nx >= 3 ? 1 : 0;
@@ -307,6 +309,9 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
         gqz += __shfl_xor_sync(0xffffffffu, gqz, o);
         cnq += __shfl_xor_sync(0xffffffffu, cnq, o);
     }
+    __shared__ long long sCn[8];
+    __shared__ int sItem[8];
+    const int warp = threadIdx.x >> 5;
     if (lane == 0) {
         if (sliceLive) {
             unsigned long long* ra = acc + 3 * (size_t)(it.row0 + a);
@@ -314,24 +319,39 @@ __global__ void __launch_bounds__(256) k_cell_pairs(const CellItemDev* __restric
             redAddI64(ra + 1, gqy);
             redAddI64(ra + 2, gqz);
         }
-        // every slot written (empty slices 0); exact: |cnq| < 2^53
-        cnPiece[it.pieceBegin + CELL_SPLIT * a + zs] = (double)cnq * crun::IFXD;
+        sCn[warp] = cnq;
+        sItem[warp] = sliceLive ? wi : -1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // one fixed-point CN addition per (CTA, item): integer, so order-independent
+        long long run = 0;
+        int cur = -1;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            if (sItem[w] != cur) {
+                if (cur >= 0) redAddI64(items[cur].cn, run);
+                cur = sItem[w];
+                run = 0;
+            }
+            run += sCn[w];
+        }
+        if (cur >= 0) redAddI64(items[cur].cn, run);
     }
 }
 
 template <int EMIT>
 static void launchPairs(cudaStream_t s, int kind, int totalA, const CellItemDev* items, int numItems,
                         const int* slots, const float4* posq, const CellBox* box, unsigned long long* acc,
-                        double* cnPiece, int* pairCount, const long long* pairOffset, int* pairs) {
+                        int* pairCount, const long long* pairOffset, int* pairs) {
     const dim3 grid((unsigned)((CELL_SPLIT * (long long)totalA * 32 + 255) / 256)), block(256);
     if (kind == 3)
-        launchPdl(k_cell_pairs<3, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc, cnPiece, pairCount,
+        launchPdl(k_cell_pairs<3, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc, pairCount,
                   pairOffset, pairs);
     else if (kind == -1)
-        launchPdl(k_cell_pairs<-1, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc, cnPiece,
+        launchPdl(k_cell_pairs<-1, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc,
                   pairCount, pairOffset, pairs);
     else
-        launchPdl(k_cell_pairs<0, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc, cnPiece, pairCount,
+        launchPdl(k_cell_pairs<0, EMIT>, grid, block, 0, s, items, numItems, slots, posq, box, acc, pairCount,
                   pairOffset, pairs);
 }
 
@@ -346,10 +366,10 @@ static void launchBin(cudaStream_t s, const CellItemDev* items, int numItems, in
 
 void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
                      const int* slots,
-                     const float4* posq, const CellBox* box, unsigned long long* acc, double* cnPiece) {
+                     const float4* posq, const CellBox* box, unsigned long long* acc) {
     if (numItems == 0 || totalA == 0) return;
     launchBin(s, items, numItems, maxB, slots, posq, box);
-    launchPairs<0>(s, kind, totalA, items, numItems, slots, posq, box, acc, cnPiece, nullptr, nullptr, nullptr);
+    launchPairs<0>(s, kind, totalA, items, numItems, slots, posq, box, acc, nullptr, nullptr, nullptr);
 }
 
 void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
@@ -359,11 +379,9 @@ void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, 
     if (numItems == 0 || totalA == 0) return;
     if (pass == 1) {
         launchBin(s, items, numItems, maxB, slots, posq, box);
-        launchPairs<1>(s, kind, totalA, items, numItems, slots, posq, box, nullptr, nullptr, pairCount, nullptr,
-                       nullptr);
+        launchPairs<1>(s, kind, totalA, items, numItems, slots, posq, box, nullptr, pairCount, nullptr, nullptr);
     } else {
-        launchPairs<2>(s, kind, totalA, items, numItems, slots, posq, box, nullptr, nullptr, nullptr, pairOffset,
-                       pairs);
+        launchPairs<2>(s, kind, totalA, items, numItems, slots, posq, box, nullptr, nullptr, pairOffset, pairs);
     }
 }
 

@@ -72,11 +72,18 @@ __global__ void k_coord_finalize(CoordRunDev R, int numItems, JacDev J, double* 
     }
     if (blockIdx.x == 0) {
         // CN of each item: thread t sums the item's pieces t, t + 256, ... (in
-        // order), then the fixed block tree (a cell-list item has 3 per A atom)
+        // order), then the fixed block tree
         __shared__ double red[32];
         for (int i = 0; i < numItems; i++) {
+            if (R.items[i].cells) {
+                // cell-list item: one exact fixed-point sum
+                if (threadIdx.x == 0) {
+                    cvv[R.items[i].cv] = (double)(long long)R.cellCn[i] * crun::IFXD;
+                    R.cellCn[i] = 0ull;
+                }
+                continue;
+            }
             double t = 0.0;
-#pragma unroll 8
             for (int k = R.items[i].pieceBegin + (int)threadIdx.x; k < R.items[i].pieceEnd; k += blockDim.x)
                 t += R.cnPiece[k];
             double v[1] = {t};

@@ -63,7 +63,6 @@ int buildCoordPieces(std::vector<CoordStep>& steps, const std::vector<int>& begi
     for (size_t i = 0; i < items.size(); i++) {
         std::sort(per[i].begin(), per[i].end());
         items[i].pieceBegin = slot;
-        if (items[i].cells) slot += CELL_SPLIT * items[i].nA;   // partials of the A atoms' stencil slices
         for (int s : per[i]) steps[s].pieceSlot = slot++;
         items[i].pieceEnd = slot;
     }

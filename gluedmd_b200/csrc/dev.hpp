@@ -92,7 +92,7 @@ struct CoordItem {
     int row0;       // first fixed-point accumulator row (A rows, then B rows)
     int pieceBegin, pieceEnd;   // this item's run-piece CN partials in cnPiece
     int cells;      // 1: cutoff item evaluated by the cell-list path (coord_cells.cu):
-                    // no tile steps; one CN partial per A atom in cnPiece
+                    // no tile steps, no run pieces; its CN is summed in CoordRunDev::cellCn
 };
 
 struct CoordDev {
@@ -117,12 +117,13 @@ struct CellBox {
 
 constexpr int CELL_MAX_DIM = 8;                      // cells per box dimension at most
 constexpr int CELL_MAX = CELL_MAX_DIM * CELL_MAX_DIM * CELL_MAX_DIM;
-constexpr int CELL_SPLIT = 3;   // warps per A atom (one per z slice of the stencil); CN partials per A atom
+constexpr int CELL_SPLIT = 3;   // warps per A atom (one per z slice of the stencil)
 
 struct CellItemDev {
     int item;               // coordination item (accumulator rows, CN partials)
     int a0, nA, b0, nB;     // into the coordination atom slots
-    int row0, pieceBegin;   // first accumulator row (A rows, then B rows); first CN partial
+    int row0;               // first accumulator row (A rows, then B rows)
+    unsigned long long* cn; // the item's CN accumulator (CoordRunDev::cellCn), 64-bit fixed point
     float r0, n, m;
     double rc2;             // rc * rc in FP64
     double rc;
@@ -177,6 +178,7 @@ struct CoordRunDev {
     const BoxDev* sysBox;      // box of system CoordStep::sys
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
     double* cnPiece;           // CN partial of every run piece, item-contiguous (CoordItem::pieceBegin/End)
+    unsigned long long* cellCn;  // [items]: CN of cell-list items in 64-bit fixed point (cleared by the reader)
 };
 
 // Equal static ranges of the coordination steps: CTA b of a grid of G runs

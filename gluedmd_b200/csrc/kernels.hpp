@@ -34,13 +34,13 @@ void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int
                        int* gA, int ta = COORD_TA, int ch = COORD_CH);
 int coordRunOccupancy(int kind, int boxKind, bool hi);
 // Cutoff coordination items on the cell-list path (coord_cells.cu): bin the B
-// atoms, then pair terms into acc / cnPiece (before k_coord_finalize). kind as
+// atoms, then pair terms into acc and the items' CN accumulators (before
+// k_coord_finalize). kind as
 // launchCoord. launchCellPairList: pass 1 bins and counts the pairs of every warp
 // (CELL_SPLIT per A atom: pairCount[CELL_SPLIT * totalA]); pass 2 writes them
 // at pairOffset (int pairs (a, b)).
 void launchCellCoord(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
-                     const int* slots, const float4* posq, const CellBox* box, unsigned long long* acc,
-                     double* cnPiece);
+                     const int* slots, const float4* posq, const CellBox* box, unsigned long long* acc);
 void launchCellPairList(cudaStream_t s, const CellItemDev* items, int numItems, int totalA, int maxB, int kind,
                         const int* slots, const float4* posq, const CellBox* box, int* pairCount,
                         const long long* pairOffset, int* pairs, int pass);
