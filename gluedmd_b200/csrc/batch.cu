@@ -722,7 +722,7 @@ struct Batch::Impl {
     std::vector<int> coordAtoms;
     std::vector<CoordStep> steps;
     DBuf walkersD, simpleD, harmD, itemsD, atomsD, stepsD, gBD, gAD, stepPosqD, boxesD, sysPosqD, acc, cnPiece;
-    DBuf hillCvPosD, hillCvTypeD, rowAtomD;
+    DBuf hillCvPosD, hillCvTypeD, rowAtomD, stepConstD;
     std::vector<BSimple> simpleH;
     DBuf hillPart, cvv, energy, hillEnergy, status, scratchForce;
     DBuf hMirror, hCenters, hHeights, hCount;
@@ -791,12 +791,17 @@ struct Batch::Impl {
         put(stepPosqD, stepPosq.data(), sizeof(const float4*) * n);
         launchStepGathers(0, stepsD.as<CoordStep>(), (int)steps.size(), grid, atomsD.as<int>(), gBD.as<int>(),
                           gAD.as<int>(), ta, ch);
+        // per-step pair constants (items and walker boxes are fixed for the batch)
+        if (stepConstD.bytes < runConstBytes() * n) { stepConstD.alloc(runConstBytes() * n); destroyGraph(); }
+        launchStepConsts(0, stepsD.as<CoordStep>(), (int)steps.size(), itemsD.as<CoordItem>(), boxesD.as<BoxDev>(),
+                         static_cast<RunConst*>(stepConstD.p));
         cudaCheck(cudaGetLastError(), "gather tables");
         cudaCheck(cudaDeviceSynchronize(), "gather tables");
         dev.R.numSteps = (int)steps.size();
         dev.R.gB = gBD.as<int>();
         dev.R.gA = gAD.as<int>();
         dev.R.stepPosq = stepPosqD.as<const float4*>();
+        dev.R.stepConst = static_cast<const RunConst*>(stepConstD.p);
         dev.R.steps = stepsD.as<CoordStep>();
         dev.R.items = itemsD.as<CoordItem>();
         dev.items = itemsD.as<CoordItem>();

@@ -130,6 +130,22 @@ __global__ void k_step_gathers(const CoordStep* __restrict__ steps, int numSteps
     }
 }
 
+// Pair constants of every step (runConst of its item and system box), for runs
+// whose items and boxes are fixed: the runs kernel then copies them with the
+// step records instead of computing them from two more dependent loads.
+__global__ void k_step_consts(const CoordStep* __restrict__ steps, int numSteps, const CoordItem* __restrict__ items,
+                              const BoxDev* __restrict__ sysBox, RunConst* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < numSteps) out[s] = runConst(items[steps[s].item], sysBox[steps[s].sys]);
+}
+
+void launchStepConsts(cudaStream_t s, const CoordStep* steps, int numSteps, const CoordItem* items,
+                      const BoxDev* sysBox, RunConst* out) {
+    if (numSteps > 0) k_step_consts<<<(numSteps + 255) / 256, 256, 0, s>>>(steps, numSteps, items, sysBox, out);
+}
+
+size_t runConstBytes() { return sizeof(RunConst); }
+
 void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
                        int* gA, int ta, int ch) {
     const long long n = (long long)numSteps * (ta > ch ? ta : ch);

@@ -62,7 +62,7 @@ constexpr int F_FIRST = COORD_F_FIRST, F_LAST = COORD_F_LAST;
 }  // namespace crun
 
 // Pair constants of one item in scaled units (coordinates divided by r0).
-struct RunConst {
+struct alignas(16) RunConst {
     float lo, hi;       // valid pairs: lo <= x^2 < hi
     float n, m;         // general exponents (kind 0)
     int ni, mi;         // integer exponents (kind -1)
@@ -77,7 +77,7 @@ struct CoordRunSmem {
     float4 apos[2][crun::NW * RA];
     float g[2][crun::NW][32 * RB * 3];
     CoordStep st[crun::WIN];
-    RunConst kst[crun::WIN];   // constants of the window's steps that start a tile run
+    alignas(16) RunConst kst[crun::WIN];   // constants of the window's steps (those that start a tile run)
     double red[2][crun::NW];
 };
 
@@ -361,27 +361,45 @@ __device__ void coordRun(const CoordRunDev& R, int s0, int s1, CoordRunSmem<RA, 
             if (tid < TA && ia != -1) cpAsync16(&sm.apos[b][tid], pq + (ia >= 0 ? ia : 0), ia >= 0);
             cpAsyncCommit();
         };
-        // the window's first two steps: gathers first, then the step records
-        // (both independent), then the constants of the steps that start a tile
-        // run, while the gathers land
-        {
+        if (R.stepConst) {
+            // constants precomputed per step: the step records and constants of the
+            // window are copied along with the first two steps' gathers (nothing
+            // to wait for before issuing them), one round trip after the indices
+            const int4* src = reinterpret_cast<const int4*>(R.steps + w0);
+            for (int i = tid; i < nw * 2; i += blockDim.x) cpAsync16(reinterpret_cast<int4*>(sm.st) + i, src + i, true);
+            constexpr int W16 = (int)(sizeof(RunConst) / 16);
+            const int4* cs = reinterpret_cast<const int4*>(R.stepConst + w0);
+            for (int i = tid; i < nw * W16; i += blockDim.x)
+                cpAsync16(reinterpret_cast<int4*>(sm.kst) + i, cs + i, true);
             int ib0, ia0, ib1 = -1, ia1 = -1;
             const float4 *pq0, *pq1 = nullptr;
             loadIdx(0, ib0, ia0, pq0);
             if (nw > 1) loadIdx(1, ib1, ia1, pq1);
             issue(0, ib0, ia0, pq0);
             if (nw > 1) issue(1, ib1, ia1, pq1);
-        }
-        {
-            const int4* src = reinterpret_cast<const int4*>(R.steps + w0);
-            int4* dst = reinterpret_cast<int4*>(sm.st);
-            for (int i = tid; i < nw * 2; i += blockDim.x) dst[i] = __ldg(src + i);
-        }
-        __syncthreads();
-        for (int i = tid; i < nw; i += blockDim.x) {
-            const CoordStep& d = sm.st[i];
-            if (w0 + i == s0 || i == 0 || (stepFlags(d.packed) & F_FIRST))
-                sm.kst[i] = runConst(R.items[d.item], R.sysBox[d.sys]);
+        } else {
+            // the window's first two steps: gathers first, then the step records
+            // (both independent), then the constants of the steps that start a
+            // tile run, while the gathers land
+            {
+                int ib0, ia0, ib1 = -1, ia1 = -1;
+                const float4 *pq0, *pq1 = nullptr;
+                loadIdx(0, ib0, ia0, pq0);
+                if (nw > 1) loadIdx(1, ib1, ia1, pq1);
+                issue(0, ib0, ia0, pq0);
+                if (nw > 1) issue(1, ib1, ia1, pq1);
+            }
+            {
+                const int4* src = reinterpret_cast<const int4*>(R.steps + w0);
+                int4* dst = reinterpret_cast<int4*>(sm.st);
+                for (int i = tid; i < nw * 2; i += blockDim.x) dst[i] = __ldg(src + i);
+            }
+            __syncthreads();
+            for (int i = tid; i < nw; i += blockDim.x) {
+                const CoordStep& d = sm.st[i];
+                if (w0 + i == s0 || i == 0 || (stepFlags(d.packed) & F_FIRST))
+                    sm.kst[i] = runConst(R.items[d.item], R.sysBox[d.sys]);
+            }
         }
         cpAsyncWaitAll();
         __syncthreads();

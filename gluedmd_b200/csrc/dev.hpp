@@ -74,6 +74,8 @@ struct GroupDev {
     int nInl;
 };
 
+struct RunConst;   // pair constants of a coordination step (coord_run.cuh)
+
 // Coordination CVs: all-pairs tiles with deterministic partial sums.
 struct CoordItem {
     int cv;
@@ -177,6 +179,7 @@ struct CoordRunDev {
     const float4* const* sysPosq;  // positions of system CoordStep::sys
     const BoxDev* sysBox;      // box of system CoordStep::sys
     unsigned long long* acc;   // [rows][3] fixed-point gradient sums
+    const RunConst* stepConst;  // [numSteps] pair constants of every step, or nullptr: computed in the kernel
     double* cnPiece;           // CN partial of every run piece, item-contiguous (CoordItem::pieceBegin/End)
     unsigned long long* cellCn;  // [items]: CN of cell-list items in 64-bit fixed point (cleared by the reader)
 };

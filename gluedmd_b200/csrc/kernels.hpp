@@ -33,6 +33,10 @@ void launchComposeSlots(cudaStream_t s, const int* atoms, const int* u2g, int* s
 void launchStepGathers(cudaStream_t s, const CoordStep* steps, int numSteps, int grid, const int* slots, int* gB,
                        int* gA, int ta = COORD_TA, int ch = COORD_CH);
 int coordRunOccupancy(int kind, int boxKind, bool hi);
+// out[s] = pair constants of step s (fixed items and boxes); runConstBytes() = sizeof(RunConst)
+void launchStepConsts(cudaStream_t s, const CoordStep* steps, int numSteps, const CoordItem* items,
+                      const BoxDev* sysBox, RunConst* out);
+size_t runConstBytes();
 // Cutoff coordination items on the cell-list path (coord_cells.cu): bin the B
 // atoms, then pair terms into acc and the items' CN accumulators (before
 // k_coord_finalize). kind as
