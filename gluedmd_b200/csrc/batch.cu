@@ -12,11 +12,12 @@
 //      run piece), then evaluates an equal slice of the shared hill table for
 //      every walker (slice and hill-CV atoms staged in shared memory when the
 //      CTA starts), one FP64 partial per (CTA, walker).
-//   2. k_batch_finalize, walkers x parts CTAs: each part clears and scatters its
-//      share of the walker's coordination rows (dU/dCN needs only CN and the
-//      harmonic terms: the hill bias acts on distance/angle/dihedral CVs); part
-//      0 also sums the hill partials in CTA order and completes the walker
-//      (harmonic terms, energy, the distance/angle/dihedral rows).
+//   2. k_batch_finalize, walkers x parts CTAs: parts 1, 2, ... clear and scatter
+//      their shares of the walker's coordination rows (dU/dCN needs only CN and
+//      the harmonic terms: the hill bias acts on distance/angle/dihedral CVs);
+//      part 0 sums the hill partials in CTA order and completes the walker
+//      (harmonic terms, energy, the distance/angle/dihedral rows), and takes
+//      the rows too only when it is the walker's one part.
 //
 // Every reduction has a fixed order or is an integer sum, so a step is bitwise
 // reproducible. Deposition (updateState at pace): one hill per walker, in walker
@@ -458,10 +459,13 @@ __global__ void __launch_bounds__(RUNS_THREADS, 1) k_batch_runs(BatchDev B) {
 //     harmonic terms (the hill bias acts only on distance/angle/dihedral CVs);
 //     the part's coordination rows are scattered (gradient rounded to float as
 //     in the per-context Jacobian table);
-//   - part 0 also completes the walker: distance/angle/dihedral CVs, the hill
+//   - part 0 completes the walker: distance/angle/dihedral CVs, the hill
 //     partials of the runs CTAs summed in CTA order (lane-strided, fixed xor
 //     tree), harmonic terms and hill bias, CVs and energies, and the
-//     distance/angle/dihedral rows.
+//     distance/angle/dihedral rows. With more than one part it has no
+//     coordination rows: its own chain of dependent steps is the longest, and
+//     without the rows' loads and scatter the walker's last CTA ends ~1.3 us
+//     earlier at C4 (64 walkers, 1,280 rows each).
 // Copies n bytes (multiple of 4) from global to shared memory, all threads.
 __device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
     const int* s = static_cast<const int*>(src);
@@ -497,8 +501,11 @@ __device__ void finalizeItem(const BatchDev& B, int fi, FinSmem& fs) {
     const BHill& hb = B.hill;
     unsigned long long* st = B.fstamps ? B.fstamps + 6 * (size_t)fi : nullptr;
     if (st && tid == 0) st[0] = globalTimer();
-    const int r0 = (int)((long long)B.rowsPerWalker * part / B.parts);
-    const int r1 = (int)((long long)B.rowsPerWalker * (part + 1) / B.parts);
+    // coordination rows: with more than one part, part 0 only completes the
+    // walker and parts 1, 2, ... share the rows; a single part does both
+    const int rowParts = B.parts > 1 ? B.parts - 1 : 1, rp = B.parts > 1 ? part - 1 : 0;
+    const int r0 = rp < 0 ? 0 : (int)((long long)B.rowsPerWalker * rp / rowParts);
+    const int r1 = rp < 0 ? 0 : (int)((long long)B.rowsPerWalker * (rp + 1) / rowParts);
     long long vx[ROWS_PER_THREAD], vy[ROWS_PER_THREAD], vz[ROWS_PER_THREAD];
     int rItem[ROWS_PER_THREAD], rAtom[ROWS_PER_THREAD];
     const size_t rowBase = (size_t)w * B.rowsPerWalker;
@@ -808,7 +815,10 @@ struct Batch::Impl {
         dev.R.cnPiece = cnPiece.as<double>();
     }
 
-    int minParts() const { return std::max(1, (rows + FT * ROWS_PER_THREAD - 1) / (FT * ROWS_PER_THREAD)); }
+    // finalize CTAs whose rows fit: ceil(rows / (FT ROWS_PER_THREAD)), plus the
+    // walker part when that is more than one
+    int rowCTAs() const { return std::max(1, (rows + FT * ROWS_PER_THREAD - 1) / (FT * ROWS_PER_THREAD)); }
+    int minParts() const { return rowCTAs() == 1 ? 1 : rowCTAs() + 1; }
 
     void plan() {
         // coordination steps over all walkers' items (walker-major)
@@ -1122,7 +1132,12 @@ void Batch::setTuning(const BatchTuning& t) {
     impl_->plan();
 }
 
-BatchTuning Batch::tuning() const { return impl_->tune; }
+// The tuning in effect: finalize parts as launched (requested, or the fewest).
+BatchTuning Batch::tuning() const {
+    BatchTuning t = impl_->tune;
+    t.parts = impl_->parts;
+    return t;
+}
 bool Batch::lastTuneCached() const { return impl_->cachedTune; }
 
 void Batch::setSumPrecision(int mode) {
@@ -1219,15 +1234,22 @@ BatchTuning Batch::autotune(bool useCache) {
     for (auto& e : ev) cudaCheck(cudaEventCreate(&e), "event");
     BatchTuning best = I.tune;
     float bestMs = 1e30f;
-    const int base = I.minParts();
+    // finalize parts: the fewest, then r row CTAs + the walker part for r = the
+    // fewest row CTAs + 0, 1, 2 and x2, x4 (a grid over the SMs' resident CTAs
+    // adds a second wave: 64 walkers x 7 parts of 256 threads at 80 registers
+    // run 4 CTAs late and cost C4 ~1 us against 6 parts)
+    const int rb = I.rowCTAs();
+    std::vector<int> partsList = {I.minParts()};
+    for (int r : {rb, rb + 1, rb + 2, 2 * rb, 4 * rb})
+        if (std::find(partsList.begin(), partsList.end(), r + 1) == partsList.end()) partsList.push_back(r + 1);
     std::vector<BatchTuning> cands;
     for (int ra : {8, 4})
         for (int ch : {128, 256}) {
             if (!shapeAvailable(I.boxKind, I.kind, I.sumMode == SUM_FP32C, ra, ch)) continue;
             for (int plain : {0, 1})
-                for (int mul : {1, 2, 4}) {
+                for (int parts : partsList) {
                     BatchTuning t;
-                    t.ra = ra; t.ch = ch; t.parts = base * mul; t.plain = plain;
+                    t.ra = ra; t.ch = ch; t.plain = plain; t.parts = parts;
                     cands.push_back(t);
                 }
         }

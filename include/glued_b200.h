@@ -285,8 +285,10 @@ int glued_batch_create(const glued_force* const* forces, int num_walkers, const 
 int glued_batch_destroy(glued_batch* b);
 int glued_batch_set_stream(glued_batch* b, void* stream);
 /* Tuning: tune[4] = {ra (A atoms per warp of a coordination tile: 4 or 8, tile =
- * 16 ra atoms), finalize_parts (finalize CTAs per walker; 0 = the fewest that
- * cover the walker's coordination rows), finalize launch (0: a programmatic
+ * 16 ra atoms), finalize_parts (finalize CTAs per walker, 512 coordination
+ * rows at most per CTA; 0 = the fewest: one when the walker has at most 512
+ * rows, otherwise the CTAs that cover them plus one that completes the walker;
+ * raised to that number when lower), finalize launch (0: a programmatic
  * dependent launch of the runs kernel, 1: a plain stream-ordered launch), B chunk
  * (128 or 256 atoms; 0 = 128)}. Tile shapes other than ra 8 / chunk 128 exist for
  * the n = 6, m = 12 switch in rectangular or no boxes with plain FP32 sums.
@@ -297,7 +299,9 @@ int glued_batch_set_stream(glued_batch* b, void* stream);
  * is cached for the process per (walker count, coordination group sizes, hill
  * count to a power of two, box kind, switch kind, sum precision);
  * glued_batch_autotune uses the cache, glued_batch_autotune_ex(use_cache = 0)
- * times again (*cached = 1 when the returned choice came from the cache).      */
+ * times again (*cached = 1 when the returned choice came from the cache).
+ * glued_batch_get_tuning returns the tuning in effect (finalize_parts as
+ * launched).                                                                   */
 int glued_batch_set_tuning(glued_batch* b, const int tune[4]);
 int glued_batch_get_tuning(glued_batch* b, int tune[4]);
 int glued_batch_autotune(glued_batch* b, int tune[4]);

@@ -52,16 +52,22 @@ def _oracle(w, biases, hill):
     return s
 
 
-@pytest.mark.parametrize("coord,parts,plain", [((64, 256), 0, 0), ((64, 256), 5, 1), ((900, 1500), 0, 0)])
+@pytest.mark.parametrize("coord,parts,plain", [((64, 256), 0, 0), ((64, 256), 2, 0), ((64, 256), 5, 1),
+                                                ((900, 1500), 0, 0)])
 @pytest.mark.parametrize("with_hills", [False, True])
 def test_batch_matches_fp64_oracle(with_hills, coord, parts, plain):
     """The batched step against the FP64 oracle: full coordination tiles with
-    the fewest finalize parts per walker (programmatic dependent launch) and
-    with more parts than rows need (plain launch), and ragged tiles (partial A
-    tiles and B chunks, 2,400 rows per walker over five finalize parts)."""
+    the fewest finalize parts per walker (one CTA for the walker and its 320
+    rows, programmatic dependent launch), with a walker part and one row part,
+    and with more parts than the rows need (plain launch); ragged tiles
+    (partial A tiles and B chunks, 2,400 rows per walker: five row parts and
+    the walker part)."""
     ws, hill = _walkers(coord=coord)
     b, walkers, specs = _setup(ws, hill, with_hills)
     b.set_tuning(8, parts, plain)
+    rows = sum(coord)
+    fewest = 1 if rows <= 512 else -(-rows // 512) + 1
+    assert b.tuning["parts"] == max(parts, fewest)
     for wk in walkers:
         wk.force.zero_()
     b.execute()
