@@ -559,6 +559,24 @@ def run_c4(args, torch, ws, hill):
                 graphed=True, runs_us=runs_us, finalize_us=fin_us, hill_wait_us=hill_wait_us, parity=parity)
 
 
+def c4_phase_timeline(b, flush, calls=15):
+    """Medians over `calls` steps (L2 flushed before each) of Batch.phase_times
+    and, from the raw per-CTA stamps (%globaltimer), the finalize CTAs' six
+    stamps per part relative to the exit of the last runs CTA (microseconds)."""
+    pts, rel = [], []
+    for _ in range(calls):
+        flush.add_(1.0)
+        pts.append(b.phase_times())
+        runs, fin = b.phase_stamps()
+        r, f = runs[:, 2:].astype(np.int64), fin.astype(np.int64)
+        end = r[:, 5].max()
+        parts = int(pts[-1]["parts"])
+        part = np.arange(f.shape[0]) % parts
+        rel.append([[float(np.median(f[part == q, k] - end)) * 1e-3 for k in range(6)] for q in range(parts)])
+    return {"phase_times": {k: round(float(np.median([p[k] for p in pts])), 3) for k in pts[0]},
+            "finalize_stamps_after_runs_end_us": np.round(np.median(np.array(rel), axis=0), 3).tolist()}
+
+
 def cpu_reference_c4(ws, hill, steps_budget_s=20.0, threads=None):
     """The reference's kernels compiled for the host (oracle/_ref), one RefSystem
     per walker, walkers spread over host threads (ctypes releases the GIL).
@@ -709,6 +727,8 @@ def main():
     ap.add_argument("--walkers", type=int, default=64, help="C4 walker count (profiling of small cases)")
     ap.add_argument("--hills", type=int, default=50000, help="C4 hill count (profiling of small cases)")
     ap.add_argument("--tuning", default="8,0,0", help="fixed C4 tuning ra,finalize_parts,plain_finalize_launch (--profile)")
+    ap.add_argument("--phases", action="store_true",
+                    help="with --profile --config c4: per-CTA phase stamps of 15 more steps (Batch.phase_times)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -777,8 +797,11 @@ def main():
         b.set_tuning(tv[0], tv[1], tv[2])
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
         ms = time_steps(torch, lambda i: (b.update_state(i), b.execute()), args.steps, args.warmup, flush)
-        print(json.dumps({"profile": "c4", "walkers": args.walkers, "hills": b.num_hills(), "ms_per_step": ms / args.steps,
-                          "status": b.status(), "tuning": b.tuning}))
+        out = {"profile": "c4", "walkers": args.walkers, "hills": b.num_hills(), "ms_per_step": ms / args.steps,
+               "status": b.status(), "tuning": b.tuning}
+        if args.phases:
+            out["phases"] = c4_phase_timeline(b, flush)
+        print(json.dumps(out))
         return
 
     if args.config == "c4":
