@@ -464,8 +464,8 @@ __global__ void __launch_bounds__(RUNS_THREADS, 1) k_batch_runs(BatchDev B) {
 //     tree), harmonic terms and hill bias, CVs and energies, and the
 //     distance/angle/dihedral rows. With more than one part it has no
 //     coordination rows: its own chain of dependent steps is the longest, and
-//     without the rows' loads and scatter the walker's last CTA ends ~1.3 us
-//     earlier at C4 (64 walkers, 1,280 rows each).
+//     without the rows' loads and scatter it ends ~0.6 us earlier and the C4
+//     step (64 walkers, 1,280 rows each) takes ~1 us less.
 // Copies n bytes (multiple of 4) from global to shared memory, all threads.
 __device__ __forceinline__ void copyWords(void* dst, const void* src, int n) {
     const int* s = static_cast<const int*>(src);
@@ -1237,7 +1237,7 @@ BatchTuning Batch::autotune(bool useCache) {
     // finalize parts: the fewest, then r row CTAs + the walker part for r = the
     // fewest row CTAs + 0, 1, 2 and x2, x4 (a grid over the SMs' resident CTAs
     // adds a second wave: 64 walkers x 7 parts of 256 threads at 80 registers
-    // run 4 CTAs late and cost C4 ~1 us against 6 parts)
+    // run 4 CTAs late and cost C4 ~2 us against 6 parts)
     const int rb = I.rowCTAs();
     std::vector<int> partsList = {I.minParts()};
     for (int r : {rb, rb + 1, rb + 2, 2 * rb, 4 * rb})
