@@ -83,6 +83,53 @@ def test_batch_matches_fp64_oracle(with_hills, coord, parts, plain):
         assert err < 1e-4, (i, err)
 
 
+@pytest.mark.parametrize("group2,parts", [((32, 128), 0), ((32, 128), 3), ((96, 400), 0), ((96, 400), 5)])
+def test_batch_two_coordination_items(group2, parts):
+    """Two coordination CVs per walker, both restrained: the finalize's rows run
+    over both items (item 0's A and B rows, then item 1's) and split across the
+    row CTAs at arbitrary row boundaries. 480 rows fit one CTA (the fewest parts:
+    one CTA completes the walker and takes every row; 3 parts: the walker CTA
+    and two row CTAs); 816 rows need two row CTAs and the walker CTA (the
+    fewest), or four."""
+    import torch
+    from gluedmd_b200.batch import Batch, Walker, force_for, c4_biases
+    from gluedmd_b200 import workloads as W
+    ws, hill = _walkers(n_walkers=4, coord=(64, 256))
+    nA2, nB2 = group2
+    forces, walkers, specs = [], [], []
+    for i, w in enumerate(ws):
+        rng = np.random.default_rng(77 + i)
+        A2 = rng.choice(w["n"], nA2, replace=False)
+        B2 = rng.choice(w["n"], nB2, replace=False)
+        w["cvs"] = list(w["cvs"]) + [(W.CV_COORDINATION, [nA2] + [int(x) for x in A2] + [int(x) for x in B2],
+                                      [0.35, 6, 12])]
+        cn1 = W.coordination_cn_fp64(w["pos"], w["A"], w["B"], w["L"])
+        cn2 = W.coordination_cn_fp64(w["pos"], A2, B2, w["L"])
+        biases = c4_biases(dict(w, d0=w["d0"] + 0.05), hill["params"], hill["iparams"], cn0=cn1 * 1.01 + 2.0)
+        biases.append((1, [4], [100.0, cn2 * 1.01 + 2.0], [0]))
+        forces.append(force_for(w["cvs"], biases))
+        walkers.append(Walker(w["pos"], w["box"]))
+        specs.append(biases)
+    b = Batch(forces, walkers)
+    b.set_hills(hill["centers"], hill["heights"])
+    b.set_tuning(8, parts, 0)
+    rows = 64 + 256 + nA2 + nB2
+    fewest = 1 if rows <= 512 else -(-rows // 512) + 1
+    assert b.tuning["parts"] == max(parts, fewest)
+    for wk in walkers:
+        wk.force.zero_()
+    b.execute()
+    E = b.energies()
+    cv = b.cv_values()
+    assert b.status() == 0
+    for i, w in enumerate(ws):
+        r = _oracle(w, specs[i], hill).execute(w["pos"], w["box"].ravel())
+        np.testing.assert_allclose(cv[i], r["cv_values"], rtol=1e-5, atol=1e-5)
+        assert abs(E[i] - r["energy"]) <= 1e-4 * max(1.0, abs(r["energy"])), (i, E[i], r["energy"])
+        err = O.max_rel_force_err(walkers[i].forces(), r["forces"])
+        assert err < 1e-4, (i, err)
+
+
 def test_batch_repeatable_and_autotuned():
     ws, hill = _walkers(n_walkers=5)
     b, walkers, specs = _setup(ws, hill, True)
